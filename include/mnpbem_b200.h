@@ -1,0 +1,229 @@
+/*
+ * mnpbem_b200 -- C ABI of the B200 boundary-element hot path.
+ *
+ * Plain C types only: device pointers are raw addresses of caller-owned
+ * device memory (the library never frees caller memory), host pointers are
+ * host memory, sizes are int64_t, streams are cudaStream_t passed as void*.
+ * Every entry point returns 0 on success or one of the MNPB_E* codes; the
+ * message of the last failure on the calling thread is returned by
+ * mnpb_last_error().  No entry point falls back to the CPU.
+ *
+ * Layouts (all column-major, "ld" = leading dimension in elements):
+ *   c128 matrix  : interleaved complex double, element (i,j) at 2*(j*ld+i)
+ *   c32p matrix  : planar complex float, a real plane then an imaginary
+ *                  plane, each n x n with leading dimension ld; the planes
+ *                  are `plane` elements apart
+ *   batches      : `batch` matrices `stride` elements apart
+ *
+ * The reference (PyMNPBEM) has no native interface; each entry point below
+ * names the reference Python function whose arithmetic it replaces.  The
+ * Python classes in mnpbem_b200/ (BEMRet, BEMStat, CompGreenRet, ...) keep
+ * the reference call surface and call these functions through ctypes.
+ */
+#ifndef MNPBEM_B200_H
+#define MNPBEM_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MNPB_OK 0
+#define MNPB_EINVAL 1      /* invalid argument (null pointer, bad size)     */
+#define MNPB_ECUDA 2       /* CUDA runtime / launch error                  */
+#define MNPB_ESINGULAR 3   /* exactly zero pivot met during factorisation  */
+#define MNPB_ENOCONV 4     /* iterative method did not reach its tolerance */
+#define MNPB_ETIMEOUT 5    /* a bounded device-side wait gave up           */
+#define MNPB_ENOMEM 6      /* workspace too small                          */
+
+/* Library version (major*10000 + minor*100 + patch). */
+int mnpb_version(void);
+
+/* Text of the last error on the calling thread ("" if none). */
+const char *mnpb_last_error(void);
+
+/* Number of kernel launches issued by this library since load (host-side
+ * counter; used to report how many of the library's kernels ran). */
+int64_t mnpb_launch_count(void);
+
+/* ---------------------------------------------------------------------------
+ * Geometry set-up (once per particle mesh)
+ * ------------------------------------------------------------------------- */
+
+/* Near/self classification of face pairs, host side, integer-exact.
+ * Replaces mnpbem/greenfun/refine_utils.py:29 refinematrix (and its twin
+ * mnpbem/greenfun/utils.py:43).  pos*: n x 3 row-major doubles, rad*:
+ * boundary-element radii.  Writes CSR rows (row_ptr n1+1), column indices
+ * and kinds (1 near, 2 self) for up to `cap` pairs; *nnz receives the total
+ * count.  Returns MNPB_ENOMEM (after setting *nnz) if cap is too small. */
+int mnpb_refinematrix(int64_t n1, int64_t n2, const double *pos1, const double *pos2,
+                      const double *rad1, const double *rad2, double abs_cutoff,
+                      double rel_cutoff, int64_t cap, int64_t *nnz, int64_t *row_ptr,
+                      int32_t *cols, int8_t *kinds);
+
+/* Refined Green-function Taylor coefficients on the GPU (FP64).
+ * Replaces mnpbem/greenfun/greenret_refined.py:122-516 (_refine_diagonal and
+ * _refine_offdiagonal, deriv='cart', order 5) and the static refinement of
+ * mnpbem/greenfun/compgreen_stat.py:327-416.
+ * Device inputs: face data pos/nvec/tvec1/tvec2 (n x 3 row-major), pair list
+ * rows/cols/kinds (nref), face-quadrature points qpos (P x 3), weights qw and
+ * per-face offsets qoff (n+1), polar points ppos/pw/poff likewise.
+ * Device outputs: g (nref x 6), f (nref x 3 x 6) real Taylor coefficients,
+ * gstat, fstat (nref) static G and F values of the refined pairs. */
+int mnpb_refine_coefficients(void *stream, int64_t n, const double *pos, const double *nvec,
+                             const double *tvec1, const double *tvec2, int64_t nref,
+                             const int32_t *rows, const int32_t *cols, const int8_t *kinds,
+                             const double *qpos, const double *qw, const int64_t *qoff,
+                             const double *ppos, const double *pw, const int64_t *poff,
+                             double *g, double *f, double *gstat, double *fstat);
+
+/* Adds the closed-surface correction corr_i nvec_i to f[:, :, 0] of the self
+ * pairs, corr_i = -2 pi cdir_i - fsum_i on faces with cdir_i = +-1 (the
+ * normal direction of their closed surface; 0 = not closed; cdir may be
+ * NULL), and writes fn[:, m] = nvec_row . f[:, :, m].
+ * Replaces mnpbem/greenfun/compgreen_ret.py:376-400 (_apply_diag_corrections)
+ * and the nvec contraction of greenret_refined.py:769-774. */
+int mnpb_refine_finalize(void *stream, int64_t n, int64_t nref, const int32_t *rows,
+                         const int32_t *cols, const double *nvec, const double *cdir,
+                         const double *fsum, double *f, double *fn);
+
+/* Closed-surface sums f_j = sum_i a_i F_ij / a_j of the refined static F over
+ * the closed surface of face j (rows grp_lo[j]..grp_hi[j]-1).  Replaces
+ * mnpbem/greenfun/compgreen_ret.py:302-356 (_fun_closed).  The refined pairs
+ * are passed column-sorted (CSC: cptr n+1, crows, cfstat). */
+int mnpb_closure_sums(void *stream, int64_t n, const double *pos, const double *nvec,
+                      const double *area, const int64_t *grp_lo, const int64_t *grp_hi,
+                      const int64_t *cptr, const int32_t *crows, const double *cfstat,
+                      double *fsum);
+
+/* Full refined quasistatic F (n x n real, column-major) with the closure
+ * term -2 pi cdir_i - fsum_i added on the diagonal of closed faces.  Replaces
+ * mnpbem/greenfun/compgreen_stat.py:219-294 (+ _handle_closed_surfaces).
+ * Refined pairs in CSR (rptr, rcols, rfstat). */
+int mnpb_static_matrix(void *stream, int64_t n, const double *pos, const double *nvec,
+                       const double *area, const int64_t *rptr, const int32_t *rcols,
+                       const double *rfstat, const double *cdir, const double *fsum, double *F,
+                       int64_t ld);
+
+/* ---------------------------------------------------------------------------
+ * Per-wavelength retarded assembly (batched over wavelengths)
+ * ------------------------------------------------------------------------- */
+
+/* Writes G1, H1, G2, H2 for `batch` wavelengths.  Replaces
+ * mnpbem/bem/bem_ret.py:407-423 with mnpbem/greenfun/compgreen_ret.py:739-858
+ * and greenret_refined.py:654-810 (G = a/d, F = n.r (ik-1/d)/d^2 a, refined
+ * overlay sum_n c_n (ik)^n, phase exp(ikd), H = F +- 2 pi on the diagonal).
+ * Particle blocks: nparts particles, face offsets poff (nparts+1, host).
+ * kblk (device): batch x 2 x nparts x nparts complex wavenumbers (re,im)
+ * for side 1 (G1/H1) and side 2 (G2/H2); sblk (device, same shape) real
+ * signs (+1, -1 or 0 = block absent).
+ * Refined pairs: nref, rows, cols, g (nref x 6), fn (nref x 6) where
+ * fn[:, m] = n_row . f[:, :, m].
+ * out_mode 0: c128 outputs (G1,H1,G2,H2 pointers, ld, stride).
+ * out_mode 1: c32p outputs (planar float; plane offset `plane`). */
+int mnpb_assemble_ret(void *stream, int64_t n, int64_t batch, const double *pos,
+                      const double *nvec, const double *area, int nparts, const int64_t *poff,
+                      const double *kblk, const double *sblk, int64_t nref, const int32_t *rows,
+                      const int32_t *cols, const double *g, const double *fn, int out_mode,
+                      void *G1, void *H1, void *G2, void *H2, int64_t ld, int64_t stride,
+                      int64_t plane);
+
+/* ---------------------------------------------------------------------------
+ * Dense retarded solve (BEMRet), FP64, batched over wavelengths
+ * ------------------------------------------------------------------------- */
+
+/* Workspace bytes needed by mnpb_bemret_init_f64 for (n, batch). */
+int64_t mnpb_bemret_workspace_f64(int64_t n, int64_t batch);
+
+/* In place: G1 -> LU(G1), G2 -> LU(G2), H1 -> Sigma1 = H1 G1^-1,
+ * H2 -> Sigma (combined, LU-factorised), D -> Delta^-1.
+ * Replaces mnpbem/bem/bem_ret.py:437-523 (init).  eps (device, batch x 2
+ * complex): inside / outside dielectric constants (scalar per wavelength);
+ * kvac (device, batch) vacuum wavenumbers 2 pi / enei; nvec (device n x 3).
+ * piv (device int32, batch x 3 x n) receives the pivots of G1, G2, Sigma.
+ * All matrices c128, leading dimension ld, batch stride `stride`.
+ * info (device int32, batch) receives the first zero pivot (1-based) or 0. */
+int mnpb_bemret_init_f64(void *stream, int64_t n, int64_t batch, double *G1, double *G2,
+                         double *H1, double *H2, double *D, int64_t ld, int64_t stride,
+                         const double *eps, const double *kvac, const double *nvec,
+                         int32_t *piv, int32_t *info, void *work, int64_t work_bytes);
+
+/* Excitation variables phi, a, alpha, De (x_in layout of the solve) from
+ * the potentials of a batch of excitations.  Replaces
+ * mnpbem/bem/bem_ret.py:1360-1429 (_excitation).  pots (device c128,
+ * [batch][16][nrhs][n]): phi1, phi1p, a1 (x,y,z), a1p (x,y,z), phi2, phi2p,
+ * a2 (x,y,z), a2p (x,y,z). */
+int mnpb_bemret_excitation(void *stream, int64_t n, int64_t batch, int64_t nrhs,
+                           const double *pots, const double *eps, const double *kvac,
+                           const double *nvec, double *x_in);
+
+/* Surface charges/currents for nrhs excitations per wavelength.
+ * Replaces mnpbem/bem/bem_ret.py:1690-1810 (solve, Eqs. 19-20 of Garcia de
+ * Abajo & Howie).  In (device, c128, batch-major): phi (n x nrhs), a (n x 3 x
+ * nrhs), alpha (n x 3 x nrhs), De (n x nrhs) -- stored as one block
+ * x_in[batch][8][nrhs][n] in the order phi, a_x, a_y, a_z, De, alpha_x..z.
+ * Out: x_out[batch][8][nrhs][n] in the order sig1, h1x..z, sig2, h2x..z. */
+int mnpb_bemret_solve_f64(void *stream, int64_t n, int64_t batch, int64_t nrhs,
+                          const double *G1, const double *G2, const double *S1,
+                          const double *S, const double *D, int64_t ld, int64_t stride,
+                          const int32_t *piv, const double *eps, const double *kvac,
+                          const double *nvec, const double *x_in, double *x_out,
+                          void *work, int64_t work_bytes);
+
+/* ---------------------------------------------------------------------------
+ * Dense building blocks (exposed for tests and for the quasistatic solver)
+ * ------------------------------------------------------------------------- */
+
+/* Batched complex LU with partial pivoting (FP64, c128).  Replaces
+ * scipy.linalg.lu_factor as called from mnpbem/utils/gpu.py:145
+ * (lu_factor_dispatch).  piv: 0-based row interchanges, LAPACK order. */
+int mnpb_getrf_f64(void *stream, int64_t n, int64_t batch, double *A, int64_t ld,
+                   int64_t stride, int32_t *piv, int64_t pstride, int32_t *info);
+
+/* Batched LU solve A X = B for nrhs right-hand sides (c128, in place on B).
+ * Replaces scipy.linalg.lu_solve (mnpbem/utils/gpu.py:194). */
+int mnpb_getrs_f64(void *stream, int64_t n, int64_t batch, int64_t nrhs, const double *LU,
+                   int64_t ld, int64_t stride, const int32_t *piv, int64_t pstride,
+                   double *B, int64_t ldb, int64_t bstride);
+
+/* Batched complex GEMM C = alpha A B + beta C (c128, column-major). */
+int mnpb_zgemm(void *stream, int64_t m, int64_t n, int64_t k, int64_t batch,
+               double alpha_re, double alpha_im, const double *A, int64_t lda, int64_t sA,
+               const double *B, int64_t ldb, int64_t sB, double beta_re, double beta_im,
+               double *C, int64_t ldc, int64_t sC);
+
+/* Quasistatic matrix for a batch of wavelengths: M_b = -(diag(lambda_b) + F)
+ * with lambda = 2 pi (eps1+eps2)/(eps1-eps2) per face (eps12: device,
+ * batch x n x 2 complex).  Replaces mnpbem/bem/bem_stat.py:318-330. */
+int mnpb_stat_matrix(void *stream, int64_t n, int64_t batch, const double *F, int64_t ldf,
+                     const double *eps12, double *M, int64_t ld, int64_t stride);
+
+/* ---------------------------------------------------------------------------
+ * Plane-wave excitation and cross sections (batched over wavelengths)
+ * ------------------------------------------------------------------------- */
+
+/* Plane-wave potentials for a batch of wavelengths, written in the pots
+ * layout of mnpb_bemret_excitation.  Replaces
+ * mnpbem/simulation/planewave_ret.py:257-361 (potential).  pol, dirs: npol x 3
+ * (host-independent device arrays); kmed (batch complex), k0 (batch). */
+int mnpb_planewave_potential(void *stream, int64_t n, int64_t batch, int64_t npol,
+                             const double *pos, const double *nvec, const int8_t *side_in,
+                             const int8_t *side_out, const double *pol, const double *dirs,
+                             const double *kmed, const double *k0, double *pots);
+
+/* Far field e (ndir x 3 x npol per wavelength) of the solution for the
+ * directions dirs (ndir x 3).  Replaces mnpbem/spectrum/spectrum_ret.py:231
+ * (farfield).  side_in/side_out (device int8, n): 1 if the face's inside /
+ * outside medium is the embedding medium.  kmed: batch complex wavenumbers
+ * in the medium; k0: batch vacuum wavenumbers.  sol as written by
+ * mnpb_bemret_solve_f64.  e_out, h_out: device c128 [batch][npol][ndir][3]. */
+int mnpb_farfield(void *stream, int64_t n, int64_t batch, int64_t npol, int64_t ndir,
+                  const double *pos, const double *area, const int8_t *side_in,
+                  const int8_t *side_out, const double *dirs, const double *kmed,
+                  const double *k0, const double *sol, double *e_out, double *h_out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MNPBEM_B200_H */

@@ -1,0 +1,306 @@
+"""Dense BEM solvers on the GPU: ``BEMRet`` (retarded) and ``BEMStat``
+(quasistatic), with the reference call surface
+
+    sig, bem = bem.solve(exc)          # exc = PlaneWaveRet(...).potential(p, enei)
+
+(mnpbem/bem/bem_ret.py:138-1986, mnpbem/bem/bem_stat.py:101-807).  Every
+wavelength's matrices are assembled, factorised and solved by the CUDA
+library; results come back as host NumPy arrays in a ``CompStruct``.
+
+``solve_spectrum`` runs a whole list of wavelengths through the same kernels
+in batches (all wavelengths of a batch share every launch), which is how a
+spectrum should be computed on the GPU.
+"""
+
+import numpy as np
+import torch
+
+from . import _lib
+from ._lib import call, ptr
+from .compstruct import CompStruct
+from .greenfun import CompGreenRet, CompGreenStat
+from .materials import eps_k
+
+__all__ = ["BEMRet", "BEMStat"]
+
+
+def _check_particle(p, name):
+    if p is None:
+        raise ValueError("{}: 'p' must be a ComParticle (or compatible particle object), "
+                         "got None.".format(name))
+    if not (hasattr(p, 'pos') and hasattr(p, 'nvec') and hasattr(p, 'eps')):
+        raise TypeError("{}: 'p' must expose ComParticle-like attributes (pos, nvec, eps); "
+                        "got {!r}.".format(name, type(p).__name__))
+
+
+def _scalar_eps(p, enei):
+    """Inside/outside dielectric constants; must be uniform over the faces."""
+    e1 = np.asarray(p.eps1(enei))
+    e2 = np.asarray(p.eps2(enei))
+    if not (np.allclose(e1, e1[0]) and np.allclose(e2, e2[0])):
+        raise NotImplementedError("BEMRet: face-dependent eps (several materials on one side) "
+                                  "is not supported by the GPU solver")
+    return complex(e1[0]), complex(e2[0])
+
+
+class _RetBatch(object):
+    """Device buffers of one factorised batch of wavelengths (FP64)."""
+
+    def __init__(self, tables, eneis):
+        dev = tables.device
+        n = tables.n
+        B = len(eneis)
+        self.n, self.B, self.eneis = n, B, list(eneis)
+        c128 = dict(dtype=torch.complex128, device=dev)
+        self.G1, self.G2, self.H1, self.H2, self.D = [torch.empty((B, n, n), **c128) for _ in range(5)]
+        self.piv = torch.empty((B, 3 * n), dtype=torch.int32, device=dev)
+        self.info = torch.zeros(B, dtype=torch.int32, device=dev)
+        wb = int(_lib.lib().mnpb_bemret_workspace_f64(n, B))
+        self.work = torch.empty(wb, dtype=torch.uint8, device=dev)
+
+
+class BEMRet(object):
+    """Retarded BEM solver (full Maxwell equations), dense, on the GPU."""
+
+    def __init__(self, p, enei=None, **options):
+        _check_particle(p, 'BEMRet')
+        self.p = p
+        self.enei = None
+        self.options = dict(options)
+        refun = self.options.pop('refun', None)
+        schur = self.options.pop('schur', False)
+        if refun is not None or schur:
+            raise NotImplementedError("BEMRet: refun/schur are not supported by the GPU solver")
+        self.g = CompGreenRet(p, p, **self.options)
+        self.tables = self.g.tables
+        self.nvec = np.asarray(p.nvec)
+        self._batch = None
+        self.k = None
+        if enei is not None:
+            self.init(enei)
+
+    # ------------------------------------------------------------------ init
+    def _eps_tables(self, eneis):
+        B = len(eneis)
+        eps = np.zeros((B, 4))
+        kvac = np.zeros(B)
+        for b, enei in enumerate(eneis):
+            e1, e2 = _scalar_eps(self.p, enei)
+            eps[b] = (e1.real, e1.imag, e2.real, e2.imag)
+            kvac[b] = 2 * np.pi / enei
+        return eps, kvac
+
+    def _factor(self, eneis, stream=None):
+        t = self.tables
+        bt = _RetBatch(t, eneis)
+        kblk, sblk = t.k_tables(eneis)
+        t.assemble(kblk, sblk, (bt.G1, bt.H1, bt.G2, bt.H2), mode=0, stream=stream)
+        eps, kvac = self._eps_tables(eneis)
+        bt.eps = torch.from_numpy(eps).to(t.device)
+        bt.kvac = torch.from_numpy(kvac).to(t.device)
+        n, B = t.n, len(eneis)
+        call('mnpb_bemret_init_f64', _lib.stream_handle(stream), n, B, ptr(bt.G1), ptr(bt.G2),
+             ptr(bt.H1), ptr(bt.H2), ptr(bt.D), n, n * n, ptr(bt.eps), ptr(bt.kvac),
+             ptr(t.nvec), ptr(bt.piv), ptr(bt.info), ptr(bt.work), bt.work.numel())
+        return bt
+
+    def init(self, enei):
+        """Matrices for wavelength ``enei``; no-op if already there (bem_ret.py:293-311)."""
+        if self.enei is not None and np.isclose(self.enei, enei):
+            return self
+        self._batch = self._factor([enei])
+        info = self._batch.info.cpu().numpy()
+        if info.any():
+            raise _lib.MNPBError('BEMRet.init', 3, "zero pivot at column {}".format(int(info.max())))
+        self.enei = enei
+        self.k = 2 * np.pi / enei
+        return self
+
+    __call__ = init
+
+    def clear(self):
+        self._batch = None
+        self.enei = None
+        return self
+
+    # ----------------------------------------------------------------- solve
+    @staticmethod
+    def _pots(exc, n):
+        """Potentials of an excitation as a (16, K, n) complex host array."""
+        def get(name):
+            v = exc.get(name, 0) if hasattr(exc, 'get') else getattr(exc, name, 0)
+            return v if isinstance(v, np.ndarray) else None
+        fields = [get(k) for k in ('phi1', 'phi1p', 'a1', 'a1p', 'phi2', 'phi2p', 'a2', 'a2p')]
+        K = 1
+        for f in fields:
+            if f is not None:
+                if f.ndim == 3:
+                    K = max(K, f.shape[2])
+                elif f.ndim == 2 and f.shape[1] != 3:
+                    K = max(K, f.shape[1])
+        out = np.zeros((16, K, n), dtype=complex)
+        comp = 0
+        for f, width in zip(fields, (1, 1, 3, 3, 1, 1, 3, 3)):
+            if f is not None:
+                if width == 1:
+                    v = f.reshape(n, -1)
+                    out[comp] = np.broadcast_to(v, (n, K)).T
+                else:
+                    v = f.reshape(n, 3, -1)
+                    out[comp:comp + 3] = np.broadcast_to(v, (n, 3, K)).transpose(1, 2, 0)
+            comp += width
+        return out, K
+
+    def _solve_batch(self, bt, pots_dev, K, stream=None):
+        """x_out (B, 8, K, n) device for potentials (B, 16, K, n) device."""
+        t = self.tables
+        n, B = t.n, bt.B
+        sh = _lib.stream_handle(stream)
+        xin = torch.empty((B, 8, K, n), dtype=torch.complex128, device=t.device)
+        xout = torch.empty_like(xin)
+        call('mnpb_bemret_excitation', sh, n, B, K, ptr(pots_dev), ptr(bt.eps), ptr(bt.kvac),
+             ptr(t.nvec), ptr(xin))
+        wb = B * n * 15 * K * 16
+        work = torch.empty(wb, dtype=torch.uint8, device=t.device)
+        call('mnpb_bemret_solve_f64', sh, n, B, K, ptr(bt.G1), ptr(bt.G2), ptr(bt.H1),
+             ptr(bt.H2), ptr(bt.D), n, n * n, ptr(bt.piv), ptr(bt.eps), ptr(bt.kvac),
+             ptr(t.nvec), ptr(xin), ptr(xout), ptr(work), wb)
+        return xout
+
+    def solve(self, exc):
+        """Surface charges and currents for an excitation (bem_ret.py:1569-1831)."""
+        enei = exc['enei']
+        self.init(enei)
+        n = self.tables.n
+        pots, K = self._pots(exc, n)
+        d_pots = torch.from_numpy(pots).to(self.tables.device).unsqueeze(0)
+        xout = self._solve_batch(self._batch, d_pots, K)
+        x = xout[0].cpu().numpy()
+        sig = self._to_compstruct(x, K, enei)
+        return sig, self
+
+    def _to_compstruct(self, x, K, enei):
+        n = self.tables.n
+        sig1 = x[0].T.copy()
+        h1 = x[1:4].transpose(2, 0, 1).copy()
+        sig2 = x[4].T.copy()
+        h2 = x[5:8].transpose(2, 0, 1).copy()
+        if K == 1:
+            sig1, sig2 = sig1[:, 0], sig2[:, 0]
+            h1, h2 = h1[:, :, 0], h2[:, :, 0]
+        return CompStruct(self.p, enei, sig1=sig1, sig2=sig2, h1=h1, h2=h2)
+
+    def __truediv__(self, exc):
+        return self.solve(exc)
+
+    # ------------------------------------------------------- spectrum sweeps
+    def solve_spectrum(self, exc, eneis, batch=16, stream=None):
+        """Solutions for every wavelength of ``eneis`` (host CompStructs).
+
+        ``exc`` is a plane-wave excitation of this package (its potentials
+        are generated on the GPU) or any object with ``potential(p, enei)``.
+        """
+        out = []
+        for s in range(0, len(eneis), batch):
+            chunk = list(eneis[s:s + batch])
+            bt = self._factor(chunk, stream=stream)
+            pots, K = self._spectrum_pots(exc, chunk, stream)
+            xout = self._solve_batch(bt, pots, K, stream=stream)
+            x = xout.cpu().numpy()
+            for b, enei in enumerate(chunk):
+                out.append(self._to_compstruct(x[b], K, enei))
+        return out
+
+    def _spectrum_pots(self, exc, eneis, stream=None):
+        if hasattr(exc, 'potential_device'):
+            return exc.potential_device(self.p, self.tables, eneis, stream=stream)
+        n = self.tables.n
+        arrs = []
+        K = 1
+        for enei in eneis:
+            pots, K = self._pots(exc.potential(self.p, enei), n)
+            arrs.append(pots)
+        return torch.from_numpy(np.stack(arrs)).to(self.tables.device), K
+
+
+class BEMStat(object):
+    """Quasistatic BEM solver, dense, on the GPU (mnpbem/bem/bem_stat.py:101-807)."""
+
+    def __init__(self, p, enei=None, **options):
+        _check_particle(p, 'BEMStat')
+        self.p = p
+        self.options = dict(options)
+        if self.options.pop('schur', False):
+            raise NotImplementedError("BEMStat: schur is not supported by the GPU solver")
+        self.g = CompGreenStat(p, p, **self.options)
+        self.tables = self.g.tables
+        self.enei = None
+        self._M = None
+        if enei is not None:
+            self(enei)
+
+    @property
+    def F(self):
+        return self.g.F
+
+    def _factor(self, eneis, stream=None):
+        t = self.tables
+        n, B = t.n, len(eneis)
+        eps12 = np.zeros((B, n, 4))
+        for b, enei in enumerate(eneis):
+            e1 = np.asarray(self.p.eps1(enei))
+            e2 = np.asarray(self.p.eps2(enei))
+            eps12[b, :, 0], eps12[b, :, 1] = e1.real, e1.imag
+            eps12[b, :, 2], eps12[b, :, 3] = e2.real, e2.imag
+        d_eps = torch.from_numpy(eps12).to(t.device)
+        M = torch.empty((B, n, n), dtype=torch.complex128, device=t.device)
+        piv = torch.empty((B, n), dtype=torch.int32, device=t.device)
+        info = torch.zeros(B, dtype=torch.int32, device=t.device)
+        sh = _lib.stream_handle(stream)
+        call('mnpb_stat_matrix', sh, n, B, ptr(self.g.F_dev), n, ptr(d_eps), ptr(M), n, n * n)
+        call('mnpb_getrf_f64', sh, n, B, ptr(M), n, n * n, ptr(piv), n, ptr(info))
+        return M, piv, info
+
+    def __call__(self, enei):
+        if self.enei is None or self.enei != enei:
+            self._M, self._piv, info = self._factor([enei])
+            if info.cpu().numpy().any():
+                raise _lib.MNPBError('BEMStat', 3, "zero pivot")
+            self.enei = enei
+        return self
+
+    init = __call__
+
+    def solve(self, exc):
+        return self.__truediv__(exc)
+
+    def __truediv__(self, exc):
+        self(exc.enei)
+        phip = np.asarray(exc.phip)
+        n = self.tables.n
+        K = 1 if phip.ndim == 1 else phip.shape[1]
+        B = torch.from_numpy(np.ascontiguousarray(phip.reshape(n, K).T.astype(complex))) \
+            .to(self.tables.device).unsqueeze(0).contiguous()
+        call('mnpb_getrs_f64', _lib.stream_handle(), n, 1, K, ptr(self._M), n, n * n,
+             ptr(self._piv), n, ptr(B), n, n * K)
+        sig = B[0].cpu().numpy().T
+        if phip.ndim == 1:
+            sig = sig[:, 0]
+        return CompStruct(self.p, exc.enei, sig=sig), self
+
+    def solve_spectrum(self, phip, eneis, batch=32, stream=None):
+        """sigma (len(eneis), n, K) for a wavelength-independent phip (n, K)."""
+        n = self.tables.n
+        phip = np.asarray(phip).reshape(n, -1)
+        K = phip.shape[1]
+        out = []
+        for s in range(0, len(eneis), batch):
+            chunk = list(eneis[s:s + batch])
+            M, piv, info = self._factor(chunk, stream)
+            Bn = len(chunk)
+            rhs = torch.from_numpy(np.ascontiguousarray(
+                np.broadcast_to(phip.T.astype(complex), (Bn, K, n)))).to(self.tables.device)
+            call('mnpb_getrs_f64', _lib.stream_handle(stream), n, Bn, K, ptr(M), n, n * n,
+                 ptr(piv), n, ptr(rhs), n, n * K)
+            out.append(rhs.cpu().numpy().transpose(0, 2, 1))
+        return np.concatenate(out, axis=0)

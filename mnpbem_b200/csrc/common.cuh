@@ -1,0 +1,102 @@
+// Shared helpers for the mnpbem_b200 CUDA library (sm_100a).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <atomic>
+#include <cstdarg>
+#include <cstdio>
+#include <string>
+
+#include "../../include/mnpbem_b200.h"
+
+namespace mnpb {
+
+// ---------------------------------------------------------------------------
+// error state and launch accounting
+// ---------------------------------------------------------------------------
+void set_error(const char *fmt, ...);
+void clear_error();
+extern std::atomic<int64_t> g_launches;
+
+inline void count_launch(int64_t k = 1) { g_launches.fetch_add(k, std::memory_order_relaxed); }
+
+// Checks the last launch; returns MNPB_ECUDA with a message on failure.
+int check_launch(const char *what);
+
+#define MNPB_REQUIRE(cond, ...)            \
+    do {                                   \
+        if (!(cond)) {                     \
+            ::mnpb::set_error(__VA_ARGS__); \
+            return MNPB_EINVAL;            \
+        }                                  \
+    } while (0)
+
+#define MNPB_TRY(expr)                 \
+    do {                               \
+        int _rc = (expr);              \
+        if (_rc != MNPB_OK) return _rc; \
+    } while (0)
+
+#define MNPB_LAUNCH_CHECK(what)                          \
+    do {                                                 \
+        ::mnpb::count_launch();                          \
+        int _rc = ::mnpb::check_launch(what);            \
+        if (_rc != MNPB_OK) return _rc;                  \
+    } while (0)
+
+inline cudaStream_t as_stream(void *s) { return reinterpret_cast<cudaStream_t>(s); }
+
+inline int ceil_div(int64_t a, int64_t b) { return (int)((a + b - 1) / b); }
+
+// ---------------------------------------------------------------------------
+// complex double helpers (interleaved re, im)
+// ---------------------------------------------------------------------------
+typedef double2 cd;
+
+__host__ __device__ __forceinline__ cd cmk(double r, double i) { return make_double2(r, i); }
+__host__ __device__ __forceinline__ cd cadd(cd a, cd b) { return cmk(a.x + b.x, a.y + b.y); }
+__host__ __device__ __forceinline__ cd csub(cd a, cd b) { return cmk(a.x - b.x, a.y - b.y); }
+__host__ __device__ __forceinline__ cd cmul(cd a, cd b) {
+    return cmk(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__host__ __device__ __forceinline__ cd cscale(cd a, double s) { return cmk(a.x * s, a.y * s); }
+__host__ __device__ __forceinline__ cd cconj(cd a) { return cmk(a.x, -a.y); }
+// c + a*b with fused multiply-adds
+__device__ __forceinline__ cd cfma(cd a, cd b, cd c) {
+    c.x = fma(a.x, b.x, c.x);
+    c.x = fma(-a.y, b.y, c.x);
+    c.y = fma(a.x, b.y, c.y);
+    c.y = fma(a.y, b.x, c.y);
+    return c;
+}
+// c - a*b
+__device__ __forceinline__ cd cfms(cd a, cd b, cd c) {
+    c.x = fma(-a.x, b.x, c.x);
+    c.x = fma(a.y, b.y, c.x);
+    c.y = fma(-a.x, b.y, c.y);
+    c.y = fma(-a.y, b.x, c.y);
+    return c;
+}
+// 1 / b by Smith's scaling (robust for wide exponent ranges)
+__host__ __device__ __forceinline__ cd crcp(cd b) {
+    if (fabs(b.x) >= fabs(b.y)) {
+        double r = b.y / b.x, d = b.x + b.y * r;
+        return cmk(1.0 / d, -r / d);
+    } else {
+        double r = b.x / b.y, d = b.y + b.x * r;
+        return cmk(r / d, -1.0 / d);
+    }
+}
+__host__ __device__ __forceinline__ cd cdiv(cd a, cd b) { return cmul(a, crcp(b)); }
+__host__ __device__ __forceinline__ double cabs1(cd a) { return fabs(a.x) + fabs(a.y); }
+
+// exp(i k d) for complex k and real d
+__device__ __forceinline__ cd cexpi(cd k, double d) {
+    double s, c;
+    sincos(k.x * d, &s, &c);
+    double m = exp(-k.y * d);
+    return cmk(m * c, m * s);
+}
+
+}  // namespace mnpb

@@ -1,0 +1,105 @@
+// Error state, launch accounting and the host-side near-pair classification.
+#include "common.cuh"
+
+#include <cmath>
+#include <vector>
+
+namespace mnpb {
+
+static thread_local std::string t_err;
+std::atomic<int64_t> g_launches{0};
+
+void set_error(const char *fmt, ...) {
+    char buf[1024];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    t_err = buf;
+}
+
+void clear_error() { t_err.clear(); }
+
+int check_launch(const char *what) {
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        set_error("%s: %s", what, cudaGetErrorString(e));
+        return MNPB_ECUDA;
+    }
+    return MNPB_OK;
+}
+
+}  // namespace mnpb
+
+using namespace mnpb;
+
+extern "C" int mnpb_version(void) { return 1 * 10000 + 0 * 100 + 0; }
+
+extern "C" const char *mnpb_last_error(void) { return t_err.c_str(); }
+
+extern "C" int64_t mnpb_launch_count(void) { return g_launches.load(); }
+
+// ---------------------------------------------------------------------------
+// Near/self classification (mnpbem/greenfun/refine_utils.py:12-158).
+//
+// d = sqrt(|p1|^2 + |p2|^2 - 2 p1.p2) with d^2 < 1e-10 -> 0; kind 2 where
+// d == 0, kind 1 where (d - rad2_j < abs_cutoff) or ((d - rad2_j)/rad1_i <
+// rel_cutoff).  The norms are summed x, y, z in order; the cross term is the
+// 3-term dot product summed in the same order.  This file is compiled without
+// floating-point contraction so no fused multiply-add changes the rounding.
+// ---------------------------------------------------------------------------
+extern "C" int mnpb_refinematrix(int64_t n1, int64_t n2, const double *pos1, const double *pos2,
+                                 const double *rad1, const double *rad2, double abs_cutoff,
+                                 double rel_cutoff, int64_t cap, int64_t *nnz, int64_t *row_ptr,
+                                 int32_t *cols, int8_t *kinds) {
+    clear_error();
+    MNPB_REQUIRE(n1 >= 0 && n2 >= 0, "refinematrix: negative size");
+    MNPB_REQUIRE(pos1 && pos2 && rad1 && rad2 && nnz && row_ptr, "refinematrix: null pointer");
+    std::vector<double> sq2(n2);
+    for (int64_t j = 0; j < n2; ++j) {
+        const double *q = pos2 + 3 * j;
+        double s = q[0] * q[0];
+        s = s + q[1] * q[1];
+        s = s + q[2] * q[2];
+        sq2[j] = s;
+    }
+    int64_t count = 0;
+    row_ptr[0] = 0;
+    for (int64_t i = 0; i < n1; ++i) {
+        const double *p = pos1 + 3 * i;
+        double s1 = p[0] * p[0];
+        s1 = s1 + p[1] * p[1];
+        s1 = s1 + p[2] * p[2];
+        for (int64_t j = 0; j < n2; ++j) {
+            const double *q = pos2 + 3 * j;
+            double dot = p[0] * q[0];
+            dot = dot + p[1] * q[1];
+            dot = dot + p[2] * q[2];
+            double d2 = (s1 + sq2[j]) - 2.0 * dot;
+            if (d2 < 1e-10) d2 = 0.0;
+            double d = std::sqrt(d2);
+            int8_t kind = 0;
+            if (d == 0.0) {
+                kind = 2;
+            } else {
+                double dd = d - rad2[j];
+                double idr = dd / rad1[i];
+                if (dd < abs_cutoff || idr < rel_cutoff) kind = 1;
+            }
+            if (kind) {
+                if (count < cap && cols && kinds) {
+                    cols[count] = (int32_t)j;
+                    kinds[count] = kind;
+                }
+                ++count;
+            }
+        }
+        row_ptr[i + 1] = count;
+    }
+    *nnz = count;
+    if (count > cap) {
+        set_error("refinematrix: %lld pairs exceed capacity %lld", (long long)count, (long long)cap);
+        return MNPB_ENOMEM;
+    }
+    return MNPB_OK;
+}

@@ -368,6 +368,8 @@ class Particle(object):
         row = np.repeat(np.asarray(ind3), m)
         return pos, weight, row
 
+    quad_integration = quad
+
     def quadpol(self, ind=None):
         """Polar self-term quadrature: (pos (P,3), w (P,), row (P,)).
 
@@ -553,6 +555,8 @@ class ComParticle(object):
 
     def quad(self, ind=None):
         return self.pc.quad(ind)
+
+    quad_integration = quad
 
     def quadpol(self, ind=None):
         return self.pc.quadpol(ind)

@@ -1,0 +1,323 @@
+"""Green functions of a particle surface on the GPU.
+
+``SurfaceTables`` holds everything the assembly kernels need for one
+particle surface, resident in HBM: face data (pos, nvec, tvec1/2, area),
+the near/self pair list (CSR, from the host classifier) and the refined
+Taylor coefficients of the retarded Green function (computed on the GPU in
+FP64 from the face and polar quadrature points), closure-corrected.
+
+``CompGreenRet`` / ``CompGreenStat`` mirror the reference classes
+(mnpbem/greenfun/compgreen_ret.py:14, compgreen_stat.py:12): construction
+builds the tables, ``eval(i, j, key, enei)`` returns the (n, n) matrix of a
+region pair on the host, ``CompGreenStat.F`` the refined quasistatic F.
+
+Particles may be this package's ``ComParticle`` or any object with the same
+attributes (the reference's ``ComParticle`` included).
+"""
+
+import ctypes as C
+
+import numpy as np
+import torch
+
+from . import _lib
+from ._lib import call, ptr
+from .materials import eps_k
+
+__all__ = ["SurfaceTables", "CompGreenRet", "CompGreenStat", "region_tables"]
+
+TWO_PI = 2.0 * np.pi
+
+
+def _nfaces(p):
+    for a in ('nfaces', 'n'):
+        v = getattr(p, a, None)
+        if v is not None and not callable(v):
+            return int(v)
+    return int(np.asarray(p.pos).shape[0])
+
+
+def _face(p, name):
+    v = getattr(p, name, None)
+    if v is None and hasattr(p, 'pc'):
+        v = getattr(p.pc, name)
+    return np.ascontiguousarray(np.asarray(v, dtype=np.float64))
+
+
+def _points(p, which):
+    """Quadrature points of all faces sorted by face: pos (P,3), w (P,), off (n+1)."""
+    n = _nfaces(p)
+    ind = np.arange(n)
+    if which == 'quad':
+        fn = getattr(p, 'quad_integration', None)
+        out = fn(ind) if fn is not None else p.quad(ind)
+        pos, w = out[0], out[1]
+        if hasattr(w, 'tocoo'):
+            coo = w.tocoo()
+            row = np.empty(coo.shape[1], dtype=np.int64)
+            ww = np.empty(coo.shape[1])
+            row[coo.col] = coo.row
+            ww[coo.col] = coo.data
+            w = ww
+        else:
+            row = np.asarray(out[2])
+    else:
+        pos, w, row = p.quadpol(ind)
+    row = np.asarray(row, dtype=np.int64)
+    order = np.argsort(row, kind='stable')
+    counts = np.bincount(row, minlength=n)
+    off = np.concatenate([[0], np.cumsum(counts)]).astype(np.int64)
+    return (np.ascontiguousarray(np.asarray(pos, dtype=np.float64)[order]),
+            np.ascontiguousarray(np.asarray(w, dtype=np.float64)[order]), off)
+
+
+def refinematrix_csr(pos1, pos2, rad1, rad2, abs_cutoff=0.0, rel_cutoff=3.0):
+    """Near/self pair list as CSR (row_ptr, cols, kinds) via the C classifier."""
+    L = _lib.lib()
+    pos1 = np.ascontiguousarray(pos1, dtype=np.float64)
+    pos2 = np.ascontiguousarray(pos2, dtype=np.float64)
+    rad1 = np.ascontiguousarray(rad1, dtype=np.float64)
+    rad2 = np.ascontiguousarray(rad2, dtype=np.float64)
+    n1, n2 = pos1.shape[0], pos2.shape[0]
+    row_ptr = np.zeros(n1 + 1, dtype=np.int64)
+    nnz = C.c_int64(0)
+    rc = L.mnpb_refinematrix(n1, n2, ptr(pos1), ptr(pos2), ptr(rad1), ptr(rad2), abs_cutoff,
+                             rel_cutoff, 0, C.byref(nnz), ptr(row_ptr), None, None)
+    if rc not in (0, 6):
+        raise _lib.MNPBError('mnpb_refinematrix', rc, L.mnpb_last_error().decode())
+    cap = int(nnz.value)
+    cols = np.zeros(max(cap, 1), dtype=np.int32)
+    kinds = np.zeros(max(cap, 1), dtype=np.int8)
+    call('mnpb_refinematrix', n1, n2, ptr(pos1), ptr(pos2), ptr(rad1), ptr(rad2), abs_cutoff,
+         rel_cutoff, cap, C.byref(nnz), ptr(row_ptr), ptr(cols), ptr(kinds))
+    return row_ptr, cols[:cap], kinds[:cap]
+
+
+def closed_ranges(p):
+    """Per face: [lo, hi) face range of its closed surface and the normal sign.
+
+    Each particle is its own closed surface unless ``p.closed`` says
+    otherwise (the reference's default, compgreen_ret.py:224-229).  Only
+    closed surfaces made of consecutive particles of ``p`` are supported.
+    """
+    n = _nfaces(p)
+    parts = list(getattr(p, 'p', [p]))
+    off = np.cumsum([0] + [_nfaces(q) for q in parts]).astype(np.int64)
+    closed = list(getattr(p, 'closed', [None] * len(parts)) or [None] * len(parts))
+    if all(c is None for c in closed):
+        closed = [[k + 1] for k in range(len(parts))]
+    lo = np.zeros(n, dtype=np.int64)
+    hi = np.zeros(n, dtype=np.int64)
+    sign = np.zeros(n)
+    for i, c in enumerate(closed):
+        if c is None:
+            continue
+        c = [int(v) for v in np.atleast_1d(c)]
+        if any(v <= 0 for v in c) or sorted(c) != list(range(min(c), max(c) + 1)):
+            raise NotImplementedError("closed surfaces must be runs of this object's particles")
+        a, b = off[min(c) - 1], off[max(c)]
+        lo[off[i]:off[i + 1]] = a
+        hi[off[i]:off[i + 1]] = b
+        sign[off[i]:off[i + 1]] = 1.0
+    return lo, hi, sign, off
+
+
+class SurfaceTables(object):
+    """Device-resident face data and refined coefficients for one surface."""
+
+    def __init__(self, p, rel_cutoff=3.0, abs_cutoff=0.0, device=None):
+        self.device = torch.device(device) if device is not None else torch.device('cuda')
+        dev = self.device
+        self.p = p
+        n = _nfaces(p)
+        self.n = n
+        pos, nvec = _face(p, 'pos'), _face(p, 'nvec')
+        tv1, tv2 = _face(p, 'tvec1'), _face(p, 'tvec2')
+        area = np.ascontiguousarray(np.asarray(p.area, dtype=np.float64))
+        rad = np.ascontiguousarray(np.asarray(p.bradius(), dtype=np.float64))
+        self.h_pos, self.h_nvec, self.h_area = pos, nvec, area
+        rptr, cols, kinds = refinematrix_csr(pos, pos, rad, rad, abs_cutoff, rel_cutoff)
+        rows = np.repeat(np.arange(n, dtype=np.int32), np.diff(rptr)).astype(np.int32)
+        self.h_rptr, self.h_rows, self.h_cols, self.h_kinds = rptr, rows, cols, kinds
+        self.nref = len(cols)
+        qpos, qw, qoff = _points(p, 'quad')
+        ppos, pw, poff = _points(p, 'quadpol')
+
+        T = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+        self.pos, self.nvec, self.tvec1, self.tvec2, self.area = map(T, (pos, nvec, tv1, tv2, area))
+        self.rows, self.cols, self.kinds = T(rows), T(cols), T(kinds)
+        self.rptr = T(rptr)
+        d_qpos, d_qw, d_qoff, d_ppos, d_pw, d_poff = map(T, (qpos, qw, qoff, ppos, pw, poff))
+        nref = self.nref
+        f64 = dict(dtype=torch.float64, device=dev)
+        self.g = torch.zeros((max(nref, 1), 6), **f64)
+        self.f = torch.zeros((max(nref, 1), 3, 6), **f64)
+        self.gstat = torch.zeros(max(nref, 1), **f64)
+        self.fstat = torch.zeros(max(nref, 1), **f64)
+        self.fn = torch.zeros((max(nref, 1), 6), **f64)
+        sh = _lib.stream_handle()
+        call('mnpb_refine_coefficients', sh, n, ptr(self.pos), ptr(self.nvec), ptr(self.tvec1),
+             ptr(self.tvec2), nref, ptr(self.rows), ptr(self.cols), ptr(self.kinds), ptr(d_qpos),
+             ptr(d_qw), ptr(d_qoff), ptr(d_ppos), ptr(d_pw), ptr(d_poff), ptr(self.g),
+             ptr(self.f), ptr(self.gstat), ptr(self.fstat))
+        # closed-surface correction: sums of the refined static F per column
+        lo, hi, sign, self.part_off = closed_ranges(p)
+        order = np.lexsort((rows, cols))
+        cptr = np.concatenate([[0], np.cumsum(np.bincount(cols, minlength=n))]).astype(np.int64)
+        d_order = torch.from_numpy(order).to(dev)
+        crows = self.rows[d_order].contiguous()
+        cfstat = self.fstat[d_order].contiguous()
+        fsum = torch.zeros(n, **f64)
+        call('mnpb_closure_sums', sh, n, ptr(self.pos), ptr(self.nvec), ptr(self.area),
+             ptr(T(lo)), ptr(T(hi)), ptr(T(cptr)), ptr(crows), ptr(cfstat), ptr(fsum))
+        self.fsum = fsum
+        self.cdir = T(np.where(hi > lo, sign, 0.0))
+        self.f_raw = self.f.clone()
+        call('mnpb_refine_finalize', sh, n, nref, ptr(self.rows), ptr(self.cols), ptr(self.nvec),
+             ptr(self.cdir), ptr(self.fsum), ptr(self.f), ptr(self.fn))
+        self.parts = list(getattr(p, 'p', [p]))
+        self.nparts = len(self.parts)
+        self.inout = np.atleast_2d(np.asarray(getattr(p, 'inout', [[2, 1]]), dtype=int))
+        self.eps_funcs = list(p.eps)
+
+    # ---- per-wavelength tables --------------------------------------------
+    def k_tables(self, eneis, sides=('G1', 'G2')):
+        """Wavenumber/sign tables per particle block for a batch of wavelengths.
+
+        Side 1 is G1 = G11 - G21 (region pairs (in,in) and (out,in)), side 2
+        is G2 = G22 - G12 (compgreen_ret.py:435-505 connectivity, bem_ret.py:
+        407-423).  Returns host arrays kblk (B,2,np,np,2), sblk (B,2,np,np).
+        """
+        npart = self.nparts
+        io = self.inout
+        B = len(eneis)
+        kblk = np.zeros((B, 2, npart, npart, 2))
+        sblk = np.zeros((B, 2, npart, npart))
+        for b, enei in enumerate(eneis):
+            ks = [eps_k(e, enei)[1] for e in self.eps_funcs]
+            for p1 in range(npart):
+                for p2 in range(npart):
+                    # side 1: (in,in) direct, (out,in) subtracted
+                    if io[p1, 0] == io[p2, 0]:
+                        k, s = ks[io[p1, 0] - 1], 1.0
+                    elif io[p1, 1] == io[p2, 0]:
+                        k, s = ks[io[p1, 1] - 1], -1.0
+                    else:
+                        k, s = 0j, 0.0
+                    kblk[b, 0, p1, p2] = (k.real, k.imag)
+                    sblk[b, 0, p1, p2] = s
+                    # side 2: (out,out) direct, (in,out) subtracted
+                    if io[p1, 1] == io[p2, 1]:
+                        k, s = ks[io[p1, 1] - 1], 1.0
+                    elif io[p1, 0] == io[p2, 1]:
+                        k, s = ks[io[p1, 0] - 1], -1.0
+                    else:
+                        k, s = 0j, 0.0
+                    kblk[b, 1, p1, p2] = (k.real, k.imag)
+                    sblk[b, 1, p1, p2] = s
+        return kblk, sblk
+
+    def assemble(self, kblk, sblk, out, mode=0, stream=None):
+        """Launch the assembly into ``out`` = (G1, H1, G2, H2) device buffers."""
+        B = kblk.shape[0]
+        n = self.n
+        d_k = torch.from_numpy(np.ascontiguousarray(kblk)).to(self.device)
+        d_s = torch.from_numpy(np.ascontiguousarray(sblk)).to(self.device)
+        poff = np.ascontiguousarray(self.part_off, dtype=np.int64)
+        G1, H1, G2, H2 = out
+        if mode == 0:
+            ld, stride, plane = n, n * n, 0
+        else:
+            ld, stride, plane = n, 2 * n * n, n * n
+        call('mnpb_assemble_ret', _lib.stream_handle(stream), n, B, ptr(self.pos),
+             ptr(self.nvec), ptr(self.area), self.nparts, ptr(poff), ptr(d_k), ptr(d_s),
+             self.nref, ptr(self.rows), ptr(self.cols), ptr(self.g), ptr(self.fn), mode,
+             ptr(G1), ptr(H1), ptr(G2), ptr(H2), ld, stride, plane)
+        return d_k, d_s
+
+
+def region_tables(tables, i, j, enei):
+    """k/sign tables selecting region pair (i, j) on side 1 (compgreen_ret.py:739-858)."""
+    npart = tables.nparts
+    io = tables.inout
+    ks = [eps_k(e, enei)[1] for e in tables.eps_funcs]
+    kblk = np.zeros((1, 2, npart, npart, 2))
+    sblk = np.zeros((1, 2, npart, npart))
+    for p1 in range(npart):
+        for p2 in range(npart):
+            if io[p1, i] == io[p2, j]:
+                k = ks[io[p1, i] - 1]
+                for s in (0, 1):
+                    kblk[0, s, p1, p2] = (k.real, k.imag)
+                    sblk[0, s, p1, p2] = 1.0
+    return kblk, sblk
+
+
+class CompGreenRet(object):
+    """Retarded Green function of a particle with itself (refined, closed).
+
+    ``eval(i, j, key, enei)`` -> (n, n) complex host matrix for region pair
+    (i, j) (0 inside, 1 outside), key in G, F, H1, H2; 0 if no block
+    connects (compgreen_ret.py:507-553, 739-858).
+    """
+
+    def __init__(self, p1, p2=None, **options):
+        if p2 is not None and p2 is not p1:
+            raise NotImplementedError("CompGreenRet: only p1 is p2 (the BEM matrices) is supported")
+        self.p1 = self.p2 = p1
+        self.deriv = options.get('deriv', 'cart')
+        if self.deriv != 'cart':
+            raise NotImplementedError("CompGreenRet: deriv='cart' (the default) only")
+        if options.get('order', 5) != 5 or not options.get('refine', True):
+            raise NotImplementedError("CompGreenRet: refinement order 5 only")
+        self.tables = SurfaceTables(p1, rel_cutoff=options.get('RelCutoff', 3),
+                                    abs_cutoff=options.get('AbsCutoff', 0))
+        io = self.tables.inout
+        self.con = [[np.where(io[:, a][:, None] == io[:, b][None, :], io[:, a][:, None], 0)
+                     for b in range(2)] for a in range(2)]
+
+    def eval(self, i, j, key, enei, ind=None):
+        if ind is not None:
+            raise NotImplementedError("CompGreenRet.eval: selected elements")
+        if key not in ('G', 'F', 'H1', 'H2'):
+            raise NotImplementedError("CompGreenRet.eval: key {}".format(key))
+        if not np.any(self.con[i][j]):
+            return 0
+        t = self.tables
+        n = t.n
+        kblk, sblk = region_tables(t, i, j, enei)
+        bufs = [torch.empty((1, n, n), dtype=torch.complex128, device=t.device) for _ in range(4)]
+        t.assemble(kblk, sblk, bufs, mode=0)
+        torch.cuda.synchronize()
+        G1, H1, G2, H2 = [b[0].cpu().numpy().T for b in bufs]
+        if key == 'G':
+            return np.ascontiguousarray(G1)
+        if key == 'H1':
+            return np.ascontiguousarray(H1)
+        if key == 'H2':
+            return np.ascontiguousarray(H2)
+        F = H1.copy()
+        F[np.diag_indices(n)] -= TWO_PI
+        return F
+
+
+class CompGreenStat(object):
+    """Quasistatic Green function of a particle with itself: ``F`` (refined,
+    closed-surface corrected), mnpbem/greenfun/compgreen_stat.py:219-294, 466-528."""
+
+    def __init__(self, p1, p2=None, **options):
+        if p2 is not None and p2 is not p1:
+            raise NotImplementedError("CompGreenStat: only p1 is p2 is supported")
+        self.p1 = self.p2 = p1
+        self.tables = SurfaceTables(p1, rel_cutoff=options.get('RelCutoff', 3),
+                                    abs_cutoff=options.get('AbsCutoff', 0))
+        t = self.tables
+        n = t.n
+        self.F_dev = torch.empty((n, n), dtype=torch.float64, device=t.device)
+        call('mnpb_static_matrix', _lib.stream_handle(), n, ptr(t.pos), ptr(t.nvec), ptr(t.area),
+             ptr(t.rptr), ptr(t.cols), ptr(t.fstat), ptr(t.cdir), ptr(t.fsum), ptr(self.F_dev), n)
+
+    @property
+    def F(self):
+        torch.cuda.synchronize()
+        return np.ascontiguousarray(self.F_dev.cpu().numpy().T)
