@@ -1,0 +1,331 @@
+#!/usr/bin/env python
+"""Spectrum-sweep benchmark of the retarded BEM solve on B200.
+
+Workload (one "step"): the full 81-wavelength spectrum 400-800 nm of a gold
+Drude sphere, trisphere(1444 vertices, 40 nm) = 2884 curved faces, in vacuum,
+plane wave pol x / dir z: retarded Green-function assembly, the dense
+Sigma/Delta factorisation, the solve and the extinction of every wavelength.
+Metric: wavelength-solves per second.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--path fp64|mixed]
+    python bench.py --impl reference ...   # CPU oracle of the same workload
+
+Multi-GPU: one process per GPU (torchrun); each rank sweeps its own spectrum
+(weak scaling, replicas -- the wavelengths are independent, no collective on
+the data path); the time is the max over ranks.
+
+The timed region starts with the geometry tables resident in HBM; every
+wavelength's matrices (4 x 133 MB per wavelength) exceed L2 many times over,
+so no L2 flush is needed between steps.
+"""
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "λ-solves/s on 1 B200: mixed+learned vs plain FP64 GPU at ext err ≤1e-6"
+UNIT = "lambda-solves/s"
+WORKLOAD = ("BEMRet dense spectrum sweep: trisphere(1444, 40 nm) = 2884 curved faces, Drude Au "
+            "(eps0=10, wp=9.065 eV, gamma=0.0708 eV) in vacuum, plane wave pol x dir z, "
+            "81 wavelengths linspace(400, 800) nm, extinction per wavelength")
+DRUDE = (10.0, 9.065, 0.0708)
+NLAM = 81
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument('--gpus', type=int, default=1)
+    ap.add_argument('--steps', type=int, default=3)
+    ap.add_argument('--warmup', type=int, default=3)
+    ap.add_argument('--impl', default='ours', choices=['ours', 'reference'])
+    ap.add_argument('--path', default='fp64', choices=['fp64', 'mixed'])
+    ap.add_argument('--batch', type=int, default=27)
+    ap.add_argument('--nlam', type=int, default=81)
+    ap.add_argument('--no-cpu-baseline', action='store_true')
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------------------
+# clocks sampled during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler(object):
+    Q = ('index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,'
+         'clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,'
+         'clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap')
+
+    def __init__(self, index):
+        self.index = index
+        self.rows = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ['nvidia-smi', '-i', str(self.index), '--query-gpu=' + self.Q,
+                 '--format=csv,noheader,nounits', '-lms', '200'],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(',')])
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.thread.join(timeout=2)
+        sm, mx, reasons = [], None, set()
+        names = ['hw_slowdown', 'hw_thermal_slowdown', 'sw_thermal_slowdown', 'sw_power_cap']
+        for r in self.rows:
+            try:
+                sm.append(float(r[1]))
+                mx = float(r[2])
+            except (ValueError, IndexError):
+                continue
+            for nm, v in zip(names, r[5:9]):
+                if v.strip().lower() == 'active':
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, 'MEASURED_PEAKS.json')
+    if os.path.exists(path):
+        with open(path) as f:
+            return json.load(f), 'measured'
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}, 'fallback'
+
+
+# ---------------------------------------------------------------------------
+# CPU oracle (reference arm and cpu_baseline)
+# ---------------------------------------------------------------------------
+def cpu_oracle_sample(nlam_sample, warm=0, steps=1):
+    """Oracle restatement of the same workload timed on the host cores."""
+    from threadpoolctl import threadpool_limits
+    from mnpbem_b200.geometry import Particle, ComParticle, load_mesh
+    from oracle import bem_oracle as O
+    cores = os.cpu_count() or 1
+    drude = lambda e: O.eps_drude(*DRUDE, e)
+    vac = lambda e: O.eps_const(1.0, e)
+    v, f = load_mesh('trisphere_1444_40')
+    s = Particle(v, f, interp='curv')
+    cp = ComParticle([vac, drude], [s], [[2, 1]])
+    eneis = np.linspace(400, 800, NLAM)
+    pol = np.array([[1.0, 0, 0]])
+    dirs = np.array([[0, 0, 1.0]])
+    with threadpool_limits(limits=cores):
+        t0 = time.time()
+        b = O.BEMRetOracle(O.RetGreen(cp), [vac, drude], (2, 1))
+        ctor = time.time() - t0
+        times = []
+        idx = 0
+        for it in range(warm + steps):
+            t0 = time.time()
+            for _ in range(nlam_sample):
+                lam = eneis[(idx * 7) % NLAM]
+                idx += 1
+                b.init(lam)
+                pot = O.planewave_ret_potential(s, cp.inout_faces, 1, 1.0 + 0j, lam, pol, dirs)
+                sol = b.solve_vars(*b.excitation(*pot))
+                O.extinction(s, cp.inout_faces, 1, vac(lam)[1], lam, sol, pol, dirs)
+            if it >= warm:
+                times.append(time.time() - t0)
+    return nlam_sample / np.mean(times), cores, ctor, times
+
+
+def run_reference(args, rank):
+    if rank != 0:
+        return
+    value, cores, ctor, times = cpu_oracle_sample(1, warm=args.warmup, steps=args.steps)
+    out = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1000.0 * float(np.mean(times)), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "sample": "1 wavelength per step"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+                         "sample": "1 of the 81 wavelengths per step (numpy/scipy oracle "
+                                   "restatement of the reference, LAPACK LU)"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(out))
+
+
+# ---------------------------------------------------------------------------
+# GPU arm
+# ---------------------------------------------------------------------------
+def main():
+    args = parse()
+    rank = int(os.environ.get('RANK', '0'))
+    world = int(os.environ.get('WORLD_SIZE', '1'))
+    local = int(os.environ.get('LOCAL_RANK', '0'))
+    if args.impl == 'reference':
+        run_reference(args, rank)
+        return
+
+    import torch
+    import torch.distributed as dist
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group('nccl', timeout=timedelta(seconds=600),
+                                device_id=torch.device('cuda', local))
+    import mnpbem_b200 as M
+    from mnpbem_b200 import _lib, bem, excitation
+
+    v, f = M.load_mesh('trisphere_1444_40')
+    s = M.Particle(v, f, interp='curv')
+    cp = M.ComParticle([M.EpsConst(1.0), M.EpsDrude(*DRUDE)], [s], [[2, 1]])
+    solver = bem.BEMRet(cp)
+    exc = excitation.PlaneWaveRet(pol=[[1.0, 0, 0]], dir=[[0, 0, 1.0]])
+    global NLAM
+    NLAM = args.nlam
+    eneis = list(np.linspace(400, 800, NLAM))
+    n = solver.tables.n
+    B = args.batch
+
+    def device_step():
+        """One spectrum sweep with every array resident on the GPU."""
+        exts = []
+        for s0 in range(0, NLAM, B):
+            chunk = eneis[s0:s0 + B]
+            bt = solver._factor(chunk)
+            pots, K = exc.potential_device(cp, solver.tables, chunk)
+            xout = solver._solve_batch(bt, pots, K)
+            e, _ = exc.farfield_device(cp, solver.tables, xout, chunk, exc.dir)
+            exts.append(e)
+            del bt
+        return exts
+
+    torch.cuda.synchronize()
+    for _ in range(args.warmup):
+        device_step()
+    torch.cuda.synchronize()
+
+    clocks = ClockSampler(local)
+    clocks.start()
+    launches0 = _lib.launch_count()
+    _lib.prof_begin()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record()
+    for _ in range(args.steps):
+        device_step()
+    ev1.record()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    prof = _lib.prof_end()
+    launches = _lib.launch_count() - launches0
+    ck = clocks.stop()
+    ms = ev0.elapsed_time(ev1)
+    if world > 1:
+        t = torch.tensor([ms], device='cuda')
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = world * NLAM * args.steps / (ms / 1000.0)
+
+    # end to end through the public API with host buffers
+    torch.cuda.synchronize()
+    t0 = time.time()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        sols = solver.solve_spectrum(exc, eneis, batch=B)
+    e1.record()
+    torch.cuda.synchronize()
+    e2e_ms = e0.elapsed_time(e1)
+    if world > 1:
+        t = torch.tensor([e2e_ms], device='cuda')
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e_value = world * NLAM * args.steps / (e2e_ms / 1000.0)
+    K = 1
+    h2d = NLAM * (4 * 8 + 8 + 2 * 2 * 16 + 16 * 8)     # eps/k tables, block k tables, pol/dir
+    d2h = NLAM * 8 * K * n * 16                        # sig1, h1, sig2, h2 per wavelength
+
+    peaks, peak_kind = measured_peaks()
+    # dominant kernel by device time
+    dom = max(prof.items(), key=lambda kv: kv[1][0]) if prof else None
+    roof = None
+    if dom is not None:
+        name, (dms, work, cnt) = dom
+        tot_ms = sum(v[0] for v in prof.values())
+        if name in ('zgemm_f64',):
+            achieved = work / (dms / 1000.0) / 1e12
+            peak = 37.0
+            roof = {"kernel": name, "bound": "fp64", "achieved": achieved, "peak": peak,
+                    "unit": "TFLOP/s", "frac": achieved / peak, "traffic": None,
+                    "peak_source": "nominal B200 FP64 (no measured FP64 peak in "
+                                   "MEASURED_PEAKS.json)",
+                    "launches": cnt, "share": dms / tot_ms}
+        elif name in ('tc_gemm',):
+            achieved = work / (dms / 1000.0) / 1e12
+            peak = peaks['bf16_tflops_sustained']
+            roof = {"kernel": name, "bound": "tensor", "achieved": achieved, "peak": peak,
+                    "unit": "TFLOP/s", "frac": achieved / peak, "traffic": None,
+                    "peak_source": peak_kind + " bf16 sustained", "launches": cnt,
+                    "share": dms / tot_ms}
+        else:
+            achieved = work / (dms / 1000.0) / 1e9
+            peak = peaks['hbm_gbs']
+            roof = {"kernel": name, "bound": "hbm", "achieved": achieved, "peak": peak,
+                    "unit": "GB/s", "frac": achieved / peak, "traffic": None,
+                    "peak_source": peak_kind, "launches": cnt, "share": dms / tot_ms}
+        roof["by_class_ms"] = {k: round(v[0] / args.steps, 3) for k, v in prof.items()}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cv, cores, ctor, times = cpu_oracle_sample(2)
+        cpu = {"value": cv, "unit": UNIT, "cores": cores, "kind": "port",
+               "sample": "2 of the 81 wavelengths (numpy/scipy oracle restatement of the "
+                         "reference, LAPACK LU, %d BLAS threads); constructor %.1f s "
+                         "excluded" % (cores, ctor)}
+
+    if rank == 0:
+        out = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64" if args.path == 'fp64' else "tf32/bf16x3+f64-refine",
+            "data": "synthetic",
+            "config": {"workload": WORKLOAD, "path": args.path, "batch_wavelengths": B,
+                       "n_faces": n, "wavelengths": NLAM,
+                       "l2": "inputs larger than L2 (4 x 133 MB per wavelength)",
+                       "parallelism": "replicas over wavelengths" if world > 1 else "1 GPU"},
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h},
+            "gpu_launches": launches,
+            "roofline": roof,
+            "cpu_baseline": cpu,
+            "clocks": ck,
+        }
+        print(json.dumps(out))
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == '__main__':
+    main()

@@ -47,6 +47,17 @@ const char *mnpb_last_error(void);
  * counter; used to report how many of the library's kernels ran). */
 int64_t mnpb_launch_count(void);
 
+/* Device-time profiling of the library's own launches: between
+ * mnpb_prof_begin() and mnpb_prof_end() every launch of a profiled kernel is
+ * bracketed by CUDA events on its stream.  mnpb_prof_end synchronises and
+ * returns, per kernel class (0 assembly, 1 refinement quadrature, 2 FP64
+ * GEMM, 3 LU panel, 4 small triangular solves, 5 row/column swaps,
+ * 6 element-wise, 7 tensor-core GEMM, 8 far field, 9 FP32 GEMM, 10 matvec),
+ * the summed device time in ms, the summed algorithmic work (flops or bytes,
+ * see the kernel) and the number of launches. */
+int mnpb_prof_begin(void);
+int mnpb_prof_end(int ncls, double *ms, double *work, int64_t *count);
+
 /* ---------------------------------------------------------------------------
  * Geometry set-up (once per particle mesh)
  * ------------------------------------------------------------------------- */

@@ -20,6 +20,8 @@ SIGNATURES = {
     'mnpb_version': [],
     'mnpb_last_error': [],
     'mnpb_launch_count': [],
+    'mnpb_prof_begin': [],
+    'mnpb_prof_end': [_I, _P, _P, _P],
     'mnpb_refinematrix': [_I64, _I64, _P, _P, _P, _P, _D, _D, _I64, _P, _P, _P, _P],
     'mnpb_refine_coefficients': [_P, _I64, _P, _P, _P, _P, _I64, _P, _P, _P, _P, _P, _P, _P,
                                  _P, _P, _P, _P, _P, _P],
@@ -83,6 +85,30 @@ def call(name, *args):
 
 def launch_count():
     return int(lib().mnpb_launch_count())
+
+
+PROF_CLASSES = ['assemble', 'refine', 'zgemm_f64', 'lu_panel', 'trsm_small', 'swap',
+                'elementwise', 'tc_gemm', 'farfield', 'sgemm_f32', 'matvec']
+
+
+def prof_begin():
+    call('mnpb_prof_begin')
+
+
+def prof_end():
+    """{class: (ms, work, launches)} for the launches since prof_begin()."""
+    import numpy as np
+    n = 16
+    ms = np.zeros(n)
+    work = np.zeros(n)
+    cnt = np.zeros(n, dtype=np.int64)
+    call('mnpb_prof_end', n, ptr(ms), ptr(work), ptr(cnt))
+    out = {}
+    for i in range(n):
+        if cnt[i]:
+            name = PROF_CLASSES[i] if i < len(PROF_CLASSES) else 'class%d' % i
+            out[name] = (float(ms[i]), float(work[i]), int(cnt[i]))
+    return out
 
 
 class _Ref(object):

@@ -47,6 +47,39 @@ int check_launch(const char *what);
 
 inline cudaStream_t as_stream(void *s) { return reinterpret_cast<cudaStream_t>(s); }
 
+// ---------------------------------------------------------------------------
+// optional per-kernel-class timing with CUDA events (mnpb_prof_begin/end)
+// ---------------------------------------------------------------------------
+enum ProfClass {
+    PC_ASSEMBLE = 0,   // work = bytes written
+    PC_REFINE = 1,
+    PC_ZGEMM = 2,      // work = real flops
+    PC_PANEL = 3,
+    PC_TRSM = 4,
+    PC_SWAP = 5,
+    PC_ELEM = 6,
+    PC_TCGEMM = 7,     // work = real flops (tensor cores)
+    PC_FARFIELD = 8,
+    PC_SGEMM = 9,
+    PC_MATVEC = 10,    // work = bytes read
+    PC_COUNT = 16
+};
+bool prof_on();
+void prof_record(cudaStream_t s, int cls, double work, bool start);
+
+struct ProfScope {
+    cudaStream_t s;
+    int cls;
+    double work;
+    bool on;
+    ProfScope(cudaStream_t s_, int cls_, double work_) : s(s_), cls(cls_), work(work_), on(prof_on()) {
+        if (on) prof_record(s, cls, work, true);
+    }
+    ~ProfScope() {
+        if (on) prof_record(s, cls, work, false);
+    }
+};
+
 inline int ceil_div(int64_t a, int64_t b) { return (int)((a + b - 1) / b); }
 
 // ---------------------------------------------------------------------------

@@ -289,6 +289,7 @@ int zgemm(cudaStream_t s, int m, int n, int k, int batch, cd alpha, const cd *A,
           int64_t sC) {
     if (m <= 0 || n <= 0 || batch <= 0) return MNPB_OK;
     dim3 grid(ceil_div(m, GBM), ceil_div(n, GBN), batch);
+    ProfScope ps(s, PC_ZGEMM, 8.0 * m * n * (double)(k > 0 ? k : 0) * batch);
     if (k <= 0) {
         // C = beta C
         zgemm_kernel<<<grid, 128, 0, s>>>(m, n, 0, alpha, A, lda, sA, B, ldb, sB, beta, C, ldc, sC);
@@ -303,6 +304,7 @@ static int trsm_small(cudaStream_t s, int mode, int kb, const cd *T, int64_t ldt
                       cd *B, int64_t ldb, int64_t sB, int nvec, int batch) {
     if (nvec <= 0 || kb <= 0) return MNPB_OK;
     dim3 grid(ceil_div(nvec, 128), batch);
+    ProfScope ps(s, PC_TRSM, 4.0 * kb * kb * (double)nvec * batch);
     trsm_small_kernel<<<grid, 128, 0, s>>>(mode, kb, T, ldt, sT, B, ldb, sB, nvec);
     MNPB_LAUNCH_CHECK("trsm_small_kernel");
     return MNPB_OK;
@@ -364,6 +366,7 @@ int laswp(cudaStream_t s, cd *A, int64_t lda, int64_t sA, int ncols, int jskip0,
           const int32_t *ipiv, int64_t sP, int c0, int c1, bool forward, int batch) {
     if (ncols <= 0 || c1 <= c0) return MNPB_OK;
     dim3 grid(ceil_div(ncols, 128), batch);
+    ProfScope ps(s, PC_SWAP, 0.0);
     laswp_kernel<<<grid, 128, 0, s>>>(A, lda, sA, 0, ncols, jskip0, jskip1, ipiv, sP, c0, c1,
                                       forward ? 1 : 0);
     MNPB_LAUNCH_CHECK("laswp_kernel");
@@ -375,8 +378,11 @@ int getrf(cudaStream_t s, int n, int batch, cd *A, int64_t lda, int64_t sA, int3
     const int nb = TS;
     for (int k = 0; k < n; k += nb) {
         const int kb = (n - k < nb) ? (n - k) : nb;
-        panel_kernel<<<batch, PANEL_THREADS, 0, s>>>(n, k, kb, A, lda, sA, ipiv, sP, info);
-        MNPB_LAUNCH_CHECK("panel_kernel");
+        {
+            ProfScope ps(s, PC_PANEL, 8.0 * kb * kb * (double)(n - k) * batch / 2);
+            panel_kernel<<<batch, PANEL_THREADS, 0, s>>>(n, k, kb, A, lda, sA, ipiv, sP, info);
+            MNPB_LAUNCH_CHECK("panel_kernel");
+        }
         MNPB_TRY(laswp(s, A, lda, sA, n, k, k + kb, ipiv, sP, k, k + kb, true, batch));
         const int rest = n - k - kb;
         if (rest > 0) {
@@ -403,6 +409,7 @@ int right_solve(cudaStream_t s, int n, int m, int batch, const cd *LU, int64_t l
     MNPB_TRY(trsm_run(s, n, m, batch, LU, lda, sA, B, ldb, sB));
     MNPB_TRY(trsm_rlu(s, n, m, batch, LU, lda, sA, B, ldb, sB));
     dim3 grid(ceil_div(m, 128), batch);
+    ProfScope ps(s, PC_SWAP, 0.0);
     colswp_kernel<<<grid, 128, 0, s>>>(B, ldb, sB, m, ipiv, sP, n);
     MNPB_LAUNCH_CHECK("colswp_kernel");
     return MNPB_OK;

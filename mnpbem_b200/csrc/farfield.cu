@@ -153,6 +153,7 @@ extern "C" int mnpb_farfield(void *stream, int64_t n, int64_t batch, int64_t npo
                      h_out,
                  "farfield: null pointer");
     dim3 grid((unsigned)ndir, (unsigned)npol, (unsigned)batch);
+    ProfScope ps(as_stream(stream), PC_FARFIELD, 0.0);
     farfield_kernel<<<grid, FF_THREADS, 0, as_stream(stream)>>>(
         (int)n, (int)npol, (int)ndir, pos, area, side_in, side_out, dirs, kmed, k0,
         (const cd *)sol, (cd *)e_out, (cd *)h_out);

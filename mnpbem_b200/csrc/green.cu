@@ -435,6 +435,7 @@ extern "C" int mnpb_refine_coefficients(void *stream, int64_t n, const double *p
     if (nref == 0) return MNPB_OK;
     const int threads = 256;
     const int64_t blocks = (nref * 32 + threads - 1) / threads;
+    ProfScope ps(as_stream(stream), PC_REFINE, 0.0);
     refine_kernel<<<(unsigned)blocks, threads, 0, as_stream(stream)>>>(
         pos, nvec, tvec1, tvec2, nref, rows, cols, kinds, qpos, qw, qoff, ppos, pw, poff, g, f,
         gstat, fstat);
@@ -511,6 +512,8 @@ extern "C" int mnpb_assemble_ret(void *stream, int64_t n, int64_t batch, const d
     cudaStream_t s = as_stream(stream);
     dim3 grid(ceil_div(n, 128), (unsigned)n, (unsigned)batch);
     const int64_t tot = nref * batch;
+    ProfScope ps(s, PC_ASSEMBLE, (out_mode == 0 ? 64.0 : 32.0) * (double)n * n * batch +
+                                     96.0 * (double)nref);
     if (out_mode == 0) {
         StoreC128 st{(cd *)G1, (cd *)H1, (cd *)G2, (cd *)H2, ld, stride};
         assemble_far_kernel<StoreC128><<<grid, 128, 0, s>>>(n, parts, pos, nvec, area, kblk,

@@ -29,9 +29,88 @@ int check_launch(const char *what) {
     return MNPB_OK;
 }
 
+// ---- event profiler ---------------------------------------------------------
+namespace {
+struct Rec {
+    cudaEvent_t a, b;
+    int cls;
+    double work;
+};
+bool g_prof = false;
+std::vector<Rec> g_recs;
+std::vector<cudaEvent_t> g_pool;
+Rec g_open;
+bool g_has_open = false;
+
+cudaEvent_t take_event() {
+    if (!g_pool.empty()) {
+        cudaEvent_t e = g_pool.back();
+        g_pool.pop_back();
+        return e;
+    }
+    cudaEvent_t e;
+    cudaEventCreate(&e);
+    return e;
+}
+}  // namespace
+
+bool prof_on() { return g_prof; }
+
+void prof_record(cudaStream_t s, int cls, double work, bool start) {
+    if (start) {
+        g_open.a = take_event();
+        g_open.cls = cls;
+        g_open.work = work;
+        cudaEventRecord(g_open.a, s);
+        g_has_open = true;
+    } else if (g_has_open) {
+        g_open.b = take_event();
+        cudaEventRecord(g_open.b, s);
+        g_recs.push_back(g_open);
+        g_has_open = false;
+    }
+}
+
 }  // namespace mnpb
 
 using namespace mnpb;
+
+// Start recording CUDA events around the library's launches (host thread
+// that issues the launches; single-threaded use).
+extern "C" int mnpb_prof_begin(void) {
+    g_recs.clear();
+    g_prof = true;
+    return MNPB_OK;
+}
+
+// Stop recording; synchronise and return per class the summed device time
+// (ms), the summed algorithmic work and the launch count.
+extern "C" int mnpb_prof_end(int ncls, double *ms, double *work, int64_t *count) {
+    clear_error();
+    g_prof = false;
+    for (int c = 0; c < ncls; ++c) {
+        ms[c] = 0.0;
+        work[c] = 0.0;
+        count[c] = 0;
+    }
+    for (auto &r : g_recs) {
+        if (cudaEventSynchronize(r.b) != cudaSuccess) {
+            set_error("prof_end: event synchronize failed");
+            return MNPB_ECUDA;
+        }
+        float t = 0.f;
+        cudaEventElapsedTime(&t, r.a, r.b);
+        if (r.cls >= 0 && r.cls < ncls) {
+            ms[r.cls] += t;
+            work[r.cls] += r.work;
+            count[r.cls] += 1;
+        }
+        g_pool.push_back(r.a);
+        g_pool.push_back(r.b);
+    }
+    g_recs.clear();
+    return MNPB_OK;
+}
 
 extern "C" int mnpb_version(void) { return 1 * 10000 + 0 * 100 + 0; }
 
