@@ -47,8 +47,9 @@ def parse():
     ap.add_argument('--steps', type=int, default=3)
     ap.add_argument('--warmup', type=int, default=3)
     ap.add_argument('--impl', default='ours', choices=['ours', 'reference'])
-    ap.add_argument('--path', default='fp64', choices=['fp64', 'mixed'])
-    ap.add_argument('--batch', type=int, default=27)
+    ap.add_argument('--path', default='mixed', choices=['fp64', 'mixed'])
+    ap.add_argument('--no-accuracy', action='store_true')
+    ap.add_argument('--batch', type=int, default=81)
     ap.add_argument('--nlam', type=int, default=81)
     ap.add_argument('--no-cpu-baseline', action='store_true')
     return ap.parse_args()
@@ -196,7 +197,7 @@ def main():
     v, f = M.load_mesh('trisphere_1444_40')
     s = M.Particle(v, f, interp='curv')
     cp = M.ComParticle([M.EpsConst(1.0), M.EpsDrude(*DRUDE)], [s], [[2, 1]])
-    solver = bem.BEMRet(cp)
+    solver = bem.BEMRet(cp, precision=args.path)
     exc = excitation.PlaneWaveRet(pol=[[1.0, 0, 0]], dir=[[0, 0, 1.0]])
     global NLAM
     NLAM = args.nlam
@@ -204,18 +205,28 @@ def main():
     n = solver.tables.n
     B = args.batch
 
-    def device_step():
+    refine_iters = []
+
+    def device_step(slv=None):
         """One spectrum sweep with every array resident on the GPU."""
+        slv = slv or solver
         exts = []
         for s0 in range(0, NLAM, B):
             chunk = eneis[s0:s0 + B]
-            bt = solver._factor(chunk)
-            pots, K = exc.potential_device(cp, solver.tables, chunk)
-            xout = solver._solve_batch(bt, pots, K)
-            e, _ = exc.farfield_device(cp, solver.tables, xout, chunk, exc.dir)
+            bt = slv._factor(chunk)
+            pots, K = exc.potential_device(cp, slv.tables, chunk)
+            xout = slv._solve_batch(bt, pots, K)
+            e, _ = exc.farfield_device(cp, slv.tables, xout, chunk, exc.dir)
             exts.append(e)
+            if getattr(bt, 'iters', None) is not None:
+                refine_iters.extend(int(v) for v in bt.iters)
             del bt
         return exts
+
+    def ext_of(exts):
+        kk = np.array([complex(*exc._wavenumbers(cp, [l])[0][0]) for l in eneis])
+        e = torch.cat(exts).cpu().numpy()          # (NLAM, K=1, ndir=1, 3)
+        return np.real(4 * np.pi / kk * np.imag(np.sum(np.conj(exc.pol[0]) * e[:, 0, 0], axis=1)))
 
     torch.cuda.synchronize()
     for _ in range(args.warmup):
@@ -296,6 +307,26 @@ def main():
                     "peak_source": peak_kind, "launches": cnt, "share": dms / tot_ms}
         roof["by_class_ms"] = {k: round(v[0] / args.steps, 3) for k, v in prof.items()}
 
+    accuracy = None
+    if rank == 0 and not args.no_accuracy:
+        # extinction of this path against the plain FP64 GPU path on the same sweep
+        refine_iters.clear()
+        ext_p = ext_of(device_step())
+        iters = list(refine_iters)
+        ref_solver = solver if args.path == 'fp64' else bem.BEMRet(cp, precision='fp64')
+        torch.cuda.synchronize()
+        t0 = time.time()
+        ext_64 = ext_of(device_step(ref_solver))
+        torch.cuda.synchronize()
+        t64 = time.time() - t0
+        accuracy = {"ext_max_rel_err_vs_fp64": float(np.max(np.abs(ext_p - ext_64) / np.abs(ext_64))),
+                    "fp64_path_lambda_solves_per_s": NLAM / t64,
+                    "fp64_path_sample": "one sweep, wall clock"}
+        if iters:
+            accuracy["refine_corrections_mean"] = float(np.mean(iters))
+            accuracy["refine_corrections_max"] = int(np.max(iters))
+        del ref_solver
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cv, cores, ctor, times = cpu_oracle_sample(2)
@@ -318,6 +349,7 @@ def main():
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
             "gpu_launches": launches,
+            "accuracy": accuracy,
             "roofline": roof,
             "cpu_baseline": cpu,
             "clocks": ck,

@@ -152,9 +152,11 @@ int64_t mnpb_bemret_workspace_f64(int64_t n, int64_t batch);
  * Replaces mnpbem/bem/bem_ret.py:437-523 (init).  eps (device, batch x 2
  * complex): inside / outside dielectric constants (scalar per wavelength);
  * kvac (device, batch) vacuum wavenumbers 2 pi / enei; nvec (device n x 3).
- * piv (device int32, batch x 3 x n) receives the pivots of G1, G2, Sigma.
- * All matrices c128, leading dimension ld, batch stride `stride`.
- * info (device int32, batch) receives the first zero pivot (1-based) or 0. */
+ * piv (device int32, [3][batch][n]) receives the pivots of G1, G2, Sigma.
+ * All matrices c128, leading dimension ld, batch stride `stride`.  When G2
+ * follows G1 (G2 == G1 + batch*stride) and H2 follows H1 the two halves are
+ * factorised together, as one batch of 2 x batch matrices.
+ * info (device int32, [2][batch]) receives the first zero pivot (1-based) or 0. */
 int mnpb_bemret_init_f64(void *stream, int64_t n, int64_t batch, double *G1, double *G2,
                          double *H1, double *H2, double *D, int64_t ld, int64_t stride,
                          const double *eps, const double *kvac, const double *nvec,
@@ -182,6 +184,68 @@ int mnpb_bemret_solve_f64(void *stream, int64_t n, int64_t batch, int64_t nrhs,
                           const double *nvec, const double *x_in, double *x_out,
                           void *work, int64_t work_bytes);
 
+/* As mnpb_assemble_ret, writing in one pass both the c128 matrices (ld,
+ * stride) and planar FP32 copies (ldp, stridep, planep) -- the FP64 operator
+ * for refinement and the FP32 input of the mixed-precision factorisation. */
+int mnpb_assemble_ret2(void *stream, int64_t n, int64_t batch, const double *pos,
+                       const double *nvec, const double *area, int nparts, const int64_t *poff,
+                       const double *kblk, const double *sblk, int64_t nref, const int32_t *rows,
+                       const int32_t *cols, const double *g, const double *fn, double *G1,
+                       double *H1, double *G2, double *H2, int64_t ld, int64_t stride,
+                       float *G1p, float *H1p, float *G2p, float *H2p, int64_t ldp,
+                       int64_t stridep, int64_t planep);
+
+/* ---------------------------------------------------------------------------
+ * Dense retarded solve (BEMRet), mixed precision, batched over wavelengths
+ * ------------------------------------------------------------------------- */
+
+/* Workspace bytes of mnpb_bemret_init_mixed. */
+int64_t mnpb_bemret_workspace_mixed(int64_t n, int64_t batch);
+
+/* The algebra of mnpb_bemret_init_f64 on planar FP32 matrices (leading
+ * dimension ld, a multiple of 4; plane = ld*n; batch stride 2*ld*n) with
+ * every LU, triangular solve and GEMM on TF32 tensor cores: G1 -> LU(G1),
+ * G2 -> LU(G2), H1 -> Sigma1, H2 -> LU(Sigma), D -> Delta^-1.  Replaces
+ * mnpbem/bem/bem_ret.py:437-523 in the mixed-precision solver. */
+int mnpb_bemret_init_mixed(void *stream, int64_t n, int64_t batch, float *G1, float *G2,
+                           float *H1, float *H2, float *D, int64_t ld, const double *eps,
+                           const double *kvac, const double *nvec, int32_t *piv, int32_t *info,
+                           float *dinv, void *work, int64_t work_bytes);
+
+/* Floats of the dinv buffer (inverses of the 32 x 32 diagonal blocks of the
+ * G1, G2 and Sigma factors, written by mnpb_bemret_init_mixed and read by
+ * mnpb_bemret_solve_refine's one-launch triangular solves). */
+int64_t mnpb_bemret_dinv_floats(int64_t n, int64_t batch);
+
+/* Workspace bytes of mnpb_bemret_solve_refine. */
+int64_t mnpb_bemret_refine_workspace(int64_t n, int64_t batch, int64_t nrhs);
+
+/* Solve with the mixed factorisation and refine in FP64 against the exact
+ * operator of mnpbem/bem/bem_ret_iter.py:1362-1501 (c128 G1, G2, H1, H2 with
+ * the same ld): x = M^-1 b, then x += M^-1 (b - A x) until |b - A x| / |b| <
+ * tol or max_iter corrections (MNPB_ENOCONV then).  b: excitation layout
+ * (phi, a, De, alpha), x: solution layout (sig1, h1, sig2, h2), both
+ * [batch][8][nrhs][n] c128, nrhs <= 4.  iters, relres: host arrays (batch). */
+int mnpb_bemret_solve_refine(void *stream, int64_t n, int64_t batch, int64_t nrhs,
+                             const float *G1p, const float *G2p, const float *S1p,
+                             const float *Sp, const float *Dp, int64_t ld, const int32_t *piv,
+                             const float *dinv, const double *G1, const double *G2, const double *H1,
+                             const double *H2, const double *eps, const double *kvac,
+                             const double *nvec, const double *b, double *x, int max_iter,
+                             double tol, int32_t *iters, double *relres, void *work,
+                             int64_t work_bytes);
+
+/* Batched LU / LU solve of planar FP32 matrices with TF32 tensor-core
+ * updates (recursive LU).  work: mnpb_f32_workspace(n, batch) bytes. */
+int64_t mnpb_f32_workspace(int64_t n, int64_t batch);
+int mnpb_getrf_c32p(void *stream, int64_t n, int64_t batch, float *A, int64_t ld, int64_t plane,
+                    int64_t stride, int32_t *piv, int64_t pstride, int32_t *info, void *work,
+                    int64_t work_bytes);
+int mnpb_getrs_c32p(void *stream, int64_t n, int64_t batch, int64_t nrhs, const float *LU,
+                    int64_t ld, int64_t plane, int64_t stride, const int32_t *piv,
+                    int64_t pstride, float *B, int64_t ldb, int64_t planeB, int64_t bstride,
+                    void *work, int64_t work_bytes);
+
 /* ---------------------------------------------------------------------------
  * Dense building blocks (exposed for tests and for the quasistatic solver)
  * ------------------------------------------------------------------------- */
@@ -203,6 +267,23 @@ int mnpb_zgemm(void *stream, int64_t m, int64_t n, int64_t k, int64_t batch,
                double alpha_re, double alpha_im, const double *A, int64_t lda, int64_t sA,
                const double *B, int64_t ldb, int64_t sB, double beta_re, double beta_im,
                double *C, int64_t ldc, int64_t sC);
+
+/* Batched complex GEMM on the tensor cores (tcgen05, TF32 inputs rounded to
+ * nearest, FP32 accumulation): C = beta C + alpha A B for planar complex FP32
+ * column-major matrices (A: m x k, B: k x n).  Base addresses, ld*4 and
+ * plane*4, stride*4 must be multiples of 16 bytes.  work: at least
+ * mnpb_cgemm_tf32_workspace(m, k, batch) bytes of device memory.  Replaces
+ * the complex GEMMs of mnpbem/bem/bem_ret.py:472-495 and the LU trailing
+ * updates of scipy.linalg.lu_factor in the mixed-precision solver. */
+int64_t mnpb_cgemm_tf32_workspace(int64_t m, int64_t k, int64_t batch);
+int mnpb_cgemm_tf32(void *stream, int64_t m, int64_t n, int64_t k, int64_t batch, float alpha,
+                    const float *A, int64_t lda, int64_t planeA, int64_t sA, const float *B,
+                    int64_t ldb, int64_t planeB, int64_t sB, float beta, float *C, int64_t ldc,
+                    int64_t planeC, int64_t sC, void *work, int64_t work_bytes);
+
+/* First bounded-wait timeout recorded by a tensor-core kernel since the last
+ * call (0 = none); reading clears it. */
+int mnpb_tc_error(void *stream, int32_t *code);
 
 /* Quasistatic matrix for a batch of wavelengths: M_b = -(diag(lambda_b) + F)
  * with lambda = 2 pi (eps1+eps2)/(eps1-eps2) per face (eps12: device,

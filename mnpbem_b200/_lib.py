@@ -30,6 +30,19 @@ SIGNATURES = {
     'mnpb_static_matrix': [_P, _I64, _P, _P, _P, _P, _P, _P, _P, _P, _P, _I64],
     'mnpb_assemble_ret': [_P, _I64, _I64, _P, _P, _P, _I, _P, _P, _P, _I64, _P, _P, _P, _P, _I,
                           _P, _P, _P, _P, _I64, _I64, _I64],
+    'mnpb_assemble_ret2': [_P, _I64, _I64, _P, _P, _P, _I, _P, _P, _P, _I64, _P, _P, _P, _P,
+                           _P, _P, _P, _P, _I64, _I64, _P, _P, _P, _P, _I64, _I64, _I64],
+    'mnpb_bemret_workspace_mixed': [_I64, _I64],
+    'mnpb_bemret_init_mixed': [_P, _I64, _I64, _P, _P, _P, _P, _P, _I64, _P, _P, _P, _P, _P, _P,
+                               _P, _I64],
+    'mnpb_bemret_dinv_floats': [_I64, _I64],
+    'mnpb_bemret_refine_workspace': [_I64, _I64, _I64],
+    'mnpb_bemret_solve_refine': [_P, _I64, _I64, _I64, _P, _P, _P, _P, _P, _I64, _P, _P, _P, _P,
+                                 _P, _P, _P, _P, _P, _P, _P, _I, _D, _P, _P, _P, _I64],
+    'mnpb_f32_workspace': [_I64, _I64],
+    'mnpb_getrf_c32p': [_P, _I64, _I64, _P, _I64, _I64, _I64, _P, _I64, _P, _P, _I64],
+    'mnpb_getrs_c32p': [_P, _I64, _I64, _I64, _P, _I64, _I64, _I64, _P, _I64, _P, _I64, _I64,
+                        _I64, _P, _I64],
     'mnpb_bemret_workspace_f64': [_I64, _I64],
     'mnpb_bemret_init_f64': [_P, _I64, _I64, _P, _P, _P, _P, _P, _I64, _I64, _P, _P, _P, _P, _P,
                              _P, _I64],
@@ -40,11 +53,17 @@ SIGNATURES = {
     'mnpb_getrs_f64': [_P, _I64, _I64, _I64, _P, _I64, _I64, _P, _I64, _P, _I64, _I64],
     'mnpb_zgemm': [_P, _I64, _I64, _I64, _I64, _D, _D, _P, _I64, _I64, _P, _I64, _I64, _D, _D,
                    _P, _I64, _I64],
+    'mnpb_cgemm_tf32_workspace': [_I64, _I64, _I64],
+    'mnpb_cgemm_tf32': [_P, _I64, _I64, _I64, _I64, C.c_float, _P, _I64, _I64, _I64, _P, _I64,
+                        _I64, _I64, C.c_float, _P, _I64, _I64, _I64, _P, _I64],
+    'mnpb_tc_error': [_P, _P],
     'mnpb_stat_matrix': [_P, _I64, _I64, _P, _I64, _P, _P, _I64, _I64],
     'mnpb_planewave_potential': [_P, _I64, _I64, _I64, _P, _P, _P, _P, _P, _P, _P, _P, _P],
     'mnpb_farfield': [_P, _I64, _I64, _I64, _I64, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P],
 }
 _RESTYPE = {'mnpb_last_error': C.c_char_p, 'mnpb_launch_count': C.c_int64,
+            'mnpb_cgemm_tf32_workspace': C.c_int64, 'mnpb_bemret_workspace_mixed': C.c_int64,
+            'mnpb_bemret_refine_workspace': C.c_int64, 'mnpb_f32_workspace': C.c_int64, 'mnpb_bemret_dinv_floats': C.c_int64,
             'mnpb_bemret_workspace_f64': C.c_int64}
 
 _lib = None

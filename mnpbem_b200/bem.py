@@ -46,24 +46,71 @@ def _scalar_eps(p, enei):
 class _RetBatch(object):
     """Device buffers of one factorised batch of wavelengths (FP64)."""
 
+    mixed = False
+
     def __init__(self, tables, eneis):
         dev = tables.device
         n = tables.n
         B = len(eneis)
         self.n, self.B, self.eneis = n, B, list(eneis)
         c128 = dict(dtype=torch.complex128, device=dev)
-        self.G1, self.G2, self.H1, self.H2, self.D = [torch.empty((B, n, n), **c128) for _ in range(5)]
-        self.piv = torch.empty((B, 3 * n), dtype=torch.int32, device=dev)
-        self.info = torch.zeros(B, dtype=torch.int32, device=dev)
+        # G1/G2 and H1/H2 back to back: the solver factorises each pair as one batch
+        self.GG = torch.empty((2, B, n, n), **c128)
+        self.HH = torch.empty((2, B, n, n), **c128)
+        self.G1, self.G2 = self.GG[0], self.GG[1]
+        self.H1, self.H2 = self.HH[0], self.HH[1]
+        self.D = torch.empty((B, n, n), **c128)
+        self.piv = torch.empty((3, B, n), dtype=torch.int32, device=dev)
+        self.info = torch.zeros((2, B), dtype=torch.int32, device=dev)
         wb = int(_lib.lib().mnpb_bemret_workspace_f64(n, B))
         self.work = torch.empty(wb, dtype=torch.uint8, device=dev)
+
+
+class _MixedBatch(object):
+    """Device buffers of a mixed-precision batch: FP64 G1, G2, H1, H2 (the
+    exact operator for refinement) and their planar FP32 copies, factorised on
+    the tensor cores.  Leading dimension ld = n rounded up to 4."""
+
+    mixed = True
+
+    def __init__(self, tables, eneis):
+        dev = tables.device
+        n = tables.n
+        B = len(eneis)
+        ld = (n + 3) // 4 * 4
+        self.n, self.B, self.ld, self.eneis = n, B, ld, list(eneis)
+        c128 = dict(dtype=torch.complex128, device=dev)
+        f32 = dict(dtype=torch.float32, device=dev)
+        self.G1, self.G2, self.H1, self.H2 = [torch.empty((B, n, ld), **c128) for _ in range(4)]
+        # planar copies; G1p/G2p and H1p/H2p back to back (factorised as one batch)
+        self.GGp = torch.empty((2, B, 2, n, ld), **f32)
+        self.HHp = torch.empty((2, B, 2, n, ld), **f32)
+        self.G1p, self.G2p = self.GGp[0], self.GGp[1]
+        self.H1p, self.H2p = self.HHp[0], self.HHp[1]
+        self.Dp = torch.empty((B, 2, n, ld), **f32)
+        self.piv = torch.empty((3, B, n), dtype=torch.int32, device=dev)
+        self.info = torch.zeros((2, B), dtype=torch.int32, device=dev)
+        self.dinv = torch.empty(int(_lib.lib().mnpb_bemret_dinv_floats(n, B)), **f32)
+        wb = int(_lib.lib().mnpb_bemret_workspace_mixed(n, B))
+        self.work = torch.empty(wb, dtype=torch.uint8, device=dev)
+        self.iters = None
+        self.relres = None
 
 
 class BEMRet(object):
     """Retarded BEM solver (full Maxwell equations), dense, on the GPU."""
 
-    def __init__(self, p, enei=None, **options):
+    def __init__(self, p, enei=None, precision='fp64', refine_tol=1e-11, refine_maxit=12,
+                 **options):
+        """``precision``: 'fp64' (the reference's arithmetic) or 'mixed' (FP32
+        storage, TF32 tensor-core factorisations, FP64 iterative refinement
+        of the solution to ``refine_tol`` relative residual)."""
         _check_particle(p, 'BEMRet')
+        if precision not in ('fp64', 'mixed'):
+            raise ValueError("BEMRet: precision must be 'fp64' or 'mixed'")
+        self.precision = precision
+        self.refine_tol = refine_tol
+        self.refine_maxit = refine_maxit
         self.p = p
         self.enei = None
         self.options = dict(options)
@@ -92,16 +139,33 @@ class BEMRet(object):
 
     def _factor(self, eneis, stream=None):
         t = self.tables
-        bt = _RetBatch(t, eneis)
+        n, B = t.n, len(eneis)
         kblk, sblk = t.k_tables(eneis)
-        t.assemble(kblk, sblk, (bt.G1, bt.H1, bt.G2, bt.H2), mode=0, stream=stream)
         eps, kvac = self._eps_tables(eneis)
+        sh = _lib.stream_handle(stream)
+        if self.precision == 'fp64':
+            bt = _RetBatch(t, eneis)
+            t.assemble(kblk, sblk, (bt.G1, bt.H1, bt.G2, bt.H2), mode=0, stream=stream)
+            bt.eps = torch.from_numpy(eps).to(t.device)
+            bt.kvac = torch.from_numpy(kvac).to(t.device)
+            call('mnpb_bemret_init_f64', sh, n, B, ptr(bt.G1), ptr(bt.G2), ptr(bt.H1),
+                 ptr(bt.H2), ptr(bt.D), n, n * n, ptr(bt.eps), ptr(bt.kvac), ptr(t.nvec),
+                 ptr(bt.piv), ptr(bt.info), ptr(bt.work), bt.work.numel())
+            return bt
+        bt = _MixedBatch(t, eneis)
+        ld = bt.ld
+        d_k = torch.from_numpy(np.ascontiguousarray(kblk)).to(t.device)
+        d_s = torch.from_numpy(np.ascontiguousarray(sblk)).to(t.device)
+        poff = np.ascontiguousarray(t.part_off, dtype=np.int64)
+        call('mnpb_assemble_ret2', sh, n, B, ptr(t.pos), ptr(t.nvec), ptr(t.area), t.nparts,
+             ptr(poff), ptr(d_k), ptr(d_s), t.nref, ptr(t.rows), ptr(t.cols), ptr(t.g),
+             ptr(t.fn), ptr(bt.G1), ptr(bt.H1), ptr(bt.G2), ptr(bt.H2), ld, ld * n,
+             ptr(bt.G1p), ptr(bt.H1p), ptr(bt.G2p), ptr(bt.H2p), ld, 2 * ld * n, ld * n)
         bt.eps = torch.from_numpy(eps).to(t.device)
         bt.kvac = torch.from_numpy(kvac).to(t.device)
-        n, B = t.n, len(eneis)
-        call('mnpb_bemret_init_f64', _lib.stream_handle(stream), n, B, ptr(bt.G1), ptr(bt.G2),
-             ptr(bt.H1), ptr(bt.H2), ptr(bt.D), n, n * n, ptr(bt.eps), ptr(bt.kvac),
-             ptr(t.nvec), ptr(bt.piv), ptr(bt.info), ptr(bt.work), bt.work.numel())
+        call('mnpb_bemret_init_mixed', sh, n, B, ptr(bt.G1p), ptr(bt.G2p), ptr(bt.H1p),
+             ptr(bt.H2p), ptr(bt.Dp), ld, ptr(bt.eps), ptr(bt.kvac), ptr(t.nvec), ptr(bt.piv),
+             ptr(bt.info), ptr(bt.dinv), ptr(bt.work), bt.work.numel())
         return bt
 
     def init(self, enei):
@@ -160,12 +224,30 @@ class BEMRet(object):
         xout = torch.empty_like(xin)
         call('mnpb_bemret_excitation', sh, n, B, K, ptr(pots_dev), ptr(bt.eps), ptr(bt.kvac),
              ptr(t.nvec), ptr(xin))
-        wb = B * n * 15 * K * 16
-        work = torch.empty(wb, dtype=torch.uint8, device=t.device)
-        call('mnpb_bemret_solve_f64', sh, n, B, K, ptr(bt.G1), ptr(bt.G2), ptr(bt.H1),
-             ptr(bt.H2), ptr(bt.D), n, n * n, ptr(bt.piv), ptr(bt.eps), ptr(bt.kvac),
-             ptr(t.nvec), ptr(xin), ptr(xout), ptr(work), wb)
-        return xout
+        if not bt.mixed:
+            wb = B * n * 15 * K * 16
+            work = torch.empty(wb, dtype=torch.uint8, device=t.device)
+            call('mnpb_bemret_solve_f64', sh, n, B, K, ptr(bt.G1), ptr(bt.G2), ptr(bt.H1),
+                 ptr(bt.H2), ptr(bt.D), n, n * n, ptr(bt.piv), ptr(bt.eps), ptr(bt.kvac),
+                 ptr(t.nvec), ptr(xin), ptr(xout), ptr(work), wb)
+            return xout
+        out = []
+        for k0 in range(0, K, 4):          # the refinement solves up to 4 excitations at once
+            kk = min(4, K - k0)
+            b_in = xin[:, :, k0:k0 + kk].contiguous()
+            x = torch.empty_like(b_in)
+            wb = int(_lib.lib().mnpb_bemret_refine_workspace(n, B, kk))
+            work = torch.empty(wb, dtype=torch.uint8, device=t.device)
+            iters = np.zeros(B, dtype=np.int32)
+            relres = np.zeros(B)
+            call('mnpb_bemret_solve_refine', sh, n, B, kk, ptr(bt.G1p), ptr(bt.G2p),
+                 ptr(bt.H1p), ptr(bt.H2p), ptr(bt.Dp), bt.ld, ptr(bt.piv), ptr(bt.dinv), ptr(bt.G1),
+                 ptr(bt.G2), ptr(bt.H1), ptr(bt.H2), ptr(bt.eps), ptr(bt.kvac), ptr(t.nvec),
+                 ptr(b_in), ptr(x), int(self.refine_maxit), float(self.refine_tol), ptr(iters),
+                 ptr(relres), ptr(work), wb)
+            bt.iters, bt.relres = iters, relres
+            out.append(x)
+        return out[0] if len(out) == 1 else torch.cat(out, dim=2).contiguous()
 
     def solve(self, exc):
         """Surface charges and currents for an excitation (bem_ret.py:1569-1831)."""

@@ -1,0 +1,730 @@
+// Batched dense complex linear algebra in FP32 on planar storage (real plane,
+// imaginary plane), column-major, for the mixed-precision solver.
+//
+// LU is recursive (split the columns in halves; factor the left half; update
+// the right half with a triangular solve and a GEMM; factor the rest), so
+// nearly all flops land in large GEMMs that run on the tensor cores
+// (tc::cgemm_tf32); only the 32-column leaves run on CUDA cores.
+#include "common.cuh"
+#include "dense_f32.cuh"
+
+namespace mnpb {
+namespace f32 {
+
+using tc::CMatF;
+
+namespace {
+
+constexpr int PANEL_THREADS = 512;
+constexpr int TS = 32;
+
+struct cf {
+    float x, y;
+};
+__device__ __forceinline__ cf fmk(float r, float i) { return cf{r, i}; }
+__device__ __forceinline__ cf fmul(cf a, cf b) { return cf{a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x}; }
+__device__ __forceinline__ cf ffms(cf a, cf b, cf c) {   // c - a*b
+    c.x = fmaf(-a.x, b.x, c.x);
+    c.x = fmaf(a.y, b.y, c.x);
+    c.y = fmaf(-a.x, b.y, c.y);
+    c.y = fmaf(-a.y, b.x, c.y);
+    return c;
+}
+__device__ __forceinline__ cf frcp(cf b) {
+    if (fabsf(b.x) >= fabsf(b.y)) {
+        float r = b.y / b.x, d = b.x + b.y * r;
+        return cf{1.f / d, -r / d};
+    } else {
+        float r = b.x / b.y, d = b.y + b.x * r;
+        return cf{r / d, -1.f / d};
+    }
+}
+__device__ __forceinline__ cf ld(const float *p, int64_t plane, int64_t o) {
+    return cf{p[o], p[o + plane]};
+}
+__device__ __forceinline__ void st(float *p, int64_t plane, int64_t o, cf v) {
+    p[o] = v.x;
+    p[o + plane] = v.y;
+}
+
+// LU leaf: columns [k0, k0+kb) (kb <= 32) over rows [k0, n), one CTA per matrix.
+__global__ void __launch_bounds__(PANEL_THREADS) panel_kernel(int n, int k0, int kb, float *A,
+                                                              int64_t lda, int64_t plane,
+                                                              int64_t sA, int32_t *ipiv,
+                                                              int64_t sP, int32_t *info) {
+    __shared__ float red_v[PANEL_THREADS / 32];
+    __shared__ int red_i[PANEL_THREADS / 32];
+    __shared__ cf prow[TS];
+    __shared__ int s_piv;
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    const int64_t b = blockIdx.x;
+    A += b * sA;
+    ipiv += b * sP;
+    for (int jj = 0; jj < kb; ++jj) {
+        const int c = k0 + jj;
+        const int64_t co = (int64_t)c * lda;
+        float best = -1.f;
+        int bi = n;
+        for (int r = c + tid; r < n; r += PANEL_THREADS) {
+            float v = fabsf(A[co + r]) + fabsf(A[co + r + plane]);
+            if (v > best) { best = v; bi = r; }
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            float ov = __shfl_xor_sync(0xffffffffu, best, o);
+            int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+            if (ov > best || (ov == best && oi < bi)) { best = ov; bi = oi; }
+        }
+        if (lane == 0) { red_v[wid] = best; red_i[wid] = bi; }
+        __syncthreads();
+        if (wid == 0) {
+            best = (lane < PANEL_THREADS / 32) ? red_v[lane] : -1.f;
+            bi = (lane < PANEL_THREADS / 32) ? red_i[lane] : n;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                float ov = __shfl_xor_sync(0xffffffffu, best, o);
+                int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+                if (ov > best || (ov == best && oi < bi)) { best = ov; bi = oi; }
+            }
+            if (lane == 0) {
+                int p = bi;
+                if (!(best > 0.f)) {
+                    p = c;
+                    if (info && info[b] == 0) info[b] = c + 1;
+                }
+                s_piv = p;
+                ipiv[c] = p;
+            }
+        }
+        __syncthreads();
+        const int p = s_piv;
+        if (p != c) {
+            for (int cc = tid; cc < kb; cc += PANEL_THREADS) {
+                const int64_t o = (int64_t)(k0 + cc) * lda;
+                cf t = ld(A, plane, o + c);
+                st(A, plane, o + c, ld(A, plane, o + p));
+                st(A, plane, o + p, t);
+            }
+        }
+        __syncthreads();
+        const int rest = kb - jj;
+        for (int cc = tid; cc < rest; cc += PANEL_THREADS) prow[cc] = ld(A, plane, (int64_t)(c + cc) * lda + c);
+        __syncthreads();
+        const cf pv = prow[0];
+        const bool nz = (pv.x != 0.f || pv.y != 0.f);
+        const cf inv = nz ? frcp(pv) : fmk(0.f, 0.f);
+        for (int r = c + 1 + tid; r < n; r += PANEL_THREADS) {
+            cf l = ld(A, plane, co + r);
+            if (nz) l = fmul(l, inv);
+            st(A, plane, co + r, l);
+            for (int cc = 1; cc < rest; ++cc) {
+                const int64_t o = (int64_t)(c + cc) * lda + r;
+                st(A, plane, o, ffms(l, prow[cc], ld(A, plane, o)));
+            }
+        }
+        __syncthreads();
+    }
+}
+
+__global__ void laswp_kernel(float *A, int64_t lda, int64_t plane, int64_t sA, int j0, int j1,
+                             const int32_t *ipiv, int64_t sP, int c0, int c1, int forward) {
+    const int64_t b = blockIdx.y;
+    const int j = j0 + blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= j1) return;
+    float *col = A + b * sA + (int64_t)j * lda;
+    const int32_t *pv = ipiv + b * sP;
+    if (forward) {
+        for (int c = c0; c < c1; ++c) {
+            const int p = pv[c];
+            if (p != c) {
+                cf t = ld(col, plane, c);
+                st(col, plane, c, ld(col, plane, p));
+                st(col, plane, p, t);
+            }
+        }
+    } else {
+        for (int c = c1 - 1; c >= c0; --c) {
+            const int p = pv[c];
+            if (p != c) {
+                cf t = ld(col, plane, c);
+                st(col, plane, c, ld(col, plane, p));
+                st(col, plane, p, t);
+            }
+        }
+    }
+}
+
+__global__ void colswp_kernel(float *X, int64_t ldx, int64_t plane, int64_t sX, int m,
+                              const int32_t *ipiv, int64_t sP, int n) {
+    const int64_t b = blockIdx.y;
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= m) return;
+    float *x = X + b * sX + r;
+    const int32_t *pv = ipiv + b * sP;
+    for (int c = n - 1; c >= 0; --c) {
+        const int p = pv[c];
+        if (p != c) {
+            cf t = ld(x, plane, (int64_t)c * ldx);
+            st(x, plane, (int64_t)c * ldx, ld(x, plane, (int64_t)p * ldx));
+            st(x, plane, (int64_t)p * ldx, t);
+        }
+    }
+}
+
+// Small triangular solves (kb <= 32), same modes as the FP64 version:
+// 0 left lower unit, 1 left upper non-unit, 2 right upper non-unit,
+// 3 right lower unit.
+__global__ void __launch_bounds__(128) trsm_small_kernel(int mode, int kb, const float *T,
+                                                         int64_t ldt, int64_t planeT, int64_t sT,
+                                                         float *B, int64_t ldb, int64_t planeB,
+                                                         int64_t sB, int nvec) {
+    __shared__ cf Ts[TS][TS + 1];
+    const int64_t b = blockIdx.y;
+    T += b * sT;
+    B += b * sB;
+    for (int e = threadIdx.x; e < TS * TS; e += blockDim.x) {
+        const int r = e % TS, c = e / TS;
+        Ts[r][c] = (r < kb && c < kb) ? ld(T, planeT, (int64_t)c * ldt + r)
+                                      : fmk(r == c ? 1.f : 0.f, 0.f);
+    }
+    __syncthreads();
+    const int v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= nvec) return;
+    cf x[TS];
+    const bool left = mode < 2;
+#pragma unroll
+    for (int e = 0; e < TS; ++e)
+        x[e] = (e < kb) ? ld(B, planeB, left ? (int64_t)v * ldb + e : (int64_t)e * ldb + v)
+                        : fmk(0.f, 0.f);
+    if (mode == 0) {
+#pragma unroll
+        for (int r = 1; r < TS; ++r)
+#pragma unroll
+            for (int c = 0; c < r; ++c) x[r] = ffms(Ts[r][c], x[c], x[r]);
+    } else if (mode == 1) {
+#pragma unroll
+        for (int r = TS - 1; r >= 0; --r) {
+#pragma unroll
+            for (int c = r + 1; c < TS; ++c) x[r] = ffms(Ts[r][c], x[c], x[r]);
+            x[r] = fmul(x[r], frcp(Ts[r][r]));
+        }
+    } else if (mode == 2) {
+#pragma unroll
+        for (int c = 0; c < TS; ++c) {
+#pragma unroll
+            for (int r = 0; r < c; ++r) x[c] = ffms(x[r], Ts[r][c], x[c]);
+            x[c] = fmul(x[c], frcp(Ts[c][c]));
+        }
+    } else {
+#pragma unroll
+        for (int c = TS - 1; c >= 0; --c)
+#pragma unroll
+            for (int r = c + 1; r < TS; ++r) x[c] = ffms(x[r], Ts[r][c], x[c]);
+    }
+#pragma unroll
+    for (int e = 0; e < TS; ++e)
+        if (e < kb) st(B, planeB, left ? (int64_t)v * ldb + e : (int64_t)e * ldb + v, x[e]);
+}
+
+// Skinny GEMM C = alpha A B + beta C for at most NC (<= 16) columns (matrix
+// times a few vectors): one thread per row, A streamed once with coalesced
+// column reads, B broadcast from shared memory.  Real alpha, beta.
+constexpr int SK_N = 16, SK_KT = 64;
+
+template <int NC>
+__global__ void __launch_bounds__(128) skinny_kernel(int m, int n, int k, float alpha,
+                                                     const float *__restrict__ A, int64_t lda,
+                                                     int64_t planeA, int64_t sA,
+                                                     const float *__restrict__ B, int64_t ldb,
+                                                     int64_t planeB, int64_t sB, float beta,
+                                                     float *__restrict__ C, int64_t ldc,
+                                                     int64_t planeC, int64_t sC) {
+    __shared__ cf Bs[SK_KT][NC];
+    const int64_t b = blockIdx.y;
+    A += b * sA;
+    B += b * sB;
+    C += b * sC;
+    const int row = blockIdx.x * blockDim.x + threadIdx.x;
+    cf acc[NC];
+#pragma unroll
+    for (int j = 0; j < NC; ++j) acc[j] = fmk(0.f, 0.f);
+    for (int k0 = 0; k0 < k; k0 += SK_KT) {
+        __syncthreads();
+        for (int e = threadIdx.x; e < SK_KT * NC; e += blockDim.x) {
+            const int kk = e % SK_KT, j = e / SK_KT;
+            Bs[kk][j] = (k0 + kk < k && j < n) ? ld(B, planeB, (int64_t)j * ldb + k0 + kk)
+                                               : fmk(0.f, 0.f);
+        }
+        __syncthreads();
+        if (row < m) {
+            const int kend = min(SK_KT, k - k0);
+            const float *ar = A + (int64_t)k0 * lda + row;
+#pragma unroll 4
+            for (int kk = 0; kk < kend; ++kk) {
+                const cf a = fmk(__ldg(ar + (int64_t)kk * lda), __ldg(ar + (int64_t)kk * lda + planeA));
+#pragma unroll
+                for (int j = 0; j < NC; ++j) {
+                    acc[j].x = fmaf(a.x, Bs[kk][j].x, acc[j].x);
+                    acc[j].x = fmaf(-a.y, Bs[kk][j].y, acc[j].x);
+                    acc[j].y = fmaf(a.x, Bs[kk][j].y, acc[j].y);
+                    acc[j].y = fmaf(a.y, Bs[kk][j].x, acc[j].y);
+                }
+            }
+        }
+    }
+    if (row >= m) return;
+#pragma unroll
+    for (int j = 0; j < NC; ++j) {
+        if (j < n) {
+            const int64_t o = (int64_t)j * ldc + row;
+            cf c = beta != 0.f ? ld(C, planeC, o) : fmk(0.f, 0.f);
+            st(C, planeC, o, fmk(alpha * acc[j].x + beta * c.x, alpha * acc[j].y + beta * c.y));
+        }
+    }
+}
+
+
+// ---------------------------------------------------------------------------
+// Few-RHS triangular solves in one launch per triangle.
+//
+// Block rows of 32: block j needs the solution of every earlier block (in
+// solve order).  A CTA takes a ticket from an atomic counter and handles the
+// (block, matrix) pair of that ticket, tickets ordered block-major, so every
+// block it waits for has a lower ticket and has started: the smallest
+// unfinished ticket can always proceed.  Blocks publish their solution with a
+// release (fence + atomic flag = epoch); waiters use acquire loads, bounded
+// by a 1 s wall-clock limit after which an error word is set and the kernel
+// continues (the solve is then invalid and reported, but nothing hangs).
+// The 32 x 32 diagonal blocks are applied through precomputed inverses.
+// ---------------------------------------------------------------------------
+constexpr int TB = 32;
+constexpr uint64_t TRSV_WAIT_NS = 1000000000ull;
+
+__device__ int g_trsv_error;
+
+__device__ __forceinline__ uint64_t gtimer() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+    return t;
+}
+__device__ __forceinline__ int ld_acquire(const int *p) {
+    int v;
+    asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+// Inverse of each 32 x 32 diagonal block of the unit-lower (lower = 1) or
+// upper (lower = 0) factor; out[b][blk][2][32][32] (planar, column-major).
+__global__ void __launch_bounds__(TB) diag_inv_kernel(int n, int lower, const float *A,
+                                                      int64_t lda, int64_t plane, int64_t sA,
+                                                      float *out, int nb) {
+    __shared__ cf T[TB][TB + 1];
+    const int blk = blockIdx.x;
+    const int64_t b = blockIdx.y;
+    const int r0 = blk * TB, kb = min(TB, n - r0);
+    A += b * sA;
+    for (int c = 0; c < TB; ++c) {
+        const int r = threadIdx.x;
+        cf v = fmk(r == c ? 1.f : 0.f, 0.f);
+        if (r < kb && c < kb) {
+            const bool in = lower ? (r > c) : (r <= c);
+            if (in) v = ld(A, plane, (int64_t)(r0 + c) * lda + r0 + r);
+            else v = (lower && r == c) ? fmk(1.f, 0.f) : fmk(0.f, 0.f);
+        }
+        T[r][c] = v;
+    }
+    __syncthreads();
+    // column t of the inverse: solve T x = e_t
+    const int t = threadIdx.x;
+    cf x[TB];
+#pragma unroll
+    for (int e = 0; e < TB; ++e) x[e] = fmk(e == t ? 1.f : 0.f, 0.f);
+    if (lower) {
+#pragma unroll
+        for (int r = 1; r < TB; ++r)
+#pragma unroll
+            for (int c = 0; c < r; ++c) x[r] = ffms(T[r][c], x[c], x[r]);
+    } else {
+#pragma unroll
+        for (int r = TB - 1; r >= 0; --r) {
+#pragma unroll
+            for (int c = r + 1; c < TB; ++c) x[r] = ffms(T[r][c], x[c], x[r]);
+            x[r] = fmul(x[r], frcp(T[r][r]));
+        }
+    }
+    float *o = out + ((b * nb + blk) * 2) * TB * TB;
+#pragma unroll
+    for (int e = 0; e < TB; ++e) {
+        o[t * TB + e] = x[e].x;
+        o[TB * TB + t * TB + e] = x[e].y;
+    }
+}
+
+template <int NC>
+__global__ void __launch_bounds__(256) trsv_kernel(int n, int m, int lower, const float *A,
+                                                   int64_t lda, int64_t plane, int64_t sA,
+                                                   const float *__restrict__ Dinv, float *X,
+                                                   int64_t ldx, int64_t planeX, int64_t sX,
+                                                   int *flags, unsigned *ticket, int epoch,
+                                                   int nb, int batch) {
+    __shared__ int s_ticket;
+    __shared__ cf red[8][TB][NC];
+    __shared__ cf rhs[TB][NC];
+    const int tid = threadIdx.x, r = tid & 31, q = tid >> 5;
+    if (tid == 0) s_ticket = (int)atomicAdd(ticket, 1u);
+    __syncthreads();
+    const int tk = s_ticket;
+    const int jj = tk / batch;
+    const int64_t b = tk % batch;
+    const int j = lower ? jj : nb - 1 - jj;
+    const int r0 = j * TB, rows = min(TB, n - r0);
+    A += b * sA;
+    X += b * sX;
+    int *fl = flags + b * nb;
+    cf acc[NC];
+#pragma unroll
+    for (int c = 0; c < NC; ++c) acc[c] = fmk(0.f, 0.f);
+    for (int ii = 0; ii < jj; ++ii) {
+        const int i = lower ? ii : nb - 1 - ii;
+        if (tid == 0) {
+            const uint64_t t0 = gtimer();
+            while (ld_acquire(fl + i) != epoch) {
+                if (gtimer() - t0 > TRSV_WAIT_NS) {
+                    atomicCAS(&g_trsv_error, 0, 1);
+                    break;
+                }
+            }
+        }
+        __syncthreads();
+        if (r < rows) {
+#pragma unroll
+            for (int t = 0; t < 4; ++t) {
+                const int col = i * TB + q + 8 * t;
+                if (col < n) {
+                    const int64_t o = (int64_t)col * lda + r0 + r;
+                    const cf a = fmk(A[o], A[o + plane]);
+#pragma unroll
+                    for (int c = 0; c < NC; ++c) {
+                        if (c < m) {
+                            const int64_t xo = (int64_t)c * ldx + col;
+                            const cf xv = fmk(__ldcg(X + xo), __ldcg(X + xo + planeX));
+                            acc[c].x = fmaf(a.x, xv.x, acc[c].x);
+                            acc[c].x = fmaf(-a.y, xv.y, acc[c].x);
+                            acc[c].y = fmaf(a.x, xv.y, acc[c].y);
+                            acc[c].y = fmaf(a.y, xv.x, acc[c].y);
+                        }
+                    }
+                }
+            }
+        }
+    }
+#pragma unroll
+    for (int c = 0; c < NC; ++c) red[q][r][c] = acc[c];
+    __syncthreads();
+    for (int e = tid; e < TB * NC; e += 256) {
+        const int rr = e % TB, c = e / TB;
+        cf v = fmk(0.f, 0.f);
+        if (rr < rows && c < m) {
+            const int64_t xo = (int64_t)c * ldx + r0 + rr;
+            v = fmk(__ldcg(X + xo), __ldcg(X + xo + planeX));
+            for (int qq = 0; qq < 8; ++qq) {
+                v.x -= red[qq][rr][c].x;
+                v.y -= red[qq][rr][c].y;
+            }
+        }
+        rhs[rr][c] = v;
+    }
+    __syncthreads();
+    const float *Di = Dinv + (b * nb + j) * 2 * TB * TB;
+    for (int e = tid; e < TB * NC; e += 256) {
+        const int rr = e % TB, c = e / TB;
+        if (rr < rows && c < m) {
+            cf y = fmk(0.f, 0.f);
+            for (int k = 0; k < TB; ++k) {
+                const cf d = fmk(__ldg(Di + k * TB + rr), __ldg(Di + TB * TB + k * TB + rr));
+                y.x = fmaf(d.x, rhs[k][c].x, y.x);
+                y.x = fmaf(-d.y, rhs[k][c].y, y.x);
+                y.y = fmaf(d.x, rhs[k][c].y, y.y);
+                y.y = fmaf(d.y, rhs[k][c].x, y.y);
+            }
+            const int64_t xo = (int64_t)c * ldx + r0 + rr;
+            X[xo] = y.x;
+            X[xo + planeX] = y.y;
+        }
+    }
+    __syncthreads();
+    if (tid == 0) {
+        __threadfence();
+        atomicExch(fl + j, epoch);
+    }
+}
+
+__global__ void set_identity_kernel(float *W, int64_t ldw, int64_t plane, int64_t sW, int n) {
+    const int64_t b = blockIdx.z;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y;
+    if (i >= n) return;
+    float *w = W + b * sW + (int64_t)j * ldw + i;
+    w[0] = (i == j) ? 1.f : 0.f;
+    w[plane] = 0.f;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// host orchestration
+// ---------------------------------------------------------------------------
+Ctx::Ctx(cudaStream_t s_, int batch_, float *work_, int64_t work_bytes_)
+    : s(s_), batch(batch_), work(work_), work_bytes(work_bytes_) {}
+
+int gemm(Ctx &c, int m, int n, int k, float alpha, CMatF A, CMatF B, float beta, CMatF C) {
+    if (m <= 0 || n <= 0) return MNPB_OK;
+    if (k <= 0) {
+        if (beta == 1.f) return MNPB_OK;
+        set_error("f32 gemm: k = 0 with beta != 1 is not supported");
+        return MNPB_EINVAL;
+    }
+    if (n <= SK_N) {
+        dim3 grid(ceil_div(m, 128), c.batch);
+        ProfScope ps(c.s, PC_SGEMM, 8.0 * (double)m * k * c.batch);   // bytes of A streamed
+#define MNPB_SKINNY(NC)                                                                        \
+    skinny_kernel<NC><<<grid, 128, 0, c.s>>>(m, n, k, alpha, A.p, A.ld, A.plane, A.stride, B.p, \
+                                             B.ld, B.plane, B.stride, beta, C.p, C.ld, C.plane, \
+                                             C.stride)
+        if (n <= 1) MNPB_SKINNY(1);
+        else if (n <= 2) MNPB_SKINNY(2);
+        else if (n <= 4) MNPB_SKINNY(4);
+        else if (n <= 8) MNPB_SKINNY(8);
+        else MNPB_SKINNY(16);
+#undef MNPB_SKINNY
+        MNPB_LAUNCH_CHECK("skinny_kernel");
+        return MNPB_OK;
+    }
+    return tc::cgemm_tf32(c.s, m, n, k, c.batch, alpha, A, B, beta, C, c.work, c.work_bytes);
+}
+
+static int trsm_small(Ctx &c, int mode, int kb, CMatF T, CMatF B, int nvec) {
+    if (nvec <= 0 || kb <= 0) return MNPB_OK;
+    dim3 grid(ceil_div(nvec, 128), c.batch);
+    ProfScope ps(c.s, PC_TRSM, 4.0 * kb * kb * (double)nvec * c.batch);
+    trsm_small_kernel<<<grid, 128, 0, c.s>>>(mode, kb, T.p, T.ld, T.plane, T.stride, B.p, B.ld,
+                                             B.plane, B.stride, nvec);
+    MNPB_LAUNCH_CHECK("trsm_small_kernel(f32)");
+    return MNPB_OK;
+}
+
+static int split_point(int n) {
+    int h = n / 2;
+    h = (h / TS) * TS;
+    return h < TS ? TS : h;
+}
+
+int trsm_llu(Ctx &c, int n, int m, CMatF L, CMatF B) {
+    if (n <= TS) return trsm_small(c, 0, n, L, B, m);
+    const int n1 = split_point(n);
+    MNPB_TRY(trsm_llu(c, n1, m, L, B));
+    MNPB_TRY(gemm(c, n - n1, m, n1, -1.f, L.sub(n1, 0), B, 1.f, B.sub(n1, 0)));
+    return trsm_llu(c, n - n1, m, L.sub(n1, n1), B.sub(n1, 0));
+}
+
+int trsm_lun(Ctx &c, int n, int m, CMatF U, CMatF B) {
+    if (n <= TS) return trsm_small(c, 1, n, U, B, m);
+    const int n1 = split_point(n);
+    MNPB_TRY(trsm_lun(c, n - n1, m, U.sub(n1, n1), B.sub(n1, 0)));
+    MNPB_TRY(gemm(c, n1, m, n - n1, -1.f, U.sub(0, n1), B.sub(n1, 0), 1.f, B));
+    return trsm_lun(c, n1, m, U, B);
+}
+
+int trsm_run(Ctx &c, int n, int m, CMatF U, CMatF B) {
+    if (n <= TS) return trsm_small(c, 2, n, U, B, m);
+    const int n1 = split_point(n);
+    MNPB_TRY(trsm_run(c, n1, m, U, B));
+    MNPB_TRY(gemm(c, m, n - n1, n1, -1.f, B, U.sub(0, n1), 1.f, B.sub(0, n1)));
+    return trsm_run(c, n - n1, m, U.sub(n1, n1), B.sub(0, n1));
+}
+
+int trsm_rlu(Ctx &c, int n, int m, CMatF L, CMatF B) {
+    if (n <= TS) return trsm_small(c, 3, n, L, B, m);
+    const int n1 = split_point(n);
+    MNPB_TRY(trsm_rlu(c, n - n1, m, L.sub(n1, n1), B.sub(0, n1)));
+    MNPB_TRY(gemm(c, m, n1, n - n1, -1.f, B.sub(0, n1), L.sub(n1, 0), 1.f, B));
+    return trsm_rlu(c, n1, m, L, B);
+}
+
+int laswp(Ctx &c, CMatF A, int j0, int j1, const int32_t *ipiv, int64_t sP, int c0, int c1,
+          bool forward) {
+    if (j1 <= j0 || c1 <= c0) return MNPB_OK;
+    dim3 grid(ceil_div(j1 - j0, 128), c.batch);
+    ProfScope ps(c.s, PC_SWAP, 0.0);
+    laswp_kernel<<<grid, 128, 0, c.s>>>(A.p, A.ld, A.plane, A.stride, j0, j1, ipiv, sP, c0, c1,
+                                        forward ? 1 : 0);
+    MNPB_LAUNCH_CHECK("laswp_kernel(f32)");
+    return MNPB_OK;
+}
+
+// Factor columns [off, off+w) over rows [off, n) of the full matrix A;
+// pivots are absolute row indices.
+static int rgetrf(Ctx &c, int n, int off, int w, CMatF A, int32_t *ipiv, int64_t sP,
+                  int32_t *info) {
+    if (w <= TS) {
+        ProfScope ps(c.s, PC_PANEL, 8.0 * w * w * (double)(n - off) * c.batch / 2);
+        panel_kernel<<<c.batch, PANEL_THREADS, 0, c.s>>>(n, off, w, A.p, A.ld, A.plane, A.stride,
+                                                         ipiv, sP, info);
+        MNPB_LAUNCH_CHECK("panel_kernel(f32)");
+        return MNPB_OK;
+    }
+    const int w1 = split_point(w);
+    MNPB_TRY(rgetrf(c, n, off, w1, A, ipiv, sP, info));
+    MNPB_TRY(laswp(c, A, off + w1, off + w, ipiv, sP, off, off + w1, true));
+    MNPB_TRY(trsm_llu(c, w1, w - w1, A.sub(off, off), A.sub(off, off + w1)));
+    MNPB_TRY(gemm(c, n - off - w1, w - w1, w1, -1.f, A.sub(off + w1, off),
+                  A.sub(off, off + w1), 1.f, A.sub(off + w1, off + w1)));
+    MNPB_TRY(rgetrf(c, n, off + w1, w - w1, A, ipiv, sP, info));
+    return laswp(c, A, off, off + w1, ipiv, sP, off + w1, off + w, true);
+}
+
+int getrf(Ctx &c, int n, CMatF A, int32_t *ipiv, int64_t sP, int32_t *info) {
+    return rgetrf(c, n, 0, n, A, ipiv, sP, info);
+}
+
+int getrs(Ctx &c, int n, int nrhs, CMatF LU, const int32_t *ipiv, int64_t sP, CMatF B) {
+    MNPB_TRY(laswp(c, B, 0, nrhs, ipiv, sP, 0, n, true));
+    MNPB_TRY(trsm_llu(c, n, nrhs, LU, B));
+    return trsm_lun(c, n, nrhs, LU, B);
+}
+
+int right_solve(Ctx &c, int n, int m, CMatF LU, const int32_t *ipiv, int64_t sP, CMatF B) {
+    MNPB_TRY(trsm_run(c, n, m, LU, B));
+    MNPB_TRY(trsm_rlu(c, n, m, LU, B));
+    dim3 grid(ceil_div(m, 128), c.batch);
+    ProfScope ps(c.s, PC_SWAP, 0.0);
+    colswp_kernel<<<grid, 128, 0, c.s>>>(B.p, B.ld, B.plane, B.stride, m, ipiv, sP, n);
+    MNPB_LAUNCH_CHECK("colswp_kernel(f32)");
+    return MNPB_OK;
+}
+
+// ---- few-RHS solves ---------------------------------------------------------
+static int *g_flags = nullptr;
+static unsigned *g_ticket = nullptr;
+static int64_t g_flags_cap = 0;
+static int g_epoch = 0;
+
+static int flags_reserve(int64_t count) {
+    if (count <= g_flags_cap) return MNPB_OK;
+    if (g_flags) cudaFree(g_flags);
+    if (g_ticket) cudaFree(g_ticket);
+    g_flags = nullptr;
+    g_ticket = nullptr;
+    if (cudaMalloc(&g_flags, count * sizeof(int)) != cudaSuccess ||
+        cudaMalloc(&g_ticket, sizeof(unsigned)) != cudaSuccess ||
+        cudaMemset(g_flags, 0, count * sizeof(int)) != cudaSuccess) {
+        set_error("trsv: cannot allocate flags");
+        g_flags_cap = 0;
+        return MNPB_ENOMEM;
+    }
+    g_flags_cap = count;
+    return MNPB_OK;
+}
+
+int64_t diag_inv_floats(int n, int batch) { return (int64_t)batch * ceil_div(n, TB) * 2 * TB * TB; }
+
+int diag_inv(Ctx &c, int n, CMatF LU, float *invL, float *invU) {
+    const int nb = ceil_div(n, TB);
+    dim3 grid(nb, c.batch);
+    ProfScope ps(c.s, PC_TRSM, 0.0);
+    diag_inv_kernel<<<grid, TB, 0, c.s>>>(n, 1, LU.p, LU.ld, LU.plane, LU.stride, invL, nb);
+    MNPB_LAUNCH_CHECK("diag_inv_kernel(L)");
+    diag_inv_kernel<<<grid, TB, 0, c.s>>>(n, 0, LU.p, LU.ld, LU.plane, LU.stride, invU, nb);
+    MNPB_LAUNCH_CHECK("diag_inv_kernel(U)");
+    return MNPB_OK;
+}
+
+static int trsv(Ctx &c, bool lower, int n, int m, CMatF T, const float *inv, CMatF X) {
+    const int nb = ceil_div(n, TB);
+    MNPB_TRY(flags_reserve((int64_t)nb * c.batch));
+    if (++g_epoch <= 0) {
+        // epochs wrapped: clear the flags so that no stale value matches
+        g_epoch = 1;
+        if (cudaMemsetAsync(g_flags, 0, g_flags_cap * sizeof(int), c.s) != cudaSuccess) {
+            set_error("trsv: memset failed");
+            return MNPB_ECUDA;
+        }
+    }
+    if (cudaMemsetAsync(g_ticket, 0, sizeof(unsigned), c.s) != cudaSuccess) {
+        set_error("trsv: memset failed");
+        return MNPB_ECUDA;
+    }
+    const int grid = nb * c.batch;
+    ProfScope ps(c.s, PC_TRSM, 4.0 * (double)n * n * c.batch);   // bytes of the triangle
+#define MNPB_TRSV(NC)                                                                          \
+    trsv_kernel<NC><<<grid, 256, 0, c.s>>>(n, m, lower ? 1 : 0, T.p, T.ld, T.plane, T.stride,   \
+                                           inv, X.p, X.ld, X.plane, X.stride, g_flags,          \
+                                           g_ticket, g_epoch, nb, c.batch)
+    if (m <= 4) MNPB_TRSV(4);
+    else if (m <= 8) MNPB_TRSV(8);
+    else MNPB_TRSV(16);
+#undef MNPB_TRSV
+    MNPB_LAUNCH_CHECK("trsv_kernel");
+    return MNPB_OK;
+}
+
+int getrs_few(Ctx &c, int n, int m, CMatF LU, const int32_t *ipiv, int64_t sP,
+              const float *invL, const float *invU, CMatF B) {
+    if (m > 16) return getrs(c, n, m, LU, ipiv, sP, B);
+    MNPB_TRY(laswp(c, B, 0, m, ipiv, sP, 0, n, true));
+    MNPB_TRY(trsv(c, true, n, m, LU, invL, B));
+    return trsv(c, false, n, m, LU, invU, B);
+}
+
+int trsv_error_read_and_clear(cudaStream_t s, int *code) {
+    int v = 0, z = 0;
+    if (cudaMemcpyFromSymbolAsync(&v, g_trsv_error, sizeof(int), 0, cudaMemcpyDeviceToHost, s) !=
+            cudaSuccess ||
+        cudaMemcpyToSymbolAsync(g_trsv_error, &z, sizeof(int), 0, cudaMemcpyHostToDevice, s) !=
+            cudaSuccess ||
+        cudaStreamSynchronize(s) != cudaSuccess) {
+        set_error("trsv: cannot read the error word");
+        return MNPB_ECUDA;
+    }
+    *code = v;
+    return MNPB_OK;
+}
+
+int set_identity(Ctx &c, int n, CMatF W) {
+    dim3 grid(ceil_div(n, 128), n, c.batch);
+    set_identity_kernel<<<grid, 128, 0, c.s>>>(W.p, W.ld, W.plane, W.stride, n);
+    MNPB_LAUNCH_CHECK("set_identity_kernel(f32)");
+    return MNPB_OK;
+}
+
+}  // namespace f32
+}  // namespace mnpb
+
+using namespace mnpb;
+
+extern "C" int64_t mnpb_f32_workspace(int64_t n, int64_t batch) {
+    // packed-A buffer of the largest tensor-core GEMM the recursions issue
+    return tc::cgemm_tf32_workspace((int)n, (int)n, (int)batch);
+}
+
+extern "C" int mnpb_getrf_c32p(void *stream, int64_t n, int64_t batch, float *A, int64_t ld,
+                               int64_t plane, int64_t stride, int32_t *piv, int64_t pstride,
+                               int32_t *info, void *work, int64_t work_bytes) {
+    clear_error();
+    MNPB_REQUIRE(n > 0 && batch > 0 && batch < 65536 && ld >= n, "getrf_c32p: bad sizes");
+    MNPB_REQUIRE(A && piv && work, "getrf_c32p: null pointer");
+    f32::Ctx c(as_stream(stream), (int)batch, (float *)work, work_bytes);
+    return f32::getrf(c, (int)n, tc::CMatF{A, ld, plane, stride}, piv, pstride, info);
+}
+
+extern "C" int mnpb_getrs_c32p(void *stream, int64_t n, int64_t batch, int64_t nrhs,
+                               const float *LU, int64_t ld, int64_t plane, int64_t stride,
+                               const int32_t *piv, int64_t pstride, float *B, int64_t ldb,
+                               int64_t planeB, int64_t bstride, void *work, int64_t work_bytes) {
+    clear_error();
+    MNPB_REQUIRE(n > 0 && batch > 0 && nrhs > 0 && ld >= n && ldb >= n, "getrs_c32p: bad sizes");
+    MNPB_REQUIRE(LU && piv && B && work, "getrs_c32p: null pointer");
+    f32::Ctx c(as_stream(stream), (int)batch, (float *)work, work_bytes);
+    return f32::getrs(c, (int)n, (int)nrhs, tc::CMatF{(float *)LU, ld, plane, stride}, piv,
+                      pstride, tc::CMatF{B, ldb, planeB, bstride});
+}

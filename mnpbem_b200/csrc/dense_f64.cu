@@ -18,13 +18,16 @@ namespace mnpb {
 namespace {
 constexpr int GBM = 64, GBN = 64, GBK = 8;
 
-__global__ void __launch_bounds__(128) zgemm_kernel(int m, int n, int k, cd alpha,
-                                                    const cd *__restrict__ A, int64_t lda,
-                                                    int64_t sA, const cd *__restrict__ B,
-                                                    int64_t ldb, int64_t sB, cd beta,
-                                                    cd *__restrict__ C, int64_t ldc, int64_t sC) {
+__global__ void __launch_bounds__(128, 2) zgemm_kernel(int m, int n, int k, cd alpha,
+                                                       const cd *__restrict__ A, int64_t lda,
+                                                       int64_t sA, const cd *__restrict__ B,
+                                                       int64_t ldb, int64_t sB, cd beta,
+                                                       cd *__restrict__ C, int64_t ldc,
+                                                       int64_t sC) {
+    // B rows padded by one element: the loader's 8 consecutive threads store
+    // 8 different rows, which must not share shared-memory banks
     __shared__ cd As[GBK][GBM];
-    __shared__ cd Bs[GBK][GBN];
+    __shared__ cd Bs[GBK][GBN + 1];
     const int tid = threadIdx.x;
     const int tn = tid & 15, tm = tid >> 4;
     const int m0 = blockIdx.x * GBM, n0 = blockIdx.y * GBN;
@@ -40,47 +43,65 @@ __global__ void __launch_bounds__(128) zgemm_kernel(int m, int n, int k, cd alph
 
     const int ar = tid & 63, ak = tid >> 6;   // A loader: row, first k
     const int bk = tid & 7, bc = tid >> 3;    // B loader: k, first column
+    cd pa[4], pb[4];
+    auto load = [&](int k0) {
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            int gr = m0 + ar, gk = k0 + ak + 2 * q;
+            pa[q] = (gr < m && gk < k) ? A[(int64_t)gk * lda + gr] : cmk(0.0, 0.0);
+        }
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            int gc = n0 + bc + 16 * q, gk = k0 + bk;
+            pb[q] = (gc < n && gk < k) ? B[(int64_t)gc * ldb + gk] : cmk(0.0, 0.0);
+        }
+    };
+    if (k > 0) load(0);
     for (int k0 = 0; k0 < k; k0 += GBK) {
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            int kk = ak + 2 * q;
-            int gr = m0 + ar, gk = k0 + kk;
-            As[kk][ar] = (gr < m && gk < k) ? A[(int64_t)gk * lda + gr] : cmk(0.0, 0.0);
-        }
+        for (int q = 0; q < 4; ++q) As[ak + 2 * q][ar] = pa[q];
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            int cc = bc + 16 * q;
-            int gc = n0 + cc, gk = k0 + bk;
-            Bs[bk][cc] = (gc < n && gk < k) ? B[(int64_t)gc * ldb + gk] : cmk(0.0, 0.0);
-        }
+        for (int q = 0; q < 4; ++q) Bs[bk][bc + 16 * q] = pb[q];
         __syncthreads();
+        if (k0 + GBK < k) load(k0 + GBK);   // next tile in flight during the math
 #pragma unroll
         for (int kk = 0; kk < GBK; ++kk) {
-            cd a[8], bv[4];
-#pragma unroll
-            for (int r = 0; r < 8; ++r) a[r] = As[kk][tm * 8 + r];
+            cd bv[4];
 #pragma unroll
             for (int c = 0; c < 4; ++c) bv[c] = Bs[kk][tn + 16 * c];
 #pragma unroll
-            for (int r = 0; r < 8; ++r)
+            for (int r = 0; r < 8; ++r) {
+                const cd a = As[kk][tm * 8 + r];
 #pragma unroll
-                for (int c = 0; c < 4; ++c) acc[r][c] = cfma(a[r], bv[c], acc[r][c]);
+                for (int c = 0; c < 4; ++c) acc[r][c] = cfma(a, bv[c], acc[r][c]);
+            }
         }
         __syncthreads();
     }
     const bool beta0 = (beta.x == 0.0 && beta.y == 0.0);
+    // two halves of the C fragment: all loads of a half in flight, then stores
 #pragma unroll
-    for (int c = 0; c < 4; ++c) {
-        int gc = n0 + tn + 16 * c;
-        if (gc >= n) continue;
+    for (int h = 0; h < 2; ++h) {
+        cd cv[8][2];
 #pragma unroll
-        for (int r = 0; r < 8; ++r) {
-            int gr = m0 + tm * 8 + r;
-            if (gr >= m) continue;
-            cd *p = C + (int64_t)gc * ldc + gr;
-            cd v = cmul(alpha, acc[r][c]);
-            if (!beta0) v = cfma(beta, *p, v);
-            *p = v;
+        for (int c = 0; c < 2; ++c) {
+            const int gc = n0 + tn + 16 * (2 * h + c);
+#pragma unroll
+            for (int r = 0; r < 8; ++r) {
+                const int gr = m0 + tm * 8 + r;
+                cv[r][c] = (!beta0 && gc < n && gr < m) ? __ldg(C + (int64_t)gc * ldc + gr)
+                                                        : cmk(0.0, 0.0);
+            }
+        }
+#pragma unroll
+        for (int c = 0; c < 2; ++c) {
+            const int gc = n0 + tn + 16 * (2 * h + c);
+#pragma unroll
+            for (int r = 0; r < 8; ++r) {
+                const int gr = m0 + tm * 8 + r;
+                if (gc < n && gr < m)
+                    C[(int64_t)gc * ldc + gr] = cfma(beta, cv[r][c], cmul(alpha, acc[r][2 * h + c]));
+            }
         }
     }
 }
@@ -373,27 +394,41 @@ int laswp(cudaStream_t s, cd *A, int64_t lda, int64_t sA, int ncols, int jskip0,
     return MNPB_OK;
 }
 
+// Row interchanges piv[c0..c1) applied to the columns [j0, j1) only.
+static int laswp_range(cudaStream_t s, cd *A, int64_t lda, int64_t sA, int j0, int j1,
+                       const int32_t *ipiv, int64_t sP, int c0, int c1, int batch) {
+    if (j1 <= j0 || c1 <= c0) return MNPB_OK;
+    dim3 grid(ceil_div(j1 - j0, 128), batch);
+    ProfScope ps(s, PC_SWAP, 0.0);
+    laswp_kernel<<<grid, 128, 0, s>>>(A, lda, sA, j0, j1, 0, 0, ipiv, sP, c0, c1, 1);
+    MNPB_LAUNCH_CHECK("laswp_kernel");
+    return MNPB_OK;
+}
+
+// Recursive LU: factor columns [off, off+w) over rows [off, n); absolute pivots.
+static int rgetrf(cudaStream_t s, int n, int off, int w, int batch, cd *A, int64_t lda,
+                  int64_t sA, int32_t *ipiv, int64_t sP, int32_t *info) {
+    if (w <= TS) {
+        ProfScope ps(s, PC_PANEL, 8.0 * w * w * (double)(n - off) * batch / 2);
+        panel_kernel<<<batch, PANEL_THREADS, 0, s>>>(n, off, w, A, lda, sA, ipiv, sP, info);
+        MNPB_LAUNCH_CHECK("panel_kernel");
+        return MNPB_OK;
+    }
+    const int w1 = split_point(w);
+    MNPB_TRY(rgetrf(s, n, off, w1, batch, A, lda, sA, ipiv, sP, info));
+    MNPB_TRY(laswp_range(s, A, lda, sA, off + w1, off + w, ipiv, sP, off, off + w1, batch));
+    cd *A11 = A + off + (int64_t)off * lda;
+    cd *A12 = A + off + (int64_t)(off + w1) * lda;
+    MNPB_TRY(trsm_llu(s, w1, w - w1, batch, A11, lda, sA, A12, lda, sA));
+    MNPB_TRY(zgemm(s, n - off - w1, w - w1, w1, batch, cmk(-1, 0), A11 + w1, lda, sA, A12, lda,
+                   sA, cmk(1, 0), A12 + w1, lda, sA));
+    MNPB_TRY(rgetrf(s, n, off + w1, w - w1, batch, A, lda, sA, ipiv, sP, info));
+    return laswp_range(s, A, lda, sA, off, off + w1, ipiv, sP, off + w1, off + w, batch);
+}
+
 int getrf(cudaStream_t s, int n, int batch, cd *A, int64_t lda, int64_t sA, int32_t *ipiv,
           int64_t sP, int32_t *info) {
-    const int nb = TS;
-    for (int k = 0; k < n; k += nb) {
-        const int kb = (n - k < nb) ? (n - k) : nb;
-        {
-            ProfScope ps(s, PC_PANEL, 8.0 * kb * kb * (double)(n - k) * batch / 2);
-            panel_kernel<<<batch, PANEL_THREADS, 0, s>>>(n, k, kb, A, lda, sA, ipiv, sP, info);
-            MNPB_LAUNCH_CHECK("panel_kernel");
-        }
-        MNPB_TRY(laswp(s, A, lda, sA, n, k, k + kb, ipiv, sP, k, k + kb, true, batch));
-        const int rest = n - k - kb;
-        if (rest > 0) {
-            cd *A11 = A + k + (int64_t)k * lda;
-            cd *A12 = A + k + (int64_t)(k + kb) * lda;
-            MNPB_TRY(trsm_small(s, 0, kb, A11, lda, sA, A12, lda, sA, rest, batch));
-            MNPB_TRY(zgemm(s, rest, rest, kb, batch, cmk(-1, 0), A11 + kb, lda, sA, A12, lda, sA,
-                           cmk(1, 0), A12 + kb, lda, sA));
-        }
-    }
-    return MNPB_OK;
+    return rgetrf(s, n, 0, n, batch, A, lda, sA, ipiv, sP, info);
 }
 
 int getrs(cudaStream_t s, int n, int nrhs, int batch, const cd *LU, int64_t lda, int64_t sA,

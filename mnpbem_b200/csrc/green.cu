@@ -308,6 +308,16 @@ struct StoreC32P {
     }
 };
 
+struct StoreBoth {
+    StoreC128 a;
+    StoreC32P b;
+    __device__ __forceinline__ void put(int64_t bb, int64_t i, int64_t j, cd g1, cd h1, cd g2,
+                                        cd h2) const {
+        a.put(bb, i, j, g1, h1, g2, h2);
+        b.put(bb, i, j, g1, h1, g2, h2);
+    }
+};
+
 // Far-field formula for one entry and one wavenumber (greenret_refined.py:738,
 // 764-767, 745): G = a/d e^{ikd}, F = (nx faux x + ny faux y + nz faux z) a e^{ikd}
 // with faux = (ik - 1/d)/d^2.
@@ -538,6 +548,44 @@ extern "C" int mnpb_assemble_ret(void *stream, int64_t n, int64_t batch, const d
     } else {
         set_error("assemble_ret: unknown out_mode %d", out_mode);
         return MNPB_EINVAL;
+    }
+    return MNPB_OK;
+}
+
+extern "C" int mnpb_assemble_ret2(void *stream, int64_t n, int64_t batch, const double *pos,
+                                  const double *nvec, const double *area, int nparts,
+                                  const int64_t *poff, const double *kblk, const double *sblk,
+                                  int64_t nref, const int32_t *rows, const int32_t *cols,
+                                  const double *g, const double *fn, double *G1, double *H1,
+                                  double *G2, double *H2, int64_t ld, int64_t stride, float *G1p,
+                                  float *H1p, float *G2p, float *H2p, int64_t ldp,
+                                  int64_t stridep, int64_t planep) {
+    clear_error();
+    MNPB_REQUIRE(n > 0 && batch > 0 && ld >= n && ldp >= n && n < 65536 && batch < 65536,
+                 "assemble_ret2: bad sizes");
+    MNPB_REQUIRE(nparts >= 1 && nparts <= kMaxParts, "assemble_ret2: nparts must be 1..%d",
+                 kMaxParts);
+    MNPB_REQUIRE(pos && nvec && area && poff && kblk && sblk && G1 && H1 && G2 && H2 && G1p &&
+                     H1p && G2p && H2p,
+                 "assemble_ret2: null pointer");
+    MNPB_REQUIRE(stride >= ld * n && planep >= ldp * n && stridep >= 2 * planep,
+                 "assemble_ret2: strides too small");
+    PartTable parts;
+    parts.nparts = nparts;
+    for (int p = 0; p <= nparts; ++p) parts.off[p] = poff[p];
+    MNPB_REQUIRE(parts.off[0] == 0 && parts.off[nparts] == n, "assemble_ret2: bad offsets");
+    cudaStream_t s = as_stream(stream);
+    StoreBoth st{StoreC128{(cd *)G1, (cd *)H1, (cd *)G2, (cd *)H2, ld, stride},
+                 StoreC32P{G1p, H1p, G2p, H2p, ldp, stridep, planep}};
+    dim3 grid(ceil_div(n, 128), (unsigned)n, (unsigned)batch);
+    ProfScope ps(s, PC_ASSEMBLE, 96.0 * (double)n * n * batch + 96.0 * (double)nref);
+    assemble_far_kernel<StoreBoth><<<grid, 128, 0, s>>>(n, parts, pos, nvec, area, kblk, sblk, st);
+    MNPB_LAUNCH_CHECK("assemble_far_kernel<both>");
+    const int64_t tot = nref * batch;
+    if (tot > 0) {
+        assemble_refined_kernel<StoreBoth><<<ceil_div(tot, 128), 128, 0, s>>>(
+            nref, batch, parts, pos, kblk, sblk, rows, cols, g, fn, st);
+        MNPB_LAUNCH_CHECK("assemble_refined_kernel<both>");
     }
     return MNPB_OK;
 }

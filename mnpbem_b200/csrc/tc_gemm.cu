@@ -1,0 +1,453 @@
+// Complex GEMM on the 5th-generation tensor cores (tcgen05, sm_100a), TF32
+// inputs with FP32 accumulation in tensor memory.
+//
+//   C = beta C + alpha A B      (planar complex FP32, column-major, batched)
+//
+// Cr = Ar Br - Ai Bi and Ci = Ar Bi + Ai Br are accumulated in two TMEM
+// accumulators (128 lanes x 128 columns each); the -Ai Bi product uses the
+// negate-A bit of the instruction descriptor.  B tiles (K x 128, K contiguous
+// in a column-major matrix: K-major) are loaded by TMA straight from the
+// caller's matrix; A is first packed K-major (a transpose) with
+// round-to-nearest TF32 conversion, since a column-major A is MN-major.
+//
+// One CTA computes one 128 x 128 output tile: warp 0 / lane 0 issues the TMA
+// loads of a 3-stage ring, warp 1 / lane 0 issues the MMAs, then all four
+// warps read the accumulators (warp w owns TMEM lanes 32w..32w+31, i.e. rows
+// 32w..32w+31 of the tile) and apply the epilogue to C.  Every mbarrier wait
+// is bounded: on timeout the kernel records an error, still frees its tensor
+// memory and returns.
+#include "common.cuh"
+#include "tc_gemm.cuh"
+
+#include <cuda.h>
+#include <mutex>
+
+namespace mnpb {
+namespace tc {
+
+constexpr int BM = 128, BN = 128, BK = 32;   // BK: TF32 elements per 128-byte row
+constexpr int STAGES = 3;
+constexpr int TILE_BYTES = BM * BK * 4;        // 16 KB (same for the B tile, BN == BM)
+constexpr int STAGE_BYTES = 4 * TILE_BYTES;    // Ar, Ai, Br, Bi
+constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 + 256;
+constexpr int TMEM_COLS = 256;
+constexpr uint64_t WAIT_NS = 2000000000ull;    // a wait gives up after 2 s
+
+__device__ int g_tc_error;                     // first timeout code seen (0 = none)
+
+// ---------------------------------------------------------------------------
+// PTX helpers
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count));
+}
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ uint64_t global_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+    return t;
+}
+// Bounded parity wait (WAIT_NS of wall time); returns false on timeout.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+    const uint64_t t0 = global_ns();
+    while (true) {
+        uint32_t ok;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(ok)
+            : "r"(bar), "r"(parity)
+            : "memory");
+        if (ok) return true;
+        if (global_ns() - t0 > WAIT_NS) return false;
+    }
+}
+__device__ __forceinline__ void tma_load_3d(uint32_t dst, const CUtensorMap *map, uint32_t bar,
+                                            int c0, int c1, int c2) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes "
+        "[%0], [%1, {%3, %4, %5}], [%2];" ::"r"(dst),
+        "l"((uint64_t)map), "r"(bar), "r"(c0), "r"(c1), "r"(c2)
+        : "memory");
+}
+// K-major operand tile in shared memory, 128-byte swizzle, 8-row groups 1024 B apart.
+__device__ __forceinline__ uint64_t smem_desc_k128(uint32_t addr) {
+    uint64_t d = 0;
+    d |= (uint64_t)((addr >> 4) & 0x3FFF);          // start address
+    d |= (uint64_t)1 << 16;                          // leading byte offset (unused, 16 B)
+    d |= (uint64_t)(1024 >> 4) << 32;                // stride byte offset: 8 rows x 128 B
+    d |= (uint64_t)1 << 46;                          // descriptor version (sm_100)
+    d |= (uint64_t)2 << 61;                          // swizzle: 128 B
+    return d;
+}
+// Instruction descriptor: TF32 x TF32 -> F32, both K-major, M = 128, N = 128.
+__host__ __device__ constexpr uint32_t idesc_tf32(bool neg_a) {
+    return (1u << 4)                    // D format F32
+         | (2u << 7) | (2u << 10)       // A, B format TF32
+         | ((neg_a ? 1u : 0u) << 13)    // negate A
+         | ((uint32_t)(BN >> 3) << 17)  // N / 8
+         | ((uint32_t)(BM >> 4) << 24); // M / 16
+}
+__device__ __forceinline__ void mma_tf32(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t idesc,
+                                         uint32_t acc) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
+        "l"(a), "l"(b), "r"(idesc), "r"(acc)
+        : "memory");
+}
+__device__ __forceinline__ void mma_commit(uint32_t bar) {
+    asm volatile(
+        "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
+        : "memory");
+}
+__device__ __forceinline__ void fence_before() {
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void fence_after() {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
+    uint32_t r[32];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+        "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, "
+        "%16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, "
+        "[%32];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+          "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]),
+          "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]),
+          "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]),
+          "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]),
+          "=r"(r[31])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+struct Epi {
+    float *C;
+    int64_t ldc, planeC, strideC;
+    float alpha, beta;
+    int M, N, ktiles;
+};
+
+__global__ void __launch_bounds__(128, 1)
+    cgemm_tf32_kernel(const __grid_constant__ CUtensorMap tmA,
+                      const __grid_constant__ CUtensorMap tmBr,
+                      const __grid_constant__ CUtensorMap tmBi, Epi ep) {
+    extern __shared__ __align__(1024) uint8_t smem_raw[];
+    // 1024-byte alignment for the swizzled tiles
+    uint8_t *smem = (uint8_t *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+    uint64_t *bars = (uint64_t *)(smem + STAGES * STAGE_BYTES);
+    // bars[0..S): full, bars[S..2S): empty, bars[2S]: accumulator ready
+    uint32_t *tmem_slot = (uint32_t *)(bars + 2 * STAGES + 1);
+    volatile int *abort_flag = (volatile int *)(tmem_slot + 1);
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN, b = blockIdx.z;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < STAGES; ++s) {
+            mbar_init(smem_u32(&bars[s]), 1);
+            mbar_init(smem_u32(&bars[STAGES + s]), 1);
+        }
+        mbar_init(smem_u32(&bars[2 * STAGES]), 1);
+        *abort_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                         smem_u32(tmem_slot)),
+                     "r"(TMEM_COLS)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    fence_before();
+    __syncthreads();
+    fence_after();
+    const uint32_t tmem = *tmem_slot;
+    const uint32_t d_re = tmem, d_im = tmem + BN;
+    const int KT = ep.ktiles;
+
+    if (warp == 0 && lane == 0) {
+        // TMA producer
+        for (int kt = 0; kt < KT; ++kt) {
+            const int s = kt % STAGES;
+            if (kt >= STAGES) {
+                if (!mbar_wait(smem_u32(&bars[STAGES + s]), ((kt / STAGES) - 1) & 1)) {
+                    atomicCAS(&g_tc_error, 0, 1);
+                    *abort_flag = 1;
+                    break;
+                }
+            }
+            if (*abort_flag) break;
+            uint8_t *st = smem + s * STAGE_BYTES;
+            const uint32_t full = smem_u32(&bars[s]);
+            mbar_expect_tx(full, STAGE_BYTES);
+            const int k0 = kt * BK;
+            tma_load_3d(smem_u32(st), &tmA, full, k0, m0, 2 * b);
+            tma_load_3d(smem_u32(st + TILE_BYTES), &tmA, full, k0, m0, 2 * b + 1);
+            tma_load_3d(smem_u32(st + 2 * TILE_BYTES), &tmBr, full, k0, n0, b);
+            tma_load_3d(smem_u32(st + 3 * TILE_BYTES), &tmBi, full, k0, n0, b);
+        }
+    } else if (warp == 1 && lane == 0) {
+        // MMA issuer
+        constexpr uint32_t ID = idesc_tf32(false), IDN = idesc_tf32(true);
+        for (int kt = 0; kt < KT; ++kt) {
+            const int s = kt % STAGES;
+            if (!mbar_wait(smem_u32(&bars[s]), (kt / STAGES) & 1)) {
+                atomicCAS(&g_tc_error, 0, 2);
+                *abort_flag = 1;
+                break;
+            }
+            fence_after();
+            const uint32_t st = smem_u32(smem + s * STAGE_BYTES);
+#pragma unroll
+            for (int j = 0; j < BK / 8; ++j) {      // 8 TF32 = 32 bytes per MMA
+                const uint32_t off = 32 * j;
+                const uint64_t ar = smem_desc_k128(st + off);
+                const uint64_t ai = smem_desc_k128(st + TILE_BYTES + off);
+                const uint64_t br = smem_desc_k128(st + 2 * TILE_BYTES + off);
+                const uint64_t bi = smem_desc_k128(st + 3 * TILE_BYTES + off);
+                const uint32_t acc = (kt > 0 || j > 0) ? 1u : 0u;
+                mma_tf32(d_re, ar, br, ID, acc);
+                mma_tf32(d_re, ai, bi, IDN, 1u);
+                mma_tf32(d_im, ar, bi, ID, acc);
+                mma_tf32(d_im, ai, br, ID, 1u);
+            }
+            mma_commit(smem_u32(&bars[STAGES + s]));   // frees this stage when done
+        }
+        // accumulator ready (or abort) -- commit tracks all MMAs issued above
+        mma_commit(smem_u32(&bars[2 * STAGES]));
+    }
+    __syncwarp();
+
+    // epilogue: all four warps
+    const bool acc_ok = mbar_wait(smem_u32(&bars[2 * STAGES]), 0);
+    if (!acc_ok) atomicCAS(&g_tc_error, 0, 3);
+    fence_after();
+    const bool good = acc_ok && (*abort_flag == 0);
+    const int row = m0 + warp * 32 + lane;
+    float *Cr = ep.C + (int64_t)b * ep.strideC;
+    float *Ci = Cr + ep.planeC;
+    const uint32_t lane_base = (uint32_t)(warp * 32) << 16;
+    const bool row_ok = good && row < ep.M;
+    for (int c0 = 0; c0 < BN; c0 += 32) {
+        float vr[32], vi[32];
+        tmem_ld32(d_re + lane_base + c0, vr);
+        tmem_ld32(d_im + lane_base + c0, vi);
+        const int ncol = min(32, ep.N - (n0 + c0));
+        if (!row_ok || ncol <= 0) continue;
+        const int64_t o0 = (int64_t)(n0 + c0) * ep.ldc + row;
+        if (ep.beta != 0.f) {
+            // issue every load of C before any store so the loads overlap
+            float cr[32], ci[32];
+#pragma unroll
+            for (int c = 0; c < 32; ++c) {
+                cr[c] = c < ncol ? __ldg(Cr + o0 + (int64_t)c * ep.ldc) : 0.f;
+                ci[c] = c < ncol ? __ldg(Ci + o0 + (int64_t)c * ep.ldc) : 0.f;
+            }
+#pragma unroll
+            for (int c = 0; c < 32; ++c) {
+                vr[c] = fmaf(ep.beta, cr[c], ep.alpha * vr[c]);
+                vi[c] = fmaf(ep.beta, ci[c], ep.alpha * vi[c]);
+            }
+        } else {
+#pragma unroll
+            for (int c = 0; c < 32; ++c) {
+                vr[c] *= ep.alpha;
+                vi[c] *= ep.alpha;
+            }
+        }
+#pragma unroll
+        for (int c = 0; c < 32; ++c) {
+            if (c < ncol) {
+                Cr[o0 + (int64_t)c * ep.ldc] = vr[c];
+                Ci[o0 + (int64_t)c * ep.ldc] = vi[c];
+            }
+        }
+    }
+    fence_before();
+    __syncthreads();
+    if (warp == 0) {
+        fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                     "r"(TMEM_COLS)
+                     : "memory");
+    }
+}
+
+// Pack a column-major planar complex A (M x K) into K-major TF32 tiles:
+// out[b][plane][Mp][Kp], zero outside M x K, round to nearest TF32.
+__global__ void pack_a_tf32_kernel(const float *__restrict__ A, int64_t lda, int64_t planeA,
+                                   int64_t strideA, int M, int K, int Mp, int Kp,
+                                   float *__restrict__ out) {
+    __shared__ float tile[32][33];
+    const int b = blockIdx.z >> 1, pl = blockIdx.z & 1;
+    const int mb = blockIdx.x * 32, kb = blockIdx.y * 32;
+    const float *src = A + (int64_t)b * strideA + (int64_t)pl * planeA;
+    // read: 32 k-columns x 32 m (m contiguous)
+    for (int j = threadIdx.y; j < 32; j += blockDim.y) {
+        const int m = mb + threadIdx.x, k = kb + j;
+        float v = (m < M && k < K) ? src[(int64_t)k * lda + m] : 0.f;
+        uint32_t t;
+        asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(t) : "f"(v));
+        tile[j][threadIdx.x] = __uint_as_float(t);
+    }
+    __syncthreads();
+    float *dst = out + ((int64_t)b * 2 + pl) * (int64_t)Mp * Kp;
+    for (int i = threadIdx.y; i < 32; i += blockDim.y) {
+        const int m = mb + i, k = kb + threadIdx.x;
+        if (m < Mp && k < Kp) dst[(int64_t)m * Kp + k] = tile[threadIdx.x][i];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------
+typedef CUresult (*EncodeFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *,
+                             const cuuint64_t *, const cuuint64_t *, const cuuint32_t *,
+                             const cuuint32_t *, CUtensorMapInterleave, CUtensorMapSwizzle,
+                             CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+static EncodeFn get_encode() {
+    static EncodeFn fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
+                cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = (EncodeFn)p;
+    });
+    return fn;
+}
+
+// 3-D FP32 map: inner dim d0 (contiguous), rows d1 (stride s1 elements),
+// planes/batch d2 (stride s2 elements); box 32 x 128 x 1, 128-byte swizzle.
+static int make_map(CUtensorMap *map, const float *base, uint64_t d0, uint64_t d1, uint64_t d2,
+                    uint64_t s1, uint64_t s2) {
+    EncodeFn enc = get_encode();
+    if (!enc) {
+        set_error("tc_gemm: cuTensorMapEncodeTiled unavailable");
+        return MNPB_ECUDA;
+    }
+    if (((uintptr_t)base & 15) || ((s1 * 4) & 15) || ((s2 * 4) & 15)) {
+        set_error("tc_gemm: operand not 16-byte aligned (base %p, strides %llu %llu)", base,
+                  (unsigned long long)s1, (unsigned long long)s2);
+        return MNPB_EINVAL;
+    }
+    cuuint64_t dims[3] = {d0, d1, d2};
+    cuuint64_t strides[2] = {s1 * 4, s2 * 4};
+    cuuint32_t box[3] = {BK, BM, 1};
+    cuuint32_t estr[3] = {1, 1, 1};
+    CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, (void *)base, dims, strides, box,
+                     estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                     CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) {
+        set_error("tc_gemm: cuTensorMapEncodeTiled failed (%d)", (int)r);
+        return MNPB_ECUDA;
+    }
+    return MNPB_OK;
+}
+
+int64_t cgemm_tf32_workspace(int M, int K, int batch) {
+    const int64_t Mp = (M + BM - 1) / BM * BM, Kp = (K + BK - 1) / BK * BK;
+    return (int64_t)batch * 2 * Mp * Kp * 4;
+}
+
+int cgemm_tf32(cudaStream_t s, int M, int N, int K, int batch, float alpha, CMatF A, CMatF B,
+               float beta, CMatF C, float *work, int64_t work_bytes) {
+    if (M <= 0 || N <= 0 || batch <= 0) return MNPB_OK;
+    if (K <= 0) {
+        set_error("tc_gemm: K must be positive");
+        return MNPB_EINVAL;
+    }
+    static bool attr_set = false;
+    if (!attr_set) {
+        if (cudaFuncSetAttribute(cgemm_tf32_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 SMEM_BYTES) != cudaSuccess) {
+            set_error("tc_gemm: cannot set shared memory size");
+            return MNPB_ECUDA;
+        }
+        attr_set = true;
+    }
+    const int Mp = (M + BM - 1) / BM * BM, Kp = (K + BK - 1) / BK * BK;
+    if (work_bytes < cgemm_tf32_workspace(M, K, batch)) {
+        set_error("tc_gemm: workspace too small");
+        return MNPB_ENOMEM;
+    }
+    {
+        dim3 g(Mp / 32, Kp / 32, batch * 2), t(32, 8);
+        ProfScope ps(s, PC_ELEM, 0.0);
+        pack_a_tf32_kernel<<<g, t, 0, s>>>(A.p, A.ld, A.plane, A.stride, M, K, Mp, Kp, work);
+        MNPB_LAUNCH_CHECK("pack_a_tf32_kernel");
+    }
+    CUtensorMap mA, mBr, mBi;
+    MNPB_TRY(make_map(&mA, work, Kp, Mp, (uint64_t)batch * 2, Kp, (uint64_t)Mp * Kp));
+    MNPB_TRY(make_map(&mBr, B.p, K, N, batch, B.ld, B.stride));
+    MNPB_TRY(make_map(&mBi, B.p + B.plane, K, N, batch, B.ld, B.stride));
+    Epi ep{C.p, C.ld, C.plane, C.stride, alpha, beta, M, N, Kp / BK};
+    dim3 grid(Mp / BM, (N + BN - 1) / BN, batch);
+    ProfScope ps(s, PC_TCGEMM, 8.0 * M * N * (double)K * batch);
+    cgemm_tf32_kernel<<<grid, 128, SMEM_BYTES, s>>>(mA, mBr, mBi, ep);
+    MNPB_LAUNCH_CHECK("cgemm_tf32_kernel");
+    return MNPB_OK;
+}
+
+int tc_error_read_and_clear(cudaStream_t s, int *code) {
+    int v = 0, z = 0;
+    if (cudaMemcpyFromSymbolAsync(&v, g_tc_error, sizeof(int), 0, cudaMemcpyDeviceToHost, s) !=
+            cudaSuccess ||
+        cudaMemcpyToSymbolAsync(g_tc_error, &z, sizeof(int), 0, cudaMemcpyHostToDevice, s) !=
+            cudaSuccess ||
+        cudaStreamSynchronize(s) != cudaSuccess) {
+        set_error("tc_gemm: cannot read the error word");
+        return MNPB_ECUDA;
+    }
+    *code = v;
+    return MNPB_OK;
+}
+
+}  // namespace tc
+}  // namespace mnpb
+
+using namespace mnpb;
+
+extern "C" int64_t mnpb_cgemm_tf32_workspace(int64_t m, int64_t k, int64_t batch) {
+    return tc::cgemm_tf32_workspace((int)m, (int)k, (int)batch);
+}
+
+extern "C" int mnpb_cgemm_tf32(void *stream, int64_t m, int64_t n, int64_t k, int64_t batch,
+                               float alpha, const float *A, int64_t lda, int64_t planeA,
+                               int64_t sA, const float *B, int64_t ldb, int64_t planeB,
+                               int64_t sB, float beta, float *C, int64_t ldc, int64_t planeC,
+                               int64_t sC, void *work, int64_t work_bytes) {
+    clear_error();
+    MNPB_REQUIRE(m >= 0 && n >= 0 && k > 0 && batch > 0 && batch < 65536,
+                 "cgemm_tf32: bad sizes");
+    MNPB_REQUIRE(A && B && C && work, "cgemm_tf32: null pointer");
+    tc::CMatF a{(float *)A, lda, planeA, sA}, b{(float *)B, ldb, planeB, sB}, c{C, ldc, planeC, sC};
+    return tc::cgemm_tf32(as_stream(stream), (int)m, (int)n, (int)k, (int)batch, alpha, a, b,
+                          beta, c, (float *)work, work_bytes);
+}
+
+extern "C" int mnpb_tc_error(void *stream, int32_t *code) {
+    clear_error();
+    MNPB_REQUIRE(code, "tc_error: null pointer");
+    int v = 0;
+    MNPB_TRY(tc::tc_error_read_and_clear(as_stream(stream), &v));
+    *code = v;
+    return MNPB_OK;
+}

@@ -1,0 +1,25 @@
+// Tensor-core complex GEMM (tcgen05, TF32 inputs, FP32 accumulation).
+#pragma once
+#include "common.cuh"
+
+namespace mnpb {
+namespace tc {
+
+// Planar complex FP32 matrix view: real plane at p, imaginary plane at
+// p + plane, column-major with leading dimension ld, batch stride `stride`.
+struct CMatF {
+    float *p;
+    int64_t ld, plane, stride;
+    __host__ __device__ CMatF sub(int64_t r, int64_t c) const {
+        return CMatF{p + c * ld + r, ld, plane, stride};
+    }
+};
+
+int64_t cgemm_tf32_workspace(int M, int K, int batch);
+// C = beta C + alpha A B (A: M x K, B: K x N, C: M x N), work >= cgemm_tf32_workspace.
+int cgemm_tf32(cudaStream_t s, int M, int N, int K, int batch, float alpha, CMatF A, CMatF B,
+               float beta, CMatF C, float *work, int64_t work_bytes);
+int tc_error_read_and_clear(cudaStream_t s, int *code);
+
+}  // namespace tc
+}  // namespace mnpb

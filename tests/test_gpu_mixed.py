@@ -1,0 +1,101 @@
+"""Mixed-precision path: TF32 tensor-core LU of planar FP32 matrices (relative
+error of a cond ~ 3 solve below 1e-2: TF32 keeps 10 mantissa bits), and the
+mixed BEMRet (TF32 factorisations + FP64 iterative refinement) against the
+reference's golden fixtures.  Tolerances: the refined solution is held to the
+FP64 operator's relative residual 1e-11, so sigma agrees with the reference
+to 1e-9 and extinction / scattering to 1e-9 (1e-6)."""
+import numpy as np
+import pytest
+import torch
+
+from conftest import golden
+import mnpbem_b200 as M
+from mnpbem_b200 import _lib, bem, excitation
+from mnpbem_b200._lib import call, ptr
+
+pytestmark = pytest.mark.gpu
+EPS = [M.EpsConst(1.0), M.EpsDrude(10.0, 9.065, 0.0708)]
+
+
+def _cp(key):
+    v, f = M.load_mesh(key)
+    s = M.Particle(v, f, interp='curv' if f.shape[1] == 9 else 'flat')
+    return M.ComParticle(EPS, [s], [[2, 1]]), s
+
+
+def rel(a, b):
+    return np.abs(np.asarray(a) - np.asarray(b)).max() / np.abs(np.asarray(b)).max()
+
+
+@pytest.mark.parametrize('n,batch,nrhs', [(32, 1, 1), (100, 2, 3), (256, 3, 5), (300, 1, 40)])
+def test_getrf_getrs_c32p(gpu_ok, n, batch, nrhs):
+    ld = (n + 3) // 4 * 4
+    g = torch.Generator().manual_seed(7)
+    # well conditioned (cond ~ 3): the TF32 updates bound the accuracy
+    Ac = (torch.randn((batch, n, n), generator=g, dtype=torch.float64) +
+          1j * torch.randn((batch, n, n), generator=g, dtype=torch.float64)) / (2 * n ** 0.5)
+    Ac = Ac + 2 * torch.eye(n)
+    X = (torch.randn((batch, n, nrhs), generator=g, dtype=torch.float64) +
+         1j * torch.randn((batch, n, nrhs), generator=g, dtype=torch.float64))
+    Bc = Ac @ X
+    A = torch.zeros((batch, 2, n, ld), dtype=torch.float32)
+    A[:, 0, :, :n] = Ac.real.transpose(1, 2).float()
+    A[:, 1, :, :n] = Ac.imag.transpose(1, 2).float()
+    B = torch.zeros((batch, 2, nrhs, n), dtype=torch.float32)
+    B[:, 0] = Bc.real.transpose(1, 2).float()
+    B[:, 1] = Bc.imag.transpose(1, 2).float()
+    A, B = A.cuda(), B.cuda()
+    piv = torch.zeros((batch, n), dtype=torch.int32, device='cuda')
+    info = torch.zeros(batch, dtype=torch.int32, device='cuda')
+    wb = int(_lib.lib().mnpb_f32_workspace(n, batch))
+    work = torch.empty(wb, dtype=torch.uint8, device='cuda')
+    sh = _lib.stream_handle()
+    call('mnpb_getrf_c32p', sh, n, batch, ptr(A), ld, n * ld, 2 * n * ld, ptr(piv), n, ptr(info),
+         ptr(work), wb)
+    call('mnpb_getrs_c32p', sh, n, batch, nrhs, ptr(A), ld, n * ld, 2 * n * ld, ptr(piv), n,
+         ptr(B), n, n * nrhs, 2 * n * nrhs, ptr(work), wb)
+    torch.cuda.synchronize()
+    assert info.sum().item() == 0
+    Xg = (B[:, 0].double() + 1j * B[:, 1].double()).transpose(1, 2).cpu()
+    err = ((Xg - X).abs().pow(2).sum() / X.abs().pow(2).sum()).sqrt().item()
+    assert err < 1e-2, err
+
+
+@pytest.fixture(scope='module')
+def tiny():
+    cp, s = _cp('trisphere_32_10')
+    return cp, bem.BEMRet(cp, precision='mixed'), golden('golden_tiny')
+
+
+def test_mixed_bemret_tiny(gpu_ok, tiny):
+    cp, b, z = tiny
+    exc = excitation.PlaneWaveRet(pol=[[1, 0, 0], [0, 1, 0]], dir=[[0, 0, 1], [0, 0, 1]])
+    for i, lam in enumerate(z['lams']):
+        sig, _ = b.solve(exc.potential(cp, lam))
+        assert rel(sig.sig1, z['sig1_%d' % i]) < 1e-9
+        assert rel(sig.sig2, z['sig2_%d' % i]) < 1e-9
+        assert rel(sig.h1, z['h1_%d' % i]) < 1e-7
+        assert np.allclose(exc.extinction(sig), z['ext_%d' % i], rtol=1e-9)
+        assert b._batch.relres.max() < 1e-11
+
+
+def test_mixed_c0_spectrum(gpu_ok):
+    cp, s = _cp('trisphere_144_20')
+    z = golden('golden_c0')
+    b = bem.BEMRet(cp, precision='mixed')
+    exc = excitation.PlaneWaveRet(pol=[[1, 0, 0]], dir=[[0, 0, 1]])
+    sols = b.solve_spectrum(exc, list(z['lams']), batch=41)
+    ext = np.array([exc.extinction(sg) for sg in sols])
+    sca = np.array([exc.scattering(sg)[0] for sg in sols])
+    assert np.max(np.abs(ext - z['ext']) / np.abs(z['ext'])) < 1e-9
+    assert np.max(np.abs(sca - z['sca']) / np.abs(z['sca'])) < 1e-9
+
+
+def test_mixed_c1_2884_faces(gpu_ok):
+    cp, s = _cp('trisphere_1444_40')
+    z = golden('golden_c1')
+    b = bem.BEMRet(cp, precision='mixed')
+    exc = excitation.PlaneWaveRet(pol=[[1, 0, 0]], dir=[[0, 0, 1]])
+    sols = b.solve_spectrum(exc, list(z['lams']), batch=3)
+    ext = np.array([exc.extinction(sg) for sg in sols])
+    assert np.max(np.abs(ext - z['ext']) / np.abs(z['ext'])) < 1e-6
