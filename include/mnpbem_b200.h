@@ -52,7 +52,9 @@ int64_t mnpb_launch_count(void);
  * bracketed by CUDA events on its stream.  mnpb_prof_end synchronises and
  * returns, per kernel class (0 assembly, 1 refinement quadrature, 2 FP64
  * GEMM, 3 LU panel, 4 small triangular solves, 5 row/column swaps,
- * 6 element-wise, 7 tensor-core GEMM, 8 far field, 9 FP32 GEMM, 10 matvec),
+ * 6 element-wise, 7 tensor-core GEMM, 8 far field, 9 FP32 GEMM, 10 matvec,
+ * 11 one-launch triangular solves, 12 tensor-core operand packing,
+ * 13 refinement element-wise),
  * the summed device time in ms, the summed algorithmic work (flops or bytes,
  * see the kernel) and the number of launches. */
 int mnpb_prof_begin(void);

@@ -107,7 +107,8 @@ def launch_count():
 
 
 PROF_CLASSES = ['assemble', 'refine', 'zgemm_f64', 'lu_panel', 'trsm_small', 'swap',
-                'elementwise', 'tc_gemm', 'farfield', 'sgemm_f32', 'matvec']
+                'elementwise', 'tc_gemm', 'farfield', 'sgemm_f32', 'matvec', 'trsv',
+                'tc_pack', 'refine_elementwise']
 
 
 def prof_begin():

@@ -218,12 +218,14 @@ struct DinvOff {
 
 static int convert_in(cudaStream_t s, int n, int m, int batch, const cd *X, int64_t sx, float *Y) {
     dim3 g(ceil_div((int64_t)n * m, 256), batch);
+    ProfScope ps(s, PC_REFINE_EW, 0.0);
     to_f32p<<<g, 256, 0, s>>>(n, m, X, sx, Y, 2 * (int64_t)n * m);
     MNPB_LAUNCH_CHECK("to_f32p");
     return MNPB_OK;
 }
 static int convert_out(cudaStream_t s, int n, int m, int batch, const float *Y, cd *X, int64_t sx) {
     dim3 g(ceil_div((int64_t)n * m, 256), batch);
+    ProfScope ps(s, PC_REFINE_EW, 0.0);
     from_f32p<<<g, 256, 0, s>>>(n, m, Y, 2 * (int64_t)n * m, X, sx);
     MNPB_LAUNCH_CHECK("from_f32p");
     return MNPB_OK;

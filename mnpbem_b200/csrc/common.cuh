@@ -62,6 +62,9 @@ enum ProfClass {
     PC_FARFIELD = 8,
     PC_SGEMM = 9,
     PC_MATVEC = 10,    // work = bytes read
+    PC_TRSV = 11,      // one-launch triangular solves, work = bytes of the triangle
+    PC_PACK = 12,      // tensor-core operand packing
+    PC_REFINE_EW = 13, // refinement element-wise kernels (residual, norms, conversions)
     PC_COUNT = 16
 };
 bool prof_on();

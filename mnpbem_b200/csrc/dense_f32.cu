@@ -655,7 +655,7 @@ static int trsv(Ctx &c, bool lower, int n, int m, CMatF T, const float *inv, CMa
         return MNPB_ECUDA;
     }
     const int grid = nb * c.batch;
-    ProfScope ps(c.s, PC_TRSM, 4.0 * (double)n * n * c.batch);   // bytes of the triangle
+    ProfScope ps(c.s, PC_TRSV, 4.0 * (double)n * n * c.batch);   // bytes of the triangle
 #define MNPB_TRSV(NC)                                                                          \
     trsv_kernel<NC><<<grid, 256, 0, c.s>>>(n, m, lower ? 1 : 0, T.p, T.ld, T.plane, T.stride,   \
                                            inv, X.p, X.ld, X.plane, X.stride, g_flags,          \

@@ -390,7 +390,7 @@ int cgemm_tf32(cudaStream_t s, int M, int N, int K, int batch, float alpha, CMat
     }
     {
         dim3 g(Mp / 32, Kp / 32, batch * 2), t(32, 8);
-        ProfScope ps(s, PC_ELEM, 0.0);
+        ProfScope ps(s, PC_PACK, 8.0 * (double)M * K * batch);
         pack_a_tf32_kernel<<<g, t, 0, s>>>(A.p, A.ld, A.plane, A.stride, M, K, Mp, Kp, work);
         MNPB_LAUNCH_CHECK("pack_a_tf32_kernel");
     }
