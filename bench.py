@@ -52,6 +52,7 @@ def parse():
     ap.add_argument('--batch', type=int, default=81)
     ap.add_argument('--nlam', type=int, default=81)
     ap.add_argument('--no-cpu-baseline', action='store_true')
+    ap.add_argument('--prof-dump', default=None, help='CSV of every timed launch')
     return ap.parse_args()
 
 
@@ -249,6 +250,8 @@ def main():
     if world > 1:
         dist.barrier()
     prof = _lib.prof_end()
+    if args.prof_dump:
+        _lib.call('mnpb_prof_dump', args.prof_dump.encode())
     launches = _lib.launch_count() - launches0
     ck = clocks.stop()
     ms = ev0.elapsed_time(ev1)

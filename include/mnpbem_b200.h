@@ -59,6 +59,9 @@ int64_t mnpb_launch_count(void);
  * see the kernel) and the number of launches. */
 int mnpb_prof_begin(void);
 int mnpb_prof_end(int ncls, double *ms, double *work, int64_t *count);
+/* Write every launch of the last profiled interval to a CSV file
+ * (class, ms, work, shape tag). */
+int mnpb_prof_dump(const char *path);
 
 /* ---------------------------------------------------------------------------
  * Geometry set-up (once per particle mesh)

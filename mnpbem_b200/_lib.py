@@ -22,6 +22,7 @@ SIGNATURES = {
     'mnpb_launch_count': [],
     'mnpb_prof_begin': [],
     'mnpb_prof_end': [_I, _P, _P, _P],
+    'mnpb_prof_dump': [C.c_char_p],
     'mnpb_refinematrix': [_I64, _I64, _P, _P, _P, _P, _D, _D, _I64, _P, _P, _P, _P],
     'mnpb_refine_coefficients': [_P, _I64, _P, _P, _P, _P, _I64, _P, _P, _P, _P, _P, _P, _P,
                                  _P, _P, _P, _P, _P, _P],

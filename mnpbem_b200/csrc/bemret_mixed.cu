@@ -83,19 +83,24 @@ __global__ void from_f32p(int n, int m, const float *Y, int64_t sy, cd *X, int64
 }
 
 // FP64 matrix times a few vectors: Y = A X, A n x n (c128, column-major),
-// X n x m (m <= NC <= 16), one thread per row, A streamed once.
-constexpr int ZS_KT = 32;
+// X n x m (m <= NC <= 16).  A CTA covers 64 rows with 4 K-lanes (warp w reads
+// 32 consecutive rows of every 4th column, 512 B per load), so each matrix
+// element is read once and many loads are in flight; the lanes' partial sums
+// are reduced in shared memory.
+constexpr int ZS_KT = 32, ZS_ROWS = 64, ZS_KL = 4;
 template <int NC>
-__global__ void __launch_bounds__(128) zskinny_kernel(int n, int m, const cd *__restrict__ A,
+__global__ void __launch_bounds__(256) zskinny_kernel(int n, int m, const cd *__restrict__ A,
                                                       int64_t lda, int64_t sA,
                                                       const cd *__restrict__ X, int64_t sX,
                                                       cd *__restrict__ Y, int64_t sY) {
     __shared__ cd Xs[ZS_KT][NC];
+    __shared__ cd part[ZS_KL][ZS_ROWS][NC];
     const int64_t b = blockIdx.y;
     A += b * sA;
     X += b * sX;
     Y += b * sY;
-    const int row = blockIdx.x * blockDim.x + threadIdx.x;
+    const int rl = threadIdx.x % ZS_ROWS, kl = threadIdx.x / ZS_ROWS;
+    const int row = blockIdx.x * ZS_ROWS + rl;
     cd acc[NC];
 #pragma unroll
     for (int j = 0; j < NC; ++j) acc[j] = cmk(0, 0);
@@ -109,17 +114,26 @@ __global__ void __launch_bounds__(128) zskinny_kernel(int n, int m, const cd *__
         if (row < n) {
             const int kend = min(ZS_KT, n - k0);
 #pragma unroll 4
-            for (int kk = 0; kk < kend; ++kk) {
+            for (int kk = kl; kk < kend; kk += ZS_KL) {
                 const cd a = __ldg(A + (int64_t)(k0 + kk) * lda + row);
 #pragma unroll
                 for (int j = 0; j < NC; ++j) acc[j] = cfma(a, Xs[kk][j], acc[j]);
             }
         }
     }
-    if (row >= n) return;
 #pragma unroll
-    for (int j = 0; j < NC; ++j)
-        if (j < m) Y[(int64_t)j * n + row] = acc[j];
+    for (int j = 0; j < NC; ++j) part[kl][rl][j] = acc[j];
+    __syncthreads();
+    for (int e = threadIdx.x; e < ZS_ROWS * NC; e += blockDim.x) {
+        const int r = e % ZS_ROWS, j = e / ZS_ROWS;
+        const int gr = blockIdx.x * ZS_ROWS + r;
+        if (gr < n && j < m) {
+            cd v = part[0][r][j];
+#pragma unroll
+            for (int q = 1; q < ZS_KL; ++q) v = cadd(v, part[q][r][j]);
+            Y[(int64_t)j * n + gr] = v;
+        }
+    }
 }
 
 // r = b - A x for the packed operator.  P1 = G1 [sig1|h1], P2 = G2 [sig2|h2],
@@ -204,6 +218,7 @@ struct Factors {
     int64_t ld, plane, stride;
     const int32_t *piv;   // [3][batch][n]: G1, G2, Sigma
     const float *dinv;    // diagonal-block inverses, see dinv_offsets
+    int *trsv_state;      // flags + ticket of the one-launch triangular solves
 };
 
 // Offsets (floats) into the diagonal-block-inverse buffer: G1/G2 unit-lower
@@ -248,7 +263,7 @@ static int mgetrs(f32::Ctx &c, int n, int m, const float *LU, const Factors &F,
     MNPB_TRY(convert_in(c.s, n, m, c.batch, x, sx, t1));
     const int64_t pl = (int64_t)n * m;
     MNPB_TRY(f32::getrs_few(c, n, m, CMatF{(float *)LU, F.ld, F.plane, F.stride}, piv,
-                            (int64_t)n, invL, invU, CMatF{t1, n, pl, 2 * pl}));
+                            (int64_t)n, invL, invU, CMatF{t1, n, pl, 2 * pl}, F.trsv_state));
     return convert_out(c.s, n, m, c.batch, t1, x, sx);
 }
 
@@ -368,7 +383,8 @@ extern "C" int mnpb_bemret_init_mixed(void *stream, int64_t n, int64_t batch, fl
 extern "C" int64_t mnpb_bemret_refine_workspace(int64_t n, int64_t batch, int64_t nrhs) {
     const int64_t K = nrhs;
     // msolve scratch (15 K n c128 + 2 x 16 K n float... per entry) + r, d, P1..Q2 + norms
-    return batch * n * K * (15 * 16 + 2 * 16 * 8 + 2 * 8 * 16 + 4 * 4 * 16) + 1024 +
+    return batch * n * K * (15 * 16 + 2 * 16 * 8 + 2 * 8 * 16 + 4 * 4 * 16) + 8 * 256 +
+           align_up(f32::trsv_state_bytes((int)n, (int)batch), 256) +
            align_up(tc::cgemm_tf32_workspace((int)n, 64, (int)batch), 256);
 }
 
@@ -397,7 +413,7 @@ extern "C" int mnpb_bemret_solve_refine(
     const int N = (int)n, B = (int)batch, k = (int)K;
     const int64_t plane = ld * n;
     Factors F{(float *)G1p, (float *)G2p, (float *)S1p, (float *)Sp, (float *)Dp, ld, plane,
-              2 * plane, piv, dinv};
+              2 * plane, piv, dinv, nullptr};
     const int64_t per = n * K;
     char *wp = (char *)work;
     auto take = [&](int64_t bytes) {
@@ -411,6 +427,7 @@ extern "C" int mnpb_bemret_solve_refine(
     cd *dx = (cd *)take(batch * per * 8 * 16);
     cd *P = (cd *)take(batch * per * 4 * 4 * 16);
     double *nrm = (double *)take(batch * 2 * 8);
+    F.trsv_state = (int *)take(f32::trsv_state_bytes(N, B));
     const int64_t tcw = (int64_t)((char *)work + work_bytes - wp);
     f32::Ctx c(s, B, (float *)wp, tcw);
     const int64_t sx = per * 8, sP4 = per * 4;
@@ -424,6 +441,7 @@ extern "C" int mnpb_bemret_solve_refine(
     for (int b = 0; b < B; ++b) iters[b] = 0;
     for (int it = 0; it <= max_iter; ++it) {
         dim3 gz(ceil_div(n, 128), B);
+        dim3 gzs(ceil_div(n, ZS_ROWS), B);
         const int64_t sG = ld * n;   // c128 matrices use the same leading dimension
         {
             ProfScope ps(s, PC_MATVEC, 4.0 * 16.0 * (double)n * n * batch);   // bytes of A read
@@ -431,12 +449,16 @@ extern "C" int mnpb_bemret_solve_refine(
             const cd *xs[4] = {xx, xx + 4 * per, xx, xx + 4 * per};
             cd *ys[4] = {P1, P2, Q1, Q2};
             for (int q = 0; q < 4; ++q) {
-                if (4 * k <= 4)
-                    zskinny_kernel<4><<<gz, 128, 0, s>>>(N, 4 * k, mats[q], ld, sG, xs[q], sx, ys[q], sP4);
-                else if (4 * k <= 8)
-                    zskinny_kernel<8><<<gz, 128, 0, s>>>(N, 4 * k, mats[q], ld, sG, xs[q], sx, ys[q], sP4);
-                else
-                    zskinny_kernel<16><<<gz, 128, 0, s>>>(N, 4 * k, mats[q], ld, sG, xs[q], sx, ys[q], sP4);
+                // at most 8 columns per launch (shared-memory bound of the lane reduction)
+                for (int c0 = 0; c0 < 4 * k; c0 += 8) {
+                    const int mc = min(8, 4 * k - c0);
+                    const cd *xq = xs[q] + (int64_t)c0 * N;
+                    cd *yq = ys[q] + (int64_t)c0 * N;
+                    if (mc <= 4)
+                        zskinny_kernel<4><<<gzs, 256, 0, s>>>(N, mc, mats[q], ld, sG, xq, sx, yq, sP4);
+                    else
+                        zskinny_kernel<8><<<gzs, 256, 0, s>>>(N, mc, mats[q], ld, sG, xq, sx, yq, sP4);
+                }
             }
             count_launch(3);
             MNPB_LAUNCH_CHECK("zskinny_kernel");

@@ -69,6 +69,7 @@ enum ProfClass {
 };
 bool prof_on();
 void prof_record(cudaStream_t s, int cls, double work, bool start);
+void prof_tag(const char *fmt, ...);   // annotate the launch being recorded
 
 struct ProfScope {
     cudaStream_t s;

@@ -370,6 +370,7 @@ __global__ void __launch_bounds__(256) trsv_kernel(int n, int m, int lower, cons
     __shared__ int s_ticket;
     __shared__ cf red[8][TB][NC];
     __shared__ cf rhs[TB][NC];
+    __shared__ cf dinv_s[TB][TB + 1];
     const int tid = threadIdx.x, r = tid & 31, q = tid >> 5;
     if (tid == 0) s_ticket = (int)atomicAdd(ticket, 1u);
     __syncthreads();
@@ -381,38 +382,64 @@ __global__ void __launch_bounds__(256) trsv_kernel(int n, int m, int lower, cons
     A += b * sA;
     X += b * sX;
     int *fl = flags + b * nb;
+    // stage the inverse of the diagonal block (independent of other blocks)
+    const float *Di = Dinv + (b * nb + j) * 2 * TB * TB;
+    for (int e = tid; e < TB * TB; e += 256) {
+        const int rr = e % TB, k = e / TB;
+        dinv_s[rr][k] = fmk(__ldg(Di + k * TB + rr), __ldg(Di + TB * TB + k * TB + rr));
+    }
     cf acc[NC];
 #pragma unroll
     for (int c = 0; c < NC; ++c) acc[c] = fmk(0.f, 0.f);
+    // blocks finish in chain order, so once the last dependency is published
+    // every earlier one is too
+    int known = -1;
+    if (jj > 0 && r == 0) {
+        const int last = lower ? jj - 1 : nb - jj;
+        if (ld_acquire(fl + last) == epoch) known = jj - 1;
+    }
+    known = __shfl_sync(0xffffffffu, known, 0);
+    __syncwarp();   // orders the lanes' later reads after lane 0's acquire
     for (int ii = 0; ii < jj; ++ii) {
         const int i = lower ? ii : nb - 1 - ii;
-        if (tid == 0) {
-            const uint64_t t0 = gtimer();
-            while (ld_acquire(fl + i) != epoch) {
-                if (gtimer() - t0 > TRSV_WAIT_NS) {
-                    atomicCAS(&g_trsv_error, 0, 1);
-                    break;
-                }
+        // factor entries first: they do not depend on other blocks
+        cf a[4];
+#pragma unroll
+        for (int t = 0; t < 4; ++t) {
+            const int col = i * TB + q + 8 * t;
+            a[t] = fmk(0.f, 0.f);
+            if (col < n && r < rows) {
+                const int64_t o = (int64_t)col * lda + r0 + r;
+                a[t] = fmk(A[o], A[o + plane]);
             }
         }
-        __syncthreads();
-        if (r < rows) {
+        if (ii > known) {
+            // lane 0 of each warp waits (acquire); __syncwarp orders the lanes' reads
+            if (r == 0) {
+                const uint64_t t0 = gtimer();
+                while (ld_acquire(fl + i) != epoch) {
+                    if (gtimer() - t0 > TRSV_WAIT_NS) {
+                        atomicCAS(&g_trsv_error, 0, 1);
+                        break;
+                    }
+                }
+            }
+            __syncwarp();
+            known = ii;
+        }
 #pragma unroll
-            for (int t = 0; t < 4; ++t) {
-                const int col = i * TB + q + 8 * t;
-                if (col < n) {
-                    const int64_t o = (int64_t)col * lda + r0 + r;
-                    const cf a = fmk(A[o], A[o + plane]);
+        for (int t = 0; t < 4; ++t) {
+            const int col = i * TB + q + 8 * t;
+            if (col < n && r < rows) {
 #pragma unroll
-                    for (int c = 0; c < NC; ++c) {
-                        if (c < m) {
-                            const int64_t xo = (int64_t)c * ldx + col;
-                            const cf xv = fmk(__ldcg(X + xo), __ldcg(X + xo + planeX));
-                            acc[c].x = fmaf(a.x, xv.x, acc[c].x);
-                            acc[c].x = fmaf(-a.y, xv.y, acc[c].x);
-                            acc[c].y = fmaf(a.x, xv.y, acc[c].y);
-                            acc[c].y = fmaf(a.y, xv.x, acc[c].y);
-                        }
+                for (int c = 0; c < NC; ++c) {
+                    if (c < m) {
+                        const int64_t xo = (int64_t)c * ldx + col;
+                        const cf xv = fmk(__ldcg(X + xo), __ldcg(X + xo + planeX));
+                        acc[c].x = fmaf(a[t].x, xv.x, acc[c].x);
+                        acc[c].x = fmaf(-a[t].y, xv.y, acc[c].x);
+                        acc[c].y = fmaf(a[t].x, xv.y, acc[c].y);
+                        acc[c].y = fmaf(a[t].y, xv.x, acc[c].y);
                     }
                 }
             }
@@ -427,6 +454,7 @@ __global__ void __launch_bounds__(256) trsv_kernel(int n, int m, int lower, cons
         if (rr < rows && c < m) {
             const int64_t xo = (int64_t)c * ldx + r0 + rr;
             v = fmk(__ldcg(X + xo), __ldcg(X + xo + planeX));
+#pragma unroll
             for (int qq = 0; qq < 8; ++qq) {
                 v.x -= red[qq][rr][c].x;
                 v.y -= red[qq][rr][c].y;
@@ -435,13 +463,13 @@ __global__ void __launch_bounds__(256) trsv_kernel(int n, int m, int lower, cons
         rhs[rr][c] = v;
     }
     __syncthreads();
-    const float *Di = Dinv + (b * nb + j) * 2 * TB * TB;
     for (int e = tid; e < TB * NC; e += 256) {
         const int rr = e % TB, c = e / TB;
         if (rr < rows && c < m) {
             cf y = fmk(0.f, 0.f);
+#pragma unroll 8
             for (int k = 0; k < TB; ++k) {
-                const cf d = fmk(__ldg(Di + k * TB + rr), __ldg(Di + TB * TB + k * TB + rr));
+                const cf d = dinv_s[rr][k];
                 y.x = fmaf(d.x, rhs[k][c].x, y.x);
                 y.x = fmaf(-d.y, rhs[k][c].y, y.x);
                 y.y = fmaf(d.x, rhs[k][c].y, y.y);
@@ -487,6 +515,7 @@ int gemm(Ctx &c, int m, int n, int k, float alpha, CMatF A, CMatF B, float beta,
     if (n <= SK_N) {
         dim3 grid(ceil_div(m, 128), c.batch);
         ProfScope ps(c.s, PC_SGEMM, 8.0 * (double)m * k * c.batch);   // bytes of A streamed
+        prof_tag("M=%d N=%d K=%d B=%d", m, n, k, c.batch);
 #define MNPB_SKINNY(NC)                                                                        \
     skinny_kernel<NC><<<grid, 128, 0, c.s>>>(m, n, k, alpha, A.p, A.ld, A.plane, A.stride, B.p, \
                                              B.ld, B.plane, B.stride, beta, C.p, C.ld, C.plane, \
@@ -507,6 +536,7 @@ static int trsm_small(Ctx &c, int mode, int kb, CMatF T, CMatF B, int nvec) {
     if (nvec <= 0 || kb <= 0) return MNPB_OK;
     dim3 grid(ceil_div(nvec, 128), c.batch);
     ProfScope ps(c.s, PC_TRSM, 4.0 * kb * kb * (double)nvec * c.batch);
+    prof_tag("mode=%d kb=%d nvec=%d B=%d", mode, kb, nvec, c.batch);
     trsm_small_kernel<<<grid, 128, 0, c.s>>>(mode, kb, T.p, T.ld, T.plane, T.stride, B.p, B.ld,
                                              B.plane, B.stride, nvec);
     MNPB_LAUNCH_CHECK("trsm_small_kernel(f32)");
@@ -568,6 +598,7 @@ static int rgetrf(Ctx &c, int n, int off, int w, CMatF A, int32_t *ipiv, int64_t
                   int32_t *info) {
     if (w <= TS) {
         ProfScope ps(c.s, PC_PANEL, 8.0 * w * w * (double)(n - off) * c.batch / 2);
+        prof_tag("off=%d w=%d B=%d", off, w, c.batch);
         panel_kernel<<<c.batch, PANEL_THREADS, 0, c.s>>>(n, off, w, A.p, A.ld, A.plane, A.stride,
                                                          ipiv, sP, info);
         MNPB_LAUNCH_CHECK("panel_kernel(f32)");
@@ -604,26 +635,8 @@ int right_solve(Ctx &c, int n, int m, CMatF LU, const int32_t *ipiv, int64_t sP,
 }
 
 // ---- few-RHS solves ---------------------------------------------------------
-static int *g_flags = nullptr;
-static unsigned *g_ticket = nullptr;
-static int64_t g_flags_cap = 0;
-static int g_epoch = 0;
-
-static int flags_reserve(int64_t count) {
-    if (count <= g_flags_cap) return MNPB_OK;
-    if (g_flags) cudaFree(g_flags);
-    if (g_ticket) cudaFree(g_ticket);
-    g_flags = nullptr;
-    g_ticket = nullptr;
-    if (cudaMalloc(&g_flags, count * sizeof(int)) != cudaSuccess ||
-        cudaMalloc(&g_ticket, sizeof(unsigned)) != cudaSuccess ||
-        cudaMemset(g_flags, 0, count * sizeof(int)) != cudaSuccess) {
-        set_error("trsv: cannot allocate flags");
-        g_flags_cap = 0;
-        return MNPB_ENOMEM;
-    }
-    g_flags_cap = count;
-    return MNPB_OK;
+int64_t trsv_state_bytes(int n, int batch) {
+    return ((int64_t)ceil_div(n, TB) * batch + 64) * sizeof(int);
 }
 
 int64_t diag_inv_floats(int n, int batch) { return (int64_t)batch * ceil_div(n, TB) * 2 * TB * TB; }
@@ -639,27 +652,24 @@ int diag_inv(Ctx &c, int n, CMatF LU, float *invL, float *invU) {
     return MNPB_OK;
 }
 
-static int trsv(Ctx &c, bool lower, int n, int m, CMatF T, const float *inv, CMatF X) {
+// state: caller-provided device scratch of trsv_state_bytes(n, batch) bytes
+// (flags per block and the ticket counter), cleared before each launch.
+static int trsv(Ctx &c, bool lower, int n, int m, CMatF T, const float *inv, CMatF X,
+                int *state) {
     const int nb = ceil_div(n, TB);
-    MNPB_TRY(flags_reserve((int64_t)nb * c.batch));
-    if (++g_epoch <= 0) {
-        // epochs wrapped: clear the flags so that no stale value matches
-        g_epoch = 1;
-        if (cudaMemsetAsync(g_flags, 0, g_flags_cap * sizeof(int), c.s) != cudaSuccess) {
-            set_error("trsv: memset failed");
-            return MNPB_ECUDA;
-        }
-    }
-    if (cudaMemsetAsync(g_ticket, 0, sizeof(unsigned), c.s) != cudaSuccess) {
+    int *flags = state;
+    unsigned *ticket = (unsigned *)(state + (int64_t)nb * c.batch);
+    if (cudaMemsetAsync(state, 0, trsv_state_bytes(n, c.batch), c.s) != cudaSuccess) {
         set_error("trsv: memset failed");
         return MNPB_ECUDA;
     }
     const int grid = nb * c.batch;
     ProfScope ps(c.s, PC_TRSV, 4.0 * (double)n * n * c.batch);   // bytes of the triangle
+    prof_tag("n=%d m=%d B=%d %s", n, m, c.batch, lower ? "L" : "U");
 #define MNPB_TRSV(NC)                                                                          \
     trsv_kernel<NC><<<grid, 256, 0, c.s>>>(n, m, lower ? 1 : 0, T.p, T.ld, T.plane, T.stride,   \
-                                           inv, X.p, X.ld, X.plane, X.stride, g_flags,          \
-                                           g_ticket, g_epoch, nb, c.batch)
+                                           inv, X.p, X.ld, X.plane, X.stride, flags, ticket, 1, \
+                                           nb, c.batch)
     if (m <= 4) MNPB_TRSV(4);
     else if (m <= 8) MNPB_TRSV(8);
     else MNPB_TRSV(16);
@@ -669,11 +679,11 @@ static int trsv(Ctx &c, bool lower, int n, int m, CMatF T, const float *inv, CMa
 }
 
 int getrs_few(Ctx &c, int n, int m, CMatF LU, const int32_t *ipiv, int64_t sP,
-              const float *invL, const float *invU, CMatF B) {
+              const float *invL, const float *invU, CMatF B, int *state) {
     if (m > 16) return getrs(c, n, m, LU, ipiv, sP, B);
     MNPB_TRY(laswp(c, B, 0, m, ipiv, sP, 0, n, true));
-    MNPB_TRY(trsv(c, true, n, m, LU, invL, B));
-    return trsv(c, false, n, m, LU, invU, B);
+    MNPB_TRY(trsv(c, true, n, m, LU, invL, B, state));
+    return trsv(c, false, n, m, LU, invU, B, state);
 }
 
 int trsv_error_read_and_clear(cudaStream_t s, int *code) {

@@ -32,8 +32,10 @@ int set_identity(Ctx &c, int n, tc::CMatF W);
 int64_t diag_inv_floats(int n, int batch);
 int diag_inv(Ctx &c, int n, tc::CMatF LU, float *invL, float *invU);
 // LU solve for m <= 16 right-hand sides: row swaps + one launch per triangle.
+// state: device scratch of trsv_state_bytes(n, batch) bytes (per stream).
+int64_t trsv_state_bytes(int n, int batch);
 int getrs_few(Ctx &c, int n, int m, tc::CMatF LU, const int32_t *ipiv, int64_t sP,
-              const float *invL, const float *invU, tc::CMatF B);
+              const float *invL, const float *invU, tc::CMatF B, int *state);
 int trsv_error_read_and_clear(cudaStream_t s, int *code);
 
 }  // namespace f32

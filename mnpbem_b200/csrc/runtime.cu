@@ -2,6 +2,7 @@
 #include "common.cuh"
 
 #include <cmath>
+#include <mutex>
 #include <vector>
 
 namespace mnpb {
@@ -30,19 +31,24 @@ int check_launch(const char *what) {
 }
 
 // ---- event profiler ---------------------------------------------------------
+// Events come from a pool; records are appended to a shared list under one
+// lock; each host thread keeps its own open record (launches nest only
+// within one thread's call sequence).
 namespace {
 struct Rec {
     cudaEvent_t a, b;
     int cls;
     double work;
+    char tag[64];
 };
 bool g_prof = false;
+std::mutex g_prof_mu;
 std::vector<Rec> g_recs;
 std::vector<cudaEvent_t> g_pool;
-Rec g_open;
-bool g_has_open = false;
+thread_local bool t_has_open = false;
+thread_local Rec t_open;
 
-cudaEvent_t take_event() {
+cudaEvent_t take_event() {   // caller holds g_prof_mu
     if (!g_pool.empty()) {
         cudaEvent_t e = g_pool.back();
         g_pool.pop_back();
@@ -57,27 +63,40 @@ cudaEvent_t take_event() {
 bool prof_on() { return g_prof; }
 
 void prof_record(cudaStream_t s, int cls, double work, bool start) {
+    std::lock_guard<std::mutex> lk(g_prof_mu);
     if (start) {
-        g_open.a = take_event();
-        g_open.cls = cls;
-        g_open.work = work;
-        cudaEventRecord(g_open.a, s);
-        g_has_open = true;
-    } else if (g_has_open) {
-        g_open.b = take_event();
-        cudaEventRecord(g_open.b, s);
-        g_recs.push_back(g_open);
-        g_has_open = false;
+        t_open.a = take_event();
+        t_open.cls = cls;
+        t_open.work = work;
+        t_open.tag[0] = 0;
+        cudaEventRecord(t_open.a, s);
+        t_has_open = true;
+    } else if (t_has_open) {
+        t_open.b = take_event();
+        cudaEventRecord(t_open.b, s);
+        g_recs.push_back(t_open);
+        t_has_open = false;
     }
+}
+
+void prof_tag(const char *fmt, ...) {
+    if (!g_prof || !t_has_open) return;
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(t_open.tag, sizeof(t_open.tag), fmt, ap);
+    va_end(ap);
 }
 
 }  // namespace mnpb
 
 using namespace mnpb;
 
+static std::vector<Rec> g_last;   // records of the last mnpb_prof_end (for mnpb_prof_dump)
+
 // Start recording CUDA events around the library's launches (host thread
 // that issues the launches; single-threaded use).
 extern "C" int mnpb_prof_begin(void) {
+    std::lock_guard<std::mutex> lk(g_prof_mu);
     g_recs.clear();
     g_prof = true;
     return MNPB_OK;
@@ -87,6 +106,7 @@ extern "C" int mnpb_prof_begin(void) {
 // (ms), the summed algorithmic work and the launch count.
 extern "C" int mnpb_prof_end(int ncls, double *ms, double *work, int64_t *count) {
     clear_error();
+    std::lock_guard<std::mutex> lk(g_prof_mu);
     g_prof = false;
     for (int c = 0; c < ncls; ++c) {
         ms[c] = 0.0;
@@ -105,10 +125,31 @@ extern "C" int mnpb_prof_end(int ncls, double *ms, double *work, int64_t *count)
             work[r.cls] += r.work;
             count[r.cls] += 1;
         }
+    }
+    g_last = g_recs;
+    for (auto &r : g_recs) {
         g_pool.push_back(r.a);
         g_pool.push_back(r.b);
     }
     g_recs.clear();
+    return MNPB_OK;
+}
+
+// Write the launches of the last profiled interval as CSV (class, ms, work, tag).
+extern "C" int mnpb_prof_dump(const char *path) {
+    clear_error();
+    FILE *f = fopen(path, "w");
+    if (!f) {
+        set_error("prof_dump: cannot open %s", path);
+        return MNPB_EINVAL;
+    }
+    fprintf(f, "class,ms,work,tag\n");
+    for (auto &r : g_last) {
+        float t = 0.f;
+        cudaEventElapsedTime(&t, r.a, r.b);
+        fprintf(f, "%d,%.6f,%.6g,%s\n", r.cls, t, r.work, r.tag);
+    }
+    fclose(f);
     return MNPB_OK;
 }
 

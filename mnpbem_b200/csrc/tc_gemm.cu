@@ -25,12 +25,18 @@
 namespace mnpb {
 namespace tc {
 
-constexpr int BM = 128, BN = 128, BK = 32;   // BK: TF32 elements per 128-byte row
-constexpr int STAGES = 3;
-constexpr int TILE_BYTES = BM * BK * 4;        // 16 KB (same for the B tile, BN == BM)
-constexpr int STAGE_BYTES = 4 * TILE_BYTES;    // Ar, Ai, Br, Bi
-constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 + 256;
-constexpr int TMEM_COLS = 256;
+constexpr int BM = 128, BK = 32;   // BK: TF32 elements per 128-byte row
+constexpr int MAX_STAGES = 4;
+constexpr int TILE_A_BYTES = BM * BK * 4;   // 16 KB
+template <int BN> struct Tile {
+    static constexpr int B_BYTES = BN * BK * 4;
+    static constexpr int STAGE_BYTES = 2 * TILE_A_BYTES + 2 * B_BYTES;   // Ar, Ai, Br, Bi
+    static constexpr int TMEM_COLS = 2 * BN < 32 ? 32 : 2 * BN;          // re + im accumulators
+    static constexpr int MAX_ST = ((227 * 1024 - 1280) / STAGE_BYTES) < MAX_STAGES
+                                      ? ((227 * 1024 - 1280) / STAGE_BYTES)
+                                      : MAX_STAGES;
+    static int smem_bytes(int nst) { return nst * STAGE_BYTES + 1024 + 256; }
+};
 constexpr uint64_t WAIT_NS = 2000000000ull;    // a wait gives up after 2 s
 
 __device__ int g_tc_error;                     // first timeout code seen (0 = none)
@@ -87,12 +93,12 @@ __device__ __forceinline__ uint64_t smem_desc_k128(uint32_t addr) {
     d |= (uint64_t)2 << 61;                          // swizzle: 128 B
     return d;
 }
-// Instruction descriptor: TF32 x TF32 -> F32, both K-major, M = 128, N = 128.
-__host__ __device__ constexpr uint32_t idesc_tf32(bool neg_a) {
+// Instruction descriptor: TF32 x TF32 -> F32, both K-major, M = 128, N = bn.
+__host__ __device__ constexpr uint32_t idesc_tf32(bool neg_a, int bn) {
     return (1u << 4)                    // D format F32
          | (2u << 7) | (2u << 10)       // A, B format TF32
          | ((neg_a ? 1u : 0u) << 13)    // negate A
-         | ((uint32_t)(BN >> 3) << 17)  // N / 8
+         | ((uint32_t)(bn >> 3) << 17)  // N / 8
          | ((uint32_t)(BM >> 4) << 24); // M / 16
 }
 __device__ __forceinline__ void mma_tf32(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t idesc,
@@ -134,6 +140,20 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
     for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
 }
 
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
+    uint32_t r[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+        "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+          "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]),
+          "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+
 struct Epi {
     float *C;
     int64_t ldc, planeC, strideC;
@@ -141,16 +161,21 @@ struct Epi {
     int M, N, ktiles;
 };
 
-__global__ void __launch_bounds__(128, 1)
+template <int BN>
+__global__ void __launch_bounds__(128)
     cgemm_tf32_kernel(const __grid_constant__ CUtensorMap tmA,
                       const __grid_constant__ CUtensorMap tmBr,
-                      const __grid_constant__ CUtensorMap tmBi, Epi ep) {
+                      const __grid_constant__ CUtensorMap tmBi, Epi ep, int STAGES) {
+    using TL = Tile<BN>;
+    constexpr int STAGE_BYTES = TL::STAGE_BYTES;
+    constexpr int TILE_BYTES = TILE_A_BYTES;
+    constexpr int TMEM_COLS = TL::TMEM_COLS;
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     // 1024-byte alignment for the swizzled tiles
     uint8_t *smem = (uint8_t *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
     uint64_t *bars = (uint64_t *)(smem + STAGES * STAGE_BYTES);
     // bars[0..S): full, bars[S..2S): empty, bars[2S]: accumulator ready
-    uint32_t *tmem_slot = (uint32_t *)(bars + 2 * STAGES + 1);
+    uint32_t *tmem_slot = (uint32_t *)(bars + 2 * MAX_STAGES + 1);
     volatile int *abort_flag = (volatile int *)(tmem_slot + 1);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -198,11 +223,11 @@ __global__ void __launch_bounds__(128, 1)
             tma_load_3d(smem_u32(st), &tmA, full, k0, m0, 2 * b);
             tma_load_3d(smem_u32(st + TILE_BYTES), &tmA, full, k0, m0, 2 * b + 1);
             tma_load_3d(smem_u32(st + 2 * TILE_BYTES), &tmBr, full, k0, n0, b);
-            tma_load_3d(smem_u32(st + 3 * TILE_BYTES), &tmBi, full, k0, n0, b);
+            tma_load_3d(smem_u32(st + 2 * TILE_BYTES + TL::B_BYTES), &tmBi, full, k0, n0, b);
         }
     } else if (warp == 1 && lane == 0) {
         // MMA issuer
-        constexpr uint32_t ID = idesc_tf32(false), IDN = idesc_tf32(true);
+        constexpr uint32_t ID = idesc_tf32(false, BN), IDN = idesc_tf32(true, BN);
         for (int kt = 0; kt < KT; ++kt) {
             const int s = kt % STAGES;
             if (!mbar_wait(smem_u32(&bars[s]), (kt / STAGES) & 1)) {
@@ -218,7 +243,7 @@ __global__ void __launch_bounds__(128, 1)
                 const uint64_t ar = smem_desc_k128(st + off);
                 const uint64_t ai = smem_desc_k128(st + TILE_BYTES + off);
                 const uint64_t br = smem_desc_k128(st + 2 * TILE_BYTES + off);
-                const uint64_t bi = smem_desc_k128(st + 3 * TILE_BYTES + off);
+                const uint64_t bi = smem_desc_k128(st + 2 * TILE_BYTES + TL::B_BYTES + off);
                 const uint32_t acc = (kt > 0 || j > 0) ? 1u : 0u;
                 mma_tf32(d_re, ar, br, ID, acc);
                 mma_tf32(d_re, ai, bi, IDN, 1u);
@@ -242,35 +267,37 @@ __global__ void __launch_bounds__(128, 1)
     float *Ci = Cr + ep.planeC;
     const uint32_t lane_base = (uint32_t)(warp * 32) << 16;
     const bool row_ok = good && row < ep.M;
-    for (int c0 = 0; c0 < BN; c0 += 32) {
-        float vr[32], vi[32];
-        tmem_ld32(d_re + lane_base + c0, vr);
-        tmem_ld32(d_im + lane_base + c0, vi);
-        const int ncol = min(32, ep.N - (n0 + c0));
+    constexpr int CH = 16;   // columns per TMEM load (keeps the epilogue's registers low)
+#pragma unroll 1
+    for (int c0 = 0; c0 < BN; c0 += CH) {
+        float vr[CH], vi[CH];
+        tmem_ld16(d_re + lane_base + c0, vr);
+        tmem_ld16(d_im + lane_base + c0, vi);
+        const int ncol = min(CH, ep.N - (n0 + c0));
         if (!row_ok || ncol <= 0) continue;
         const int64_t o0 = (int64_t)(n0 + c0) * ep.ldc + row;
         if (ep.beta != 0.f) {
             // issue every load of C before any store so the loads overlap
-            float cr[32], ci[32];
+            float cr[CH], ci[CH];
 #pragma unroll
-            for (int c = 0; c < 32; ++c) {
+            for (int c = 0; c < CH; ++c) {
                 cr[c] = c < ncol ? __ldg(Cr + o0 + (int64_t)c * ep.ldc) : 0.f;
                 ci[c] = c < ncol ? __ldg(Ci + o0 + (int64_t)c * ep.ldc) : 0.f;
             }
 #pragma unroll
-            for (int c = 0; c < 32; ++c) {
+            for (int c = 0; c < CH; ++c) {
                 vr[c] = fmaf(ep.beta, cr[c], ep.alpha * vr[c]);
                 vi[c] = fmaf(ep.beta, ci[c], ep.alpha * vi[c]);
             }
         } else {
 #pragma unroll
-            for (int c = 0; c < 32; ++c) {
+            for (int c = 0; c < CH; ++c) {
                 vr[c] *= ep.alpha;
                 vi[c] *= ep.alpha;
             }
         }
 #pragma unroll
-        for (int c = 0; c < 32; ++c) {
+        for (int c = 0; c < CH; ++c) {
             if (c < ncol) {
                 Cr[o0 + (int64_t)c * ep.ldc] = vr[c];
                 Ci[o0 + (int64_t)c * ep.ldc] = vi[c];
@@ -337,7 +364,7 @@ static EncodeFn get_encode() {
 // 3-D FP32 map: inner dim d0 (contiguous), rows d1 (stride s1 elements),
 // planes/batch d2 (stride s2 elements); box 32 x 128 x 1, 128-byte swizzle.
 static int make_map(CUtensorMap *map, const float *base, uint64_t d0, uint64_t d1, uint64_t d2,
-                    uint64_t s1, uint64_t s2) {
+                    uint64_t s1, uint64_t s2, uint32_t box_rows) {
     EncodeFn enc = get_encode();
     if (!enc) {
         set_error("tc_gemm: cuTensorMapEncodeTiled unavailable");
@@ -350,7 +377,7 @@ static int make_map(CUtensorMap *map, const float *base, uint64_t d0, uint64_t d
     }
     cuuint64_t dims[3] = {d0, d1, d2};
     cuuint64_t strides[2] = {s1 * 4, s2 * 4};
-    cuuint32_t box[3] = {BK, BM, 1};
+    cuuint32_t box[3] = {BK, box_rows, 1};
     cuuint32_t estr[3] = {1, 1, 1};
     CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, (void *)base, dims, strides, box,
                      estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
@@ -367,21 +394,43 @@ int64_t cgemm_tf32_workspace(int M, int K, int batch) {
     return (int64_t)batch * 2 * Mp * Kp * 4;
 }
 
+template <int BN>
+static int launch_tf32(cudaStream_t s, const CUtensorMap &mA, const CMatF &B, int M, int N,
+                       int K, int Kp, int Mp, int batch, Epi ep) {
+    using TL = Tile<BN>;
+    static bool attr_set = false;
+    if (!attr_set) {
+        if (cudaFuncSetAttribute(cgemm_tf32_kernel<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 TL::smem_bytes(TL::MAX_ST)) != cudaSuccess) {
+            set_error("tc_gemm: cannot set shared memory size");
+            return MNPB_ECUDA;
+        }
+        attr_set = true;
+    }
+    CUtensorMap mBr, mBi;
+    MNPB_TRY(make_map(&mBr, B.p, K, N, batch, B.ld, B.stride, BN));
+    MNPB_TRY(make_map(&mBi, B.p + B.plane, K, N, batch, B.ld, B.stride, BN));
+    // stages: as many as the K loop can use; the shared-memory request is at
+    // least large enough that no more CTAs share an SM than fit their
+    // accumulators in its 512 TMEM columns
+    const int KT = Kp / BK;
+    const int nst = KT < TL::MAX_ST ? KT : TL::MAX_ST;
+    const int max_ctas_tmem = 512 / TL::TMEM_COLS;
+    int dyn = TL::smem_bytes(nst);
+    const int floor_bytes = (228 * 1024) / (max_ctas_tmem + 1) + 1024;
+    if (dyn < floor_bytes) dyn = floor_bytes;
+    dim3 grid(Mp / BM, (N + BN - 1) / BN, batch);
+    cgemm_tf32_kernel<BN><<<grid, 128, dyn, s>>>(mA, mBr, mBi, ep, nst);
+    MNPB_LAUNCH_CHECK("cgemm_tf32_kernel");
+    return MNPB_OK;
+}
+
 int cgemm_tf32(cudaStream_t s, int M, int N, int K, int batch, float alpha, CMatF A, CMatF B,
                float beta, CMatF C, float *work, int64_t work_bytes) {
     if (M <= 0 || N <= 0 || batch <= 0) return MNPB_OK;
     if (K <= 0) {
         set_error("tc_gemm: K must be positive");
         return MNPB_EINVAL;
-    }
-    static bool attr_set = false;
-    if (!attr_set) {
-        if (cudaFuncSetAttribute(cgemm_tf32_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 SMEM_BYTES) != cudaSuccess) {
-            set_error("tc_gemm: cannot set shared memory size");
-            return MNPB_ECUDA;
-        }
-        attr_set = true;
     }
     const int Mp = (M + BM - 1) / BM * BM, Kp = (K + BK - 1) / BK * BK;
     if (work_bytes < cgemm_tf32_workspace(M, K, batch)) {
@@ -394,16 +443,14 @@ int cgemm_tf32(cudaStream_t s, int M, int N, int K, int batch, float alpha, CMat
         pack_a_tf32_kernel<<<g, t, 0, s>>>(A.p, A.ld, A.plane, A.stride, M, K, Mp, Kp, work);
         MNPB_LAUNCH_CHECK("pack_a_tf32_kernel");
     }
-    CUtensorMap mA, mBr, mBi;
-    MNPB_TRY(make_map(&mA, work, Kp, Mp, (uint64_t)batch * 2, Kp, (uint64_t)Mp * Kp));
-    MNPB_TRY(make_map(&mBr, B.p, K, N, batch, B.ld, B.stride));
-    MNPB_TRY(make_map(&mBi, B.p + B.plane, K, N, batch, B.ld, B.stride));
+    CUtensorMap mA;
+    MNPB_TRY(make_map(&mA, work, Kp, Mp, (uint64_t)batch * 2, Kp, (uint64_t)Mp * Kp, BM));
     Epi ep{C.p, C.ld, C.plane, C.stride, alpha, beta, M, N, Kp / BK};
-    dim3 grid(Mp / BM, (N + BN - 1) / BN, batch);
     ProfScope ps(s, PC_TCGEMM, 8.0 * M * N * (double)K * batch);
-    cgemm_tf32_kernel<<<grid, 128, SMEM_BYTES, s>>>(mA, mBr, mBi, ep);
-    MNPB_LAUNCH_CHECK("cgemm_tf32_kernel");
-    return MNPB_OK;
+    prof_tag("M=%d N=%d K=%d B=%d", M, N, K, batch);
+    if (N <= 32) return launch_tf32<32>(s, mA, B, M, N, K, Kp, Mp, batch, ep);
+    if (N <= 64) return launch_tf32<64>(s, mA, B, M, N, K, Kp, Mp, batch, ep);
+    return launch_tf32<128>(s, mA, B, M, N, K, Kp, Mp, batch, ep);
 }
 
 int tc_error_read_and_clear(cudaStream_t s, int *code) {
