@@ -286,6 +286,26 @@ int mnpb_cgemm_tf32(void *stream, int64_t m, int64_t n, int64_t k, int64_t batch
                     int64_t ldb, int64_t planeB, int64_t sB, float beta, float *C, int64_t ldc,
                     int64_t planeC, int64_t sC, void *work, int64_t work_bytes);
 
+/* Same GEMM as mnpb_cgemm_tf32, but it allocates nothing and takes no
+ * workspace: the packed TF32 copy of A goes into a fixed 64 MiB array of the
+ * library's static device memory (one per device, reserved when the module
+ * loads).  No counterpart in the reference, which has no GPU path; it is for
+ * callers that cannot provide device memory (a foreign-language host without
+ * a device allocator, a pool that owns the whole GPU, a loop that must not
+ * synchronise the device through cudaMalloc/cudaFree).
+ *   - Limit: mnpb_cgemm_tf32_workspace(m, k, batch) <= 67108864 bytes, else
+ *     MNPB_ENOMEM with the sizes in mnpb_last_error() and nothing launched.
+ *   - The first call on each device does the setup (address lookup of the
+ *     array, kernel attributes); make it before any stream capture.
+ *   - Nothing has to be zeroed beforehand: every scratch element is written
+ *     before it is read.
+ *   - Calls that overlap in time on one device (other streams, other host
+ *     threads) share the array and race; calls ordered on one stream do not. */
+int mnpb_cgemm_tf32_noalloc(void *stream, int64_t m, int64_t n, int64_t k, int64_t batch,
+                            float alpha, const float *A, int64_t lda, int64_t planeA, int64_t sA,
+                            const float *B, int64_t ldb, int64_t planeB, int64_t sB, float beta,
+                            float *C, int64_t ldc, int64_t planeC, int64_t sC);
+
 /* First bounded-wait timeout recorded by a tensor-core kernel since the last
  * call (0 = none); reading clears it. */
 int mnpb_tc_error(void *stream, int32_t *code);

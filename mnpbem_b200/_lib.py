@@ -57,6 +57,8 @@ SIGNATURES = {
     'mnpb_cgemm_tf32_workspace': [_I64, _I64, _I64],
     'mnpb_cgemm_tf32': [_P, _I64, _I64, _I64, _I64, C.c_float, _P, _I64, _I64, _I64, _P, _I64,
                         _I64, _I64, C.c_float, _P, _I64, _I64, _I64, _P, _I64],
+    'mnpb_cgemm_tf32_noalloc': [_P, _I64, _I64, _I64, _I64, C.c_float, _P, _I64, _I64, _I64,
+                                _P, _I64, _I64, _I64, C.c_float, _P, _I64, _I64, _I64],
     'mnpb_tc_error': [_P, _P],
     'mnpb_stat_matrix': [_P, _I64, _I64, _P, _I64, _P, _P, _I64, _I64],
     'mnpb_planewave_potential': [_P, _I64, _I64, _I64, _P, _P, _P, _P, _P, _P, _P, _P, _P],

@@ -498,3 +498,106 @@ extern "C" int mnpb_tc_error(void *stream, int32_t *code) {
     *code = v;
     return MNPB_OK;
 }
+
+// ---------------------------------------------------------------------------
+// Allocation-free variant of mnpb_cgemm_tf32.
+//
+// Some callers cannot hand the library a device workspace: a host program in
+// another language that binds the C ABI but owns no device allocator, a code
+// whose memory pool has already claimed the whole GPU, or a loop that must not
+// take the implicit device synchronisation that cudaMalloc/cudaFree imply.
+// For them the only scratch this GEMM needs, the packed TF32 copy of A, is
+// kept in a fixed array of this module's static device memory.  The array is
+// reserved by the CUDA runtime when the module is loaded (64 MiB per device),
+// whether or not this entry point is ever called.
+//
+// Nothing in the array has to start at zero: the pack kernel writes every
+// element of the padded Mp x Kp tiles, padding included, before the GEMM
+// reads them.  The error word the GEMM may set is the same one
+// mnpb_cgemm_tf32 uses (read and cleared by mnpb_tc_error).
+//
+// There is ONE array per device: calls that may overlap in time on the same
+// device (different streams, or different host threads) overwrite each
+// other's packed operand and race.  Calls issued in order on one stream are
+// safe.
+// ---------------------------------------------------------------------------
+namespace mnpb {
+namespace tc {
+
+constexpr int64_t kStaticPackBytes = int64_t(64) << 20;
+static __device__ __align__(256) float g_static_pack[kStaticPackBytes / 4];
+
+constexpr int kMaxDevices = 64;
+
+template <int BN> static cudaError_t opt_in_smem() {
+    using TL = Tile<BN>;
+    return cudaFuncSetAttribute(cgemm_tf32_kernel<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                TL::smem_bytes(TL::MAX_ST));
+}
+
+// Device address of g_static_pack on the current device, looked up once per
+// device (under a lock) together with the kernels' shared-memory opt-in.
+static int static_pack_scratch(float **out) {
+    static std::mutex mu;
+    static float *addr[kMaxDevices] = {};
+    int dev = -1;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) {
+        set_error("cgemm_tf32_noalloc: cudaGetDevice failed: %s", cudaGetErrorString(e));
+        return MNPB_ECUDA;
+    }
+    if (dev < 0 || dev >= kMaxDevices) {
+        set_error("cgemm_tf32_noalloc: device ordinal %d out of range", dev);
+        return MNPB_EINVAL;
+    }
+    std::lock_guard<std::mutex> lk(mu);
+    if (!addr[dev]) {
+        void *p = nullptr;
+        e = cudaGetSymbolAddress(&p, g_static_pack);
+        if (e != cudaSuccess || !p) {
+            set_error("cgemm_tf32_noalloc: cudaGetSymbolAddress failed on device %d: %s", dev,
+                      cudaGetErrorString(e));
+            return MNPB_ECUDA;
+        }
+        if ((e = opt_in_smem<32>()) != cudaSuccess || (e = opt_in_smem<64>()) != cudaSuccess ||
+            (e = opt_in_smem<128>()) != cudaSuccess) {
+            set_error("cgemm_tf32_noalloc: cannot set shared memory size on device %d: %s", dev,
+                      cudaGetErrorString(e));
+            return MNPB_ECUDA;
+        }
+        addr[dev] = (float *)p;
+    }
+    *out = addr[dev];
+    return MNPB_OK;
+}
+
+}  // namespace tc
+}  // namespace mnpb
+
+extern "C" int mnpb_cgemm_tf32_noalloc(void *stream, int64_t m, int64_t n, int64_t k,
+                                       int64_t batch, float alpha, const float *A, int64_t lda,
+                                       int64_t planeA, int64_t sA, const float *B, int64_t ldb,
+                                       int64_t planeB, int64_t sB, float beta, float *C,
+                                       int64_t ldc, int64_t planeC, int64_t sC) {
+    clear_error();
+    MNPB_REQUIRE(m >= 0 && n >= 0 && k > 0 && batch > 0 && batch < 65536,
+                 "cgemm_tf32_noalloc: bad sizes");
+    MNPB_REQUIRE(A && B && C, "cgemm_tf32_noalloc: null pointer");
+    if (m > (int64_t(1) << 30) || k > (int64_t(1) << 30)) {
+        set_error("cgemm_tf32_noalloc: m or k too large");
+        return MNPB_EINVAL;
+    }
+    const int64_t need = tc::cgemm_tf32_workspace((int)m, (int)k, (int)batch);
+    if (need > tc::kStaticPackBytes) {
+        set_error("cgemm_tf32_noalloc: packed A needs %lld bytes (m=%lld k=%lld batch=%lld), "
+                  "the static scratch holds %lld; use mnpb_cgemm_tf32 with a workspace",
+                  (long long)need, (long long)m, (long long)k, (long long)batch,
+                  (long long)tc::kStaticPackBytes);
+        return MNPB_ENOMEM;
+    }
+    float *scratch = nullptr;
+    MNPB_TRY(tc::static_pack_scratch(&scratch));
+    tc::CMatF a{(float *)A, lda, planeA, sA}, b{(float *)B, ldb, planeB, sB}, c{C, ldc, planeC, sC};
+    return tc::cgemm_tf32(as_stream(stream), (int)m, (int)n, (int)k, (int)batch, alpha, a, b,
+                          beta, c, scratch, tc::kStaticPackBytes);
+}
