@@ -27,7 +27,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 
 SPHERES = [(32, 10.0), (60, 10.0), (144, 10.0), (144, 20.0), (256, 20.0), (1444, 40.0)]
-RODS = [(20.0, 80.0, (31, 21, 41))]
+RODS = [(20.0, 80.0, (31, 21, 41)), (20.0, 80.0, (61, 31, 101)), (20.0, 80.0, (97, 47, 171))]
 
 
 def main(ref_root):

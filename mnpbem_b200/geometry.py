@@ -648,9 +648,43 @@ def trisphere(n, diameter, interp='curv'):
     return Particle(v, f, interp='curv')._as_flat()
 
 
+def trirod(diameter, height, n):
+    """Flat rod mesh (cylinder with hemispherical caps), quads + triangles.
+
+    Only the packaged parameter sets are available; they are the reference's
+    ``trirod(diameter, height, n)`` (mnpbem/geometry/mesh_generators.py:592).
+    """
+    v, f = load_mesh('trirod_{:g}_{:g}_{}_{}_{}'.format(float(diameter), float(height), *n))
+    return Particle(v, f, interp='flat')
+
+
 def _as_flat(self):
     return Particle(self.verts, self.faces, interp='flat', rule=self.quad_rules.rule,
                     npol=self.quad_rules.npol)
 
 
+def _transformed(self, fn):
+    if self.verts2 is not None:
+        v, f = fn(self.verts2), self.faces2
+    else:
+        v, f = fn(self.verts), self.faces
+    return Particle(v, f, interp=self.interp, rule=self.quad_rules.rule,
+                    npol=self.quad_rules.npol)
+
+
+def _shift(self, vec):
+    """Translated copy (vertices + vec), as mnpbem/geometry/particle.py:755."""
+    vec = np.asarray(vec, dtype=float)
+    return _transformed(self, lambda v: v + vec)
+
+
+def _scale(self, factor):
+    """Scaled copy (vertices * factor, scalar or per axis), as
+    mnpbem/geometry/particle.py:820."""
+    factor = np.asarray(factor, dtype=float)
+    return _transformed(self, lambda v: v * factor)
+
+
 Particle._as_flat = _as_flat
+Particle.shift = _shift
+Particle.scale = _scale
