@@ -340,6 +340,79 @@ int mnpb_farfield(void *stream, int64_t n, int64_t batch, int64_t npol, int64_t 
                   const int8_t *side_out, const double *dirs, const double *kmed,
                   const double *k0, const double *sol, double *e_out, double *h_out);
 
+/* ---------------------------------------------------------------------------
+ * H-matrices and GMRES (iterative retarded solver, BEMRetIter)
+ *
+ * Block rectangles are int32 quadruples (row start, rows, col start, cols) in
+ * cluster positions; c2p (int32, n) maps a cluster position to a face.  Dense
+ * matrices are complex128, column-major, face order.
+ * ------------------------------------------------------------------------- */
+
+/* Partially-pivoted ACA of nblk low-rank blocks of A, one CTA per block, in
+ * FP64.  UV: FP64 complex scratch; block b writes U (rows x cap) at
+ * UV + 2*offU[b] doubles and V (cols x cap) at UV + 2*offV[b], cap =
+ * min(rows, cols, kmax); rank[b] receives the rank.  max_mn: largest
+ * rows + cols.  kmax <= 128.  Replaces HMatrix.aca/_aca_block
+ * (mnpbem/greenfun/hmatrix.py:159-336) over ACACompGreenRet._eval_elements
+ * (mnpbem/greenfun/aca_compgreen_ret.py:196-208). */
+int mnpb_hmat_aca(void *stream, int64_t n, const double *A, int64_t lda, const int32_t *c2p,
+                  int64_t nblk, const int32_t *blocks, const int64_t *offU, const int64_t *offV,
+                  int64_t max_mn, int64_t kmax, double htol, double *UV, int32_t *rank);
+
+/* Dense (leaf x leaf) blocks of A as complex64, block b at out + 2*offD[b]
+ * floats, column-major.  Replaces the dense-block fill of HMatrix.aca
+ * (mnpbem/greenfun/hmatrix.py:173-181). */
+int mnpb_hmat_gather_dense(void *stream, const double *A, int64_t lda, const int32_t *c2p,
+                           int64_t nblk, const int32_t *blocks, const int64_t *offD, float *out);
+
+/* ACA factors from the FP64 scratch of mnpb_hmat_aca to complex64 storage
+ * with rank columns each: U of block b at U + 2*outU[b], V at V + 2*outV[b]. */
+int mnpb_hmat_compact(void *stream, int64_t nblk, const int32_t *blocks, const int32_t *rank,
+                      const int64_t *offU, const int64_t *offV, const double *UV,
+                      const int64_t *outU, const int64_t *outV, float *U, float *V);
+
+/* Y_i = H_i X_i for nmat (<= 4) H-matrices of one block partition; descs
+ * points to nmat host records of 11 pointers each: D, U, V, rank, offD,
+ * offU, offV, offT, X, Y, T (X, Y: complex128 n x nc, column stride n, face
+ * order; T: FP64 scratch of 2 * min(nc, 8) * sum(rank) doubles).  leaf_rows:
+ * int32 (start, rows) per leaf cluster; lptr/lent: CSR list per leaf of
+ * contributing blocks (e >= 0 dense block e, e < 0 low-rank block -e-1).
+ * Replaces HMatrix.mtimes_vec (mnpbem/greenfun/hmatrix.py:450-541). */
+int mnpb_hmat_matvec(void *stream, int64_t n, int64_t nc, int64_t nmat, const void *descs,
+                     const int32_t *c2p, int64_t ndense, const int32_t *dense, int64_t nlr,
+                     const int32_t *lowrank, int64_t nleaf, const int32_t *leaf_rows,
+                     const int32_t *lptr, const int32_t *lent);
+
+/* y = A x of the packed retarded operator from the four products P1 = G1 v1,
+ * P2 = G2 v2, Q1 = H1 v1, Q2 = H2 v2 (n x 4*nrhs each, columns sig then h
+ * x, y, z), scalar eps1/eps2, vacuum wavenumber k; y in the excitation layout
+ * of mnpb_bemret_excitation.  Replaces BEMRetIter._afun
+ * (mnpbem/bem/bem_ret_iter.py:1362-1501). */
+int mnpb_bem_afun(void *stream, int64_t n, int64_t nrhs, const double *P1, const double *P2,
+                  const double *Q1, const double *Q2, double *y, double e1_re, double e1_im,
+                  double e2_re, double e2_im, double k, const double *nvec);
+
+/* GMRES steps in FP64 (the Krylov solver of scipy.sparse.linalg.gmres as
+ * called by mnpbem/bem/bem_iter.py:79-89).  Vectors complex128 of length L;
+ * basis V column-major (column stride ldv); Hessenberg H column-major.
+ * arnoldi: CGS2 orthogonalisation of w against V[:, 0..j], H column j
+ * (Hcol, j + 2 entries) and V[:, j+1] = w / |w|; nrm (device) = |w|.
+ * givens: rotations on column j, new rotation j, g update; out (device) =
+ * |g[j+1]|.  update: y = R^{-1} g (m x m), x += V[:, 0..m-1] y. */
+int64_t mnpb_gmres_workspace(int64_t L, int64_t jmax);
+int mnpb_gmres_arnoldi(void *stream, int64_t L, int64_t j, double *V, int64_t ldv, double *w,
+                       double *Hcol, double *nrm, void *work, int64_t work_bytes);
+int mnpb_gmres_givens(void *stream, int64_t j, double *H, int64_t ldh, double *cs, double *sn,
+                      double *g, double *out);
+int mnpb_gmres_update(void *stream, int64_t L, int64_t m, const double *H, int64_t ldh,
+                      const double *g, const double *V, int64_t ldv, double *y, double *x);
+
+/* out[v] = |x_v| (FP64, device) for nvec complex128 vectors of length L at
+ * x + 2*v*ldx doubles; partial: nvec * ceil(L / 2048) doubles of scratch.
+ * Replaces the np.linalg.norm calls of mnpbem/bem/bem_iter.py:88. */
+int mnpb_vec_norms(void *stream, int64_t L, int64_t nvec, const double *x, int64_t ldx,
+                   double *partial, double *out);
+
 #ifdef __cplusplus
 }
 #endif

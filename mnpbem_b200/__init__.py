@@ -1,6 +1,7 @@
 """mnpbem_b200 -- the boundary-element hot path of PyMNPBEM on NVIDIA B200.
 
 Drop-in classes with the reference call surface (``BEMRet``, ``BEMStat``,
+``BEMRetIter``,
 ``CompGreenRet``, ``CompGreenStat``, ``PlaneWaveRet``, ``PlaneWaveStat``,
 ``CompStruct``, ``ComParticle``) backed by hand-written sm_100a CUDA kernels
 in ``libmnpbem_b200.so`` (C ABI: include/mnpbem_b200.h).  There is no CPU
@@ -8,7 +9,8 @@ fallback: importing the solvers requires the built library.
 """
 
 from .compstruct import CompStruct
-from .geometry import Particle, ComParticle, trisphere, load_mesh
+from .geometry import Particle, ComParticle, trisphere, trirod, load_mesh
+from .clustertree import ClusterTree
 from .materials import EpsConst, EpsDrude
 
 __version__ = "1.0.0"
@@ -19,6 +21,9 @@ def __getattr__(name):
     if name in ('BEMRet', 'BEMStat'):
         from . import bem
         return getattr(bem, name)
+    if name in ('BEMRetIter',):
+        from . import bem_iter
+        return getattr(bem_iter, name)
     if name in ('CompGreenRet', 'CompGreenStat'):
         from . import greenfun
         return getattr(greenfun, name)

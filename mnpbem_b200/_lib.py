@@ -60,6 +60,16 @@ SIGNATURES = {
     'mnpb_cgemm_tf32_noalloc': [_P, _I64, _I64, _I64, _I64, C.c_float, _P, _I64, _I64, _I64,
                                 _P, _I64, _I64, _I64, C.c_float, _P, _I64, _I64, _I64],
     'mnpb_tc_error': [_P, _P],
+    'mnpb_hmat_aca': [_P, _I64, _P, _I64, _P, _I64, _P, _P, _P, _I64, _I64, _D, _P, _P],
+    'mnpb_hmat_gather_dense': [_P, _P, _I64, _P, _I64, _P, _P, _P],
+    'mnpb_hmat_compact': [_P, _I64, _P, _P, _P, _P, _P, _P, _P, _P, _P],
+    'mnpb_hmat_matvec': [_P, _I64, _I64, _I64, _P, _P, _I64, _P, _I64, _P, _I64, _P, _P, _P],
+    'mnpb_bem_afun': [_P, _I64, _I64, _P, _P, _P, _P, _P, _D, _D, _D, _D, _D, _P],
+    'mnpb_gmres_workspace': [_I64, _I64],
+    'mnpb_gmres_arnoldi': [_P, _I64, _I64, _P, _I64, _P, _P, _P, _P, _I64],
+    'mnpb_gmres_givens': [_P, _I64, _P, _I64, _P, _P, _P, _P],
+    'mnpb_gmres_update': [_P, _I64, _I64, _P, _I64, _P, _P, _I64, _P, _P],
+    'mnpb_vec_norms': [_P, _I64, _I64, _P, _I64, _P, _P],
     'mnpb_stat_matrix': [_P, _I64, _I64, _P, _I64, _P, _P, _I64, _I64],
     'mnpb_planewave_potential': [_P, _I64, _I64, _I64, _P, _P, _P, _P, _P, _P, _P, _P, _P],
     'mnpb_farfield': [_P, _I64, _I64, _I64, _I64, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P],
@@ -67,7 +77,7 @@ SIGNATURES = {
 _RESTYPE = {'mnpb_last_error': C.c_char_p, 'mnpb_launch_count': C.c_int64,
             'mnpb_cgemm_tf32_workspace': C.c_int64, 'mnpb_bemret_workspace_mixed': C.c_int64,
             'mnpb_bemret_refine_workspace': C.c_int64, 'mnpb_f32_workspace': C.c_int64, 'mnpb_bemret_dinv_floats': C.c_int64,
-            'mnpb_bemret_workspace_f64': C.c_int64}
+            'mnpb_bemret_workspace_f64': C.c_int64, 'mnpb_gmres_workspace': C.c_int64}
 
 _lib = None
 
@@ -111,7 +121,7 @@ def launch_count():
 
 PROF_CLASSES = ['assemble', 'refine', 'zgemm_f64', 'lu_panel', 'trsm_small', 'swap',
                 'elementwise', 'tc_gemm', 'farfield', 'sgemm_f32', 'matvec', 'trsv',
-                'tc_pack', 'refine_elementwise']
+                'tc_pack', 'refine_elementwise', 'aca', 'hmat_matvec', 'gmres_arnoldi', 'mlp']
 
 
 def prof_begin():
@@ -121,7 +131,7 @@ def prof_begin():
 def prof_end():
     """{class: (ms, work, launches)} for the launches since prof_begin()."""
     import numpy as np
-    n = 16
+    n = 24
     ms = np.zeros(n)
     work = np.zeros(n)
     cnt = np.zeros(n, dtype=np.int64)

@@ -65,7 +65,11 @@ enum ProfClass {
     PC_TRSV = 11,      // one-launch triangular solves, work = bytes of the triangle
     PC_PACK = 12,      // tensor-core operand packing
     PC_REFINE_EW = 13, // refinement element-wise kernels (residual, norms, conversions)
-    PC_COUNT = 16
+    PC_ACA = 14,       // ACA of low-rank blocks, dense-block gather
+    PC_HMATVEC = 15,   // H-matrix times vectors
+    PC_GMRES = 16,     // Arnoldi orthogonalisation (work = bytes of the basis read)
+    PC_MLP = 17,       // warm-start network kernels
+    PC_COUNT = 24
 };
 bool prof_on();
 void prof_record(cudaStream_t s, int cls, double work, bool start);

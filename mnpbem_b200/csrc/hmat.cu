@@ -1,0 +1,510 @@
+// H-matrix kernels of the iterative retarded solver:
+//
+//  * partially-pivoted ACA of every low-rank block, one CTA per block, in FP64
+//    from the dense FP64 matrix (the reference samples its dense matrix the
+//    same way, mnpbem/greenfun/aca_compgreen_ret.py:196-208 and
+//    mnpbem/greenfun/hmatrix.py:195-336);
+//  * gather of the dense (leaf x leaf) blocks and compaction of the ACA
+//    factors into complex64 storage;
+//  * H-matrix times a few vectors (hmatrix.py:450-541) in two bandwidth-bound
+//    launches: t_b = V_b^T x for every low-rank block, then one CTA per leaf
+//    cluster sums the dense and U_b t_b contributions of its rows.  Each row
+//    has exactly one writer, so the result is deterministic (no atomics);
+//    factors are read as complex64 and accumulated in FP64;
+//  * the packed 8N BEM operator on top of the four products
+//    (mnpb_bem_afun, mnpbem/bem/bem_ret_iter.py:1362-1501, scalar eps).
+//
+// Matrices are column-major complex128 (A[i + j * lda]) in face order; block
+// coordinates are cluster positions, mapped to faces by c2p.
+#include "common.cuh"
+
+namespace mnpb {
+namespace hm {
+
+constexpr int ACA_T = 256;
+constexpr int ACA_MAXK = 128;   // largest supported kmax
+
+// complex arithmetic without contraction (same rounding as NumPy's complex
+// multiply a*b = (ar br - ai bi, ar bi + ai br))
+__device__ __forceinline__ cd mul_nf(cd a, cd b) {
+    return make_double2(__dsub_rn(__dmul_rn(a.x, b.x), __dmul_rn(a.y, b.y)),
+                        __dadd_rn(__dmul_rn(a.x, b.y), __dmul_rn(a.y, b.x)));
+}
+__device__ __forceinline__ cd sub_nf(cd a, cd b) {
+    return make_double2(__dsub_rn(a.x, b.x), __dsub_rn(a.y, b.y));
+}
+// Smith's complex division (R. L. Smith, CACM 5, 435 (1962)), the algorithm
+// NumPy's complex divide uses; b != 0 here.
+__device__ __forceinline__ cd div_smith(cd a, cd b) {
+    if (fabs(b.x) >= fabs(b.y)) {
+        const double rat = __ddiv_rn(b.y, b.x);
+        const double scl = __ddiv_rn(1.0, __dadd_rn(b.x, __dmul_rn(b.y, rat)));
+        return make_double2(__dmul_rn(__dadd_rn(a.x, __dmul_rn(a.y, rat)), scl),
+                            __dmul_rn(__dsub_rn(a.y, __dmul_rn(a.x, rat)), scl));
+    }
+    const double rat = __ddiv_rn(b.x, b.y);
+    const double scl = __ddiv_rn(1.0, __dadd_rn(b.y, __dmul_rn(b.x, rat)));
+    return make_double2(__dmul_rn(__dadd_rn(__dmul_rn(a.x, rat), a.y), scl),
+                        __dmul_rn(__dsub_rn(__dmul_rn(a.y, rat), a.x), scl));
+}
+__device__ __forceinline__ cd cconj_mul(cd a, cd b) {   // conj(a) * b
+    return make_double2(a.x * b.x + a.y * b.y, a.x * b.y - a.y * b.x);
+}
+
+struct ArgMax {
+    double v;
+    int i;
+};
+// larger value wins; on equal values the smaller index (np.argmax's first hit)
+__device__ __forceinline__ ArgMax amax(ArgMax a, ArgMax b) {
+    if (b.v > a.v || (b.v == a.v && b.i < a.i)) return b;
+    return a;
+}
+__device__ ArgMax block_argmax(ArgMax a, ArgMax *sh) {
+    for (int o = 16; o > 0; o >>= 1) {
+        ArgMax b{__shfl_xor_sync(0xffffffffu, a.v, o), __shfl_xor_sync(0xffffffffu, a.i, o)};
+        a = amax(a, b);
+    }
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    __syncthreads();
+    if (l == 0) sh[w] = a;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        ArgMax r = sh[0];
+        for (int k = 1; k < (int)(blockDim.x >> 5); ++k) r = amax(r, sh[k]);
+        sh[0] = r;
+    }
+    __syncthreads();
+    return sh[0];
+}
+__device__ double block_sum(double a, double *sh) {
+    for (int o = 16; o > 0; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    __syncthreads();
+    if (l == 0) sh[w] = a;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double r = 0.0;
+        for (int k = 0; k < (int)(blockDim.x >> 5); ++k) r += sh[k];
+        sh[0] = r;
+    }
+    __syncthreads();
+    return sh[0];
+}
+
+// One CTA per low-rank block.  U (m x cap) and V (n x cap) are column-major
+// FP64 scratch at UV + offU[b] / offV[b]; the block is ~ U V^T with the rank
+// written to rank_out[b].  Dynamic shared memory: m + n used-flags.
+__global__ void __launch_bounds__(ACA_T) aca_kernel(const cd *__restrict__ A, int64_t lda,
+                                                    const int *__restrict__ c2p,
+                                                    const int4 *__restrict__ blk,
+                                                    const int64_t *__restrict__ offU,
+                                                    const int64_t *__restrict__ offV, int kmax,
+                                                    double htol, cd *UV, int *rank_out) {
+    extern __shared__ unsigned char used[];
+    __shared__ cd sk[ACA_MAXK];
+    __shared__ ArgMax sa[32];
+    __shared__ double sd[32];
+    __shared__ double cross[ACA_MAXK];
+    __shared__ int s_stop;
+    const int4 bk = blk[blockIdx.x];
+    const int r0 = bk.x, m = bk.y, c0 = bk.z, n = bk.w;
+    const int cap = min(min(m, n), kmax);
+    cd *U = UV + offU[blockIdx.x];
+    cd *V = UV + offV[blockIdx.x];
+    for (int e = threadIdx.x; e < m + n; e += blockDim.x) used[e] = 0;
+    int rank = 0, prow = 0;
+    double fro = 0.0;
+    __syncthreads();
+    for (int it = 0; it < cap; ++it) {
+        // residual row prow: A(prow, :) - sum_r U[prow, r] V[:, r]
+        for (int r = threadIdx.x; r < rank; r += blockDim.x) sk[r] = U[prow + (int64_t)r * m];
+        __syncthreads();
+        const int64_t grow = c2p[r0 + prow];
+        ArgMax best{-1.0, 0x7fffffff};
+        double vsq = 0.0;
+        cd *vrow = V + (int64_t)rank * n;
+        for (int j = threadIdx.x; j < n; j += blockDim.x) {
+            cd v = A[grow + (int64_t)c2p[c0 + j] * lda];
+            for (int r = 0; r < rank; ++r) v = sub_nf(v, mul_nf(sk[r], V[j + (int64_t)r * n]));
+            vrow[j] = v;
+            vsq += v.x * v.x + v.y * v.y;
+            const double a = used[m + j] ? 0.0 : hypot(v.x, v.y);
+            best = amax(best, ArgMax{a, j});
+        }
+        best = block_argmax(best, sa);
+        const int pcol = best.i;
+        vsq = block_sum(vsq, sd);
+        const cd piv = vrow[pcol];
+        if (hypot(piv.x, piv.y) < 1e-15) break;
+        // residual column pcol, divided by the pivot
+        for (int r = threadIdx.x; r < rank; r += blockDim.x) sk[r] = V[pcol + (int64_t)r * n];
+        __syncthreads();
+        const int64_t gcol = (int64_t)c2p[c0 + pcol] * lda;
+        cd *ucol = U + (int64_t)rank * m;
+        ArgMax nextr{-1.0, 0x7fffffff};
+        double usq = 0.0;
+        for (int i = threadIdx.x; i < m; i += blockDim.x) {
+            cd c = A[c2p[r0 + i] + gcol];
+            for (int r = 0; r < rank; ++r) c = sub_nf(c, mul_nf(sk[r], U[i + (int64_t)r * m]));
+            const cd u = div_smith(c, piv);
+            ucol[i] = u;
+            usq += u.x * u.x + u.y * u.y;
+            const double a = (used[i] || i == prow) ? 0.0 : hypot(u.x, u.y);
+            nextr = amax(nextr, ArgMax{a, i});
+        }
+        nextr = block_argmax(nextr, sa);
+        usq = block_sum(usq, sd);
+        ++rank;
+        // cross terms 2 Re(<U_j, u><V_j, v>) for the earlier columns, one warp per j
+        const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+        for (int j = w; j < rank - 1; j += (int)(blockDim.x >> 5)) {
+            cd du = cmk(0, 0), dv = cmk(0, 0);
+            for (int i = l; i < m; i += 32) du = cadd(du, cconj_mul(U[i + (int64_t)j * m], ucol[i]));
+            for (int i = l; i < n; i += 32) dv = cadd(dv, cconj_mul(V[i + (int64_t)j * n], vrow[i]));
+            for (int o = 16; o > 0; o >>= 1) {
+                du.x += __shfl_xor_sync(0xffffffffu, du.x, o);
+                du.y += __shfl_xor_sync(0xffffffffu, du.y, o);
+                dv.x += __shfl_xor_sync(0xffffffffu, dv.x, o);
+                dv.y += __shfl_xor_sync(0xffffffffu, dv.y, o);
+            }
+            if (l == 0) cross[j] = 2.0 * (du.x * dv.x - du.y * dv.y);
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            used[prow] = 1;
+            used[m + pcol] = 1;
+            const double nw = usq * vsq;
+            double cr = 0.0;
+            for (int j = 0; j < rank - 1; ++j) cr += cross[j];
+            fro += nw + cr;
+            s_stop = (fro > 0.0 && sqrt(nw) < htol * sqrt(fabs(fro))) ? 1 : 0;
+        }
+        __syncthreads();
+        if (s_stop) break;
+        prow = nextr.i;
+    }
+    if (threadIdx.x == 0) rank_out[blockIdx.x] = rank;
+}
+
+// Dense blocks: out[offD[b] + i + j*m] = A(c2p[r0+i], c2p[c0+j]) as complex64.
+__global__ void gather_dense_kernel(const cd *__restrict__ A, int64_t lda,
+                                    const int *__restrict__ c2p, const int4 *__restrict__ blk,
+                                    const int64_t *__restrict__ offD, float2 *__restrict__ out) {
+    const int4 bk = blk[blockIdx.x];
+    float2 *o = out + offD[blockIdx.x];
+    const int64_t tot = (int64_t)bk.y * bk.w;
+    for (int64_t e = threadIdx.x; e < tot; e += blockDim.x) {
+        const int i = (int)(e % bk.y), j = (int)(e / bk.y);
+        const cd v = A[c2p[bk.x + i] + (int64_t)c2p[bk.z + j] * lda];
+        o[e] = make_float2((float)v.x, (float)v.y);
+    }
+}
+
+// ACA factors (FP64 scratch, capacity columns) -> complex64 at their final
+// offsets, rank columns each.
+__global__ void compact_kernel(const int4 *__restrict__ blk, const int *__restrict__ rank,
+                               const int64_t *__restrict__ offU, const int64_t *__restrict__ offV,
+                               const cd *__restrict__ UV, const int64_t *__restrict__ outU,
+                               const int64_t *__restrict__ outV, float2 *__restrict__ fU,
+                               float2 *__restrict__ fV) {
+    const int b = blockIdx.x;
+    const int4 bk = blk[b];
+    const int r = rank[b];
+    const int64_t nu = (int64_t)bk.y * r, nv = (int64_t)bk.w * r;
+    for (int64_t e = threadIdx.x; e < nu; e += blockDim.x) {
+        const cd v = UV[offU[b] + e];
+        fU[outU[b] + e] = make_float2((float)v.x, (float)v.y);
+    }
+    for (int64_t e = threadIdx.x; e < nv; e += blockDim.x) {
+        const cd v = UV[offV[b] + e];
+        fV[outV[b] + e] = make_float2((float)v.x, (float)v.y);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// H-matrix times vectors
+// ---------------------------------------------------------------------------
+// Per matrix (up to 4 in one launch, blockIdx.y):
+struct HMat {
+    const float2 *D;      // dense blocks, column-major, at offD
+    const float2 *U, *V;  // low-rank factors, column-major, at offU / offV
+    const int *rank;      // per low-rank block
+    const int64_t *offD, *offU, *offV, *offT;   // offT: t_b at T + offT[b] * nc
+    const cd *X;          // n x nc input (face order), column stride n
+    cd *Y;                // n x nc output (face order)
+    cd *T;                // scratch V^T x
+};
+struct HMats {
+    HMat h[4];
+};
+
+// t_b = V_b^T x[cols]: one CTA per low-rank block, one warp per factor column.
+template <int NC>
+__global__ void __launch_bounds__(256) hm_vtx_kernel(HMats P, int n, int nc,
+                                                     const int4 *__restrict__ lr,
+                                                     const int *__restrict__ c2p) {
+    const HMat &H = P.h[blockIdx.y];
+    const int b = blockIdx.x;
+    const int4 bk = lr[b];
+    const int r = H.rank[b];
+    const float2 *V = H.V + H.offV[b];
+    cd *T = H.T + H.offT[b] * nc;
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    for (int q = w; q < r; q += 8) {
+        cd acc[NC];
+#pragma unroll
+        for (int c = 0; c < NC; ++c) acc[c] = cmk(0, 0);
+        const float2 *vq = V + (int64_t)q * bk.w;
+        for (int j = l; j < bk.w; j += 32) {
+            const float2 v = vq[j];
+            const cd vv = cmk(v.x, v.y);
+            const int64_t row = c2p[bk.z + j];
+#pragma unroll
+            for (int c = 0; c < NC; ++c)
+                if (c < nc) acc[c] = cfma(vv, H.X[row + (int64_t)c * n], acc[c]);
+        }
+#pragma unroll
+        for (int c = 0; c < NC; ++c) {
+            for (int o = 16; o > 0; o >>= 1) {
+                acc[c].x += __shfl_xor_sync(0xffffffffu, acc[c].x, o);
+                acc[c].y += __shfl_xor_sync(0xffffffffu, acc[c].y, o);
+            }
+        }
+        if (l == 0)
+            for (int c = 0; c < nc; ++c) T[(int64_t)q * nc + c] = acc[c];
+    }
+}
+
+// One CTA per leaf cluster (rows leaf_rows[L].x .. +leaf_rows[L].y): 64 rows
+// x 4 lanes over the columns of each contributing block.  Contribution list
+// (CSR over leaves): entry e >= 0 is dense block e, entry e < 0 low-rank block
+// -e-1.
+constexpr int HM_ROWS = 64, HM_KL = 4;
+template <int NC>
+__global__ void __launch_bounds__(256) hm_rows_kernel(HMats P, int n, int nc,
+                                                      const int2 *__restrict__ leaf_rows,
+                                                      const int *__restrict__ lptr,
+                                                      const int *__restrict__ lent,
+                                                      const int4 *__restrict__ dn,
+                                                      const int4 *__restrict__ lr,
+                                                      const int *__restrict__ c2p) {
+    __shared__ cd part[HM_KL][HM_ROWS][NC];
+    const HMat &H = P.h[blockIdx.y];
+    const int2 lf = leaf_rows[blockIdx.x];
+    const int rl = threadIdx.x % HM_ROWS, kl = threadIdx.x / HM_ROWS;
+    for (int rbase = 0; rbase < lf.y; rbase += HM_ROWS) {
+        const int row = lf.x + rbase + rl;     // cluster position
+        const bool live = rbase + rl < lf.y;
+        cd acc[NC];
+#pragma unroll
+        for (int c = 0; c < NC; ++c) acc[c] = cmk(0, 0);
+        for (int e = lptr[blockIdx.x]; e < lptr[blockIdx.x + 1]; ++e) {
+            const int id = lent[e];
+            if (id >= 0) {
+                const int4 bk = dn[id];
+                const float2 *D = H.D + H.offD[id] + (row - bk.x);
+                if (live)
+                    for (int j = kl; j < bk.w; j += HM_KL) {
+                        const float2 a = D[(int64_t)j * bk.y];
+                        const cd aa = cmk(a.x, a.y);
+                        const int64_t xr = c2p[bk.z + j];
+#pragma unroll
+                        for (int c = 0; c < NC; ++c)
+                            if (c < nc) acc[c] = cfma(aa, H.X[xr + (int64_t)c * n], acc[c]);
+                    }
+            } else {
+                const int b = -id - 1;
+                const int4 bk = lr[b];
+                const int r = H.rank[b];
+                const float2 *U = H.U + H.offU[b] + (row - bk.x);
+                const cd *T = H.T + H.offT[b] * nc;
+                if (live)
+                    for (int q = kl; q < r; q += HM_KL) {
+                        const float2 a = U[(int64_t)q * bk.y];
+                        const cd aa = cmk(a.x, a.y);
+#pragma unroll
+                        for (int c = 0; c < NC; ++c)
+                            if (c < nc) acc[c] = cfma(aa, T[(int64_t)q * nc + c], acc[c]);
+                    }
+            }
+        }
+#pragma unroll
+        for (int c = 0; c < NC; ++c) part[kl][rl][c] = acc[c];
+        __syncthreads();
+        for (int e = threadIdx.x; e < HM_ROWS * nc; e += blockDim.x) {
+            const int r = e % HM_ROWS, c = e / HM_ROWS;
+            if (rbase + r < lf.y) {
+                cd v = part[0][r][c];
+#pragma unroll
+                for (int q = 1; q < HM_KL; ++q) v = cadd(v, part[q][r][c]);
+                H.Y[c2p[lf.x + rbase + r] + (int64_t)c * n] = v;
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// y = A x for the packed operator.  P1 = G1 [sig1|h1], P2 = G2 [sig2|h2],
+// Q1 = H1 [sig1|h1], Q2 = H2 [sig2|h2], each n x 4K (columns sig then h x,y,z,
+// K each); y uses the excitation layout [phi | a (3) | De | alpha (3)].
+__global__ void afun_kernel(int n, int K, const cd *P1, const cd *P2, const cd *Q1,
+                            const cd *Q2, cd *y, cd e1, cd e2, double k,
+                            const double *__restrict__ nvec) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const cd ik = cmk(0.0, k);
+    const double nv[3] = {nvec[3 * i], nvec[3 * i + 1], nvec[3 * i + 2]};
+    auto at = [&](const cd *p, int col) { return p[(int64_t)col * n + i]; };
+    for (int q = 0; q < K; ++q) {
+        const cd gs1 = at(P1, q), gs2 = at(P2, q), hs1 = at(Q1, q), hs2 = at(Q2, q);
+        const cd egs = csub(cmul(e1, gs1), cmul(e2, gs2));
+        cd negh = cmk(0, 0);
+        y[(int64_t)q * n + i] = csub(gs1, gs2);
+        for (int c = 0; c < 3; ++c) {
+            const int col = K + c * K + q;
+            const cd gh1 = at(P1, col), gh2 = at(P2, col), hh1 = at(Q1, col), hh2 = at(Q2, col);
+            y[(int64_t)(K + c * K + q) * n + i] = csub(gh1, gh2);
+            y[(int64_t)(5 * K + c * K + q) * n + i] =
+                csub(csub(hh1, hh2), cmul(ik, cscale(egs, nv[c])));
+            negh = cadd(negh, cscale(csub(cmul(e1, gh1), cmul(e2, gh2)), nv[c]));
+        }
+        y[(int64_t)(4 * K + q) * n + i] =
+            csub(csub(cmul(e1, hs1), cmul(e2, hs2)), cmul(ik, negh));
+    }
+}
+
+}  // namespace hm
+}  // namespace mnpb
+
+using namespace mnpb;
+
+extern "C" int mnpb_hmat_aca(void *stream, int64_t n, const double *A, int64_t lda,
+                             const int32_t *c2p, int64_t nblk, const int32_t *blocks,
+                             const int64_t *offU, const int64_t *offV, int64_t max_mn,
+                             int64_t kmax, double htol, double *UV, int32_t *rank) {
+    clear_error();
+    MNPB_REQUIRE(n > 0 && lda >= n && nblk >= 0 && kmax > 0 && kmax <= hm::ACA_MAXK && htol > 0,
+                 "hmat_aca: bad sizes (kmax <= %d)", hm::ACA_MAXK);
+    if (nblk == 0) return MNPB_OK;
+    MNPB_REQUIRE(A && c2p && blocks && offU && offV && UV && rank, "hmat_aca: null pointer");
+    MNPB_REQUIRE(max_mn > 0 && max_mn <= 200 * 1024, "hmat_aca: block too large (m + n = %lld)",
+                 (long long)max_mn);
+    cudaStream_t s = as_stream(stream);
+    const int smem = (int)max_mn;
+    if (smem > 48 * 1024 &&
+        cudaFuncSetAttribute(hm::aca_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) !=
+            cudaSuccess) {
+        set_error("hmat_aca: cannot reserve %d bytes of shared memory", smem);
+        return MNPB_ECUDA;
+    }
+    ProfScope ps(s, PC_ACA, 0.0);
+    hm::aca_kernel<<<(unsigned)nblk, hm::ACA_T, smem, s>>>(
+        (const cd *)A, lda, c2p, (const int4 *)blocks, offU, offV, (int)kmax, htol, (cd *)UV, rank);
+    MNPB_LAUNCH_CHECK("aca_kernel");
+    return MNPB_OK;
+}
+
+extern "C" int mnpb_hmat_gather_dense(void *stream, const double *A, int64_t lda,
+                                      const int32_t *c2p, int64_t nblk, const int32_t *blocks,
+                                      const int64_t *offD, float *out) {
+    clear_error();
+    if (nblk == 0) return MNPB_OK;
+    MNPB_REQUIRE(A && c2p && blocks && offD && out && lda > 0, "hmat_gather_dense: bad arguments");
+    cudaStream_t s = as_stream(stream);
+    ProfScope ps(s, PC_ACA, 0.0);
+    hm::gather_dense_kernel<<<(unsigned)nblk, 256, 0, s>>>((const cd *)A, lda, c2p,
+                                                          (const int4 *)blocks, offD, (float2 *)out);
+    MNPB_LAUNCH_CHECK("gather_dense_kernel");
+    return MNPB_OK;
+}
+
+extern "C" int mnpb_hmat_compact(void *stream, int64_t nblk, const int32_t *blocks,
+                                 const int32_t *rank, const int64_t *offU, const int64_t *offV,
+                                 const double *UV, const int64_t *outU, const int64_t *outV,
+                                 float *U, float *V) {
+    clear_error();
+    if (nblk == 0) return MNPB_OK;
+    MNPB_REQUIRE(blocks && rank && offU && offV && UV && outU && outV && U && V,
+                 "hmat_compact: null pointer");
+    cudaStream_t s = as_stream(stream);
+    hm::compact_kernel<<<(unsigned)nblk, 256, 0, s>>>((const int4 *)blocks, rank, offU, offV,
+                                                     (const cd *)UV, outU, outV, (float2 *)U,
+                                                     (float2 *)V);
+    MNPB_LAUNCH_CHECK("compact_kernel");
+    return MNPB_OK;
+}
+
+// One matrix of an H-matrix product, as passed through the C ABI.
+struct mnpb_hmat_desc {
+    const float *D, *U, *V;
+    const int32_t *rank;
+    const int64_t *offD, *offU, *offV, *offT;
+    const double *X;
+    double *Y, *T;
+};
+
+extern "C" int mnpb_hmat_matvec(void *stream, int64_t n, int64_t nc, int64_t nmat,
+                                const void *descs, const int32_t *c2p, int64_t ndense,
+                                const int32_t *dense, int64_t nlr, const int32_t *lowrank,
+                                int64_t nleaf, const int32_t *leaf_rows, const int32_t *lptr,
+                                const int32_t *lent) {
+    clear_error();
+    MNPB_REQUIRE(n > 0 && nc > 0 && nc <= 64 && nmat >= 1 && nmat <= 4 && nleaf > 0,
+                 "hmat_matvec: bad sizes (nc <= 64, nmat <= 4)");
+    MNPB_REQUIRE(descs && c2p && leaf_rows && lptr && lent, "hmat_matvec: null pointer");
+    cudaStream_t s = as_stream(stream);
+    const mnpb_hmat_desc *d = (const mnpb_hmat_desc *)descs;
+    hm::HMats P;
+    for (int q = 0; q < 4; ++q) {
+        const mnpb_hmat_desc &e = d[q < nmat ? q : 0];
+        P.h[q] = hm::HMat{(const float2 *)e.D, (const float2 *)e.U, (const float2 *)e.V, e.rank,
+                          e.offD, e.offU, e.offV, e.offT, (const cd *)e.X, (cd *)e.Y, (cd *)e.T};
+    }
+    ProfScope ps(s, PC_HMATVEC, 0.0);
+    // columns in chunks of at most 8 (shared-memory bound of the row kernel);
+    // T holds sum(rank) x 8 entries and is reused by every chunk
+    for (int64_t c0 = 0; c0 < nc; c0 += 8) {
+        const int ncc = (int)(nc - c0 < 8 ? nc - c0 : 8);
+        hm::HMats Q = P;
+        for (int q = 0; q < 4; ++q) {
+            Q.h[q].X = P.h[q].X + c0 * n;
+            Q.h[q].Y = P.h[q].Y + c0 * n;
+        }
+        if (nlr > 0) {
+            dim3 g((unsigned)nlr, (unsigned)nmat);
+            if (ncc <= 4)
+                hm::hm_vtx_kernel<4><<<g, 256, 0, s>>>(Q, (int)n, ncc, (const int4 *)lowrank, c2p);
+            else
+                hm::hm_vtx_kernel<8><<<g, 256, 0, s>>>(Q, (int)n, ncc, (const int4 *)lowrank, c2p);
+            MNPB_LAUNCH_CHECK("hm_vtx_kernel");
+        }
+        dim3 g((unsigned)nleaf, (unsigned)nmat);
+        if (ncc <= 4)
+            hm::hm_rows_kernel<4><<<g, 256, 0, s>>>(Q, (int)n, ncc, (const int2 *)leaf_rows, lptr,
+                                                    lent, (const int4 *)dense,
+                                                    (const int4 *)lowrank, c2p);
+        else
+            hm::hm_rows_kernel<8><<<g, 256, 0, s>>>(Q, (int)n, ncc, (const int2 *)leaf_rows, lptr,
+                                                    lent, (const int4 *)dense,
+                                                    (const int4 *)lowrank, c2p);
+        MNPB_LAUNCH_CHECK("hm_rows_kernel");
+    }
+    return MNPB_OK;
+}
+
+extern "C" int mnpb_bem_afun(void *stream, int64_t n, int64_t nrhs, const double *P1,
+                             const double *P2, const double *Q1, const double *Q2, double *y,
+                             double e1_re, double e1_im, double e2_re, double e2_im, double k,
+                             const double *nvec) {
+    clear_error();
+    MNPB_REQUIRE(n > 0 && nrhs > 0, "bem_afun: bad sizes");
+    MNPB_REQUIRE(P1 && P2 && Q1 && Q2 && y && nvec, "bem_afun: null pointer");
+    cudaStream_t s = as_stream(stream);
+    hm::afun_kernel<<<ceil_div(n, 128), 128, 0, s>>>((int)n, (int)nrhs, (const cd *)P1,
+                                                     (const cd *)P2, (const cd *)Q1, (const cd *)Q2,
+                                                     (cd *)y, cmk(e1_re, e1_im), cmk(e2_re, e2_im),
+                                                     k, nvec);
+    MNPB_LAUNCH_CHECK("afun_kernel");
+    return MNPB_OK;
+}

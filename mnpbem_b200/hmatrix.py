@@ -1,0 +1,176 @@
+"""H-matrices on the GPU: ACA compression of dense Green-function matrices and
+H-matrix times vectors (mnpbem/greenfun/hmatrix.py, aca_compgreen_ret.py).
+
+``HTopology`` holds what depends only on the cluster tree and block partition
+(block rectangles, leaf contribution lists, scratch offsets) as device
+arrays; ``HMatrixGPU`` holds one compressed matrix: dense leaf blocks and
+low-rank factors U, V (A_block ~ U V^T) in complex64, ranks per block.
+"""
+
+import numpy as np
+import torch
+
+from . import _lib
+from ._lib import call, ptr
+from .clustertree import BlockPartition
+
+__all__ = ["HTopology", "HMatrixGPU", "hmat_matvec"]
+
+
+def _i32(a, dev):
+    return torch.from_numpy(np.ascontiguousarray(a, dtype=np.int32)).to(dev)
+
+
+def _i64(a, dev):
+    return torch.from_numpy(np.ascontiguousarray(a, dtype=np.int64)).to(dev)
+
+
+class HTopology(object):
+    """Device-side structure of one block partition of one cluster tree."""
+
+    def __init__(self, part, kmax, device):
+        if not isinstance(part, BlockPartition):
+            raise TypeError("HTopology: expected a BlockPartition")
+        tree = part.tree
+        self.part = part
+        self.n = tree.n
+        self.kmax = int(kmax)
+        self.device = device
+        dn, lr = part.dense, part.lowrank
+        self.ndense, self.nlr = dn.shape[0], lr.shape[0]
+        self.c2p = _i32(tree.ind[:, 0], device)
+        self.dense = _i32(dn.reshape(-1, 4), device)
+        self.lowrank = _i32(lr.reshape(-1, 4), device)
+        # dense storage offsets (complex entries)
+        dsz = dn[:, 1].astype(np.int64) * dn[:, 3]
+        self.offD_h = np.concatenate([[0], np.cumsum(dsz)[:-1]]).astype(np.int64) if dn.size else \
+            np.zeros(0, np.int64)
+        self.dense_entries = int(dsz.sum())
+        self.offD = _i64(self.offD_h, device)
+        # ACA scratch offsets (FP64 complex entries): U (m x cap), V (n x cap)
+        m, k = lr[:, 1].astype(np.int64), lr[:, 3].astype(np.int64)
+        cap = np.minimum(np.minimum(m, k), self.kmax)
+        sizes = np.stack([m * cap, k * cap], axis=1).reshape(-1)
+        offs = np.concatenate([[0], np.cumsum(sizes)[:-1]]).astype(np.int64) if sizes.size else \
+            np.zeros(0, np.int64)
+        self.scr_offU = _i64(offs[0::2], device)
+        self.scr_offV = _i64(offs[1::2], device)
+        self.scratch_entries = int(sizes.sum())
+        self.max_mn = int((m + k).max()) if lr.size else 0
+        # leaves (cluster rows) and their contribution lists
+        leaves = tree.leaves()
+        order = np.argsort(tree.cind[leaves, 0])
+        leaves = leaves[order]
+        lstart = tree.cind[leaves, 0]
+        lsize = tree.cind[leaves, 1] - lstart + 1
+        self.nleaf = leaves.size
+        self.leaf_rows = _i32(np.stack([lstart, lsize], axis=1), device)
+        lists = [[] for _ in range(self.nleaf)]
+        for kind, blocks in ((0, dn), (1, lr)):
+            for b, (r0, rm, _, _) in enumerate(blocks):
+                lo = np.searchsorted(lstart, r0)
+                hi = np.searchsorted(lstart, r0 + rm)
+                code = b if kind == 0 else -b - 1
+                for L in range(lo, hi):
+                    lists[L].append(code)
+        lptr = np.zeros(self.nleaf + 1, dtype=np.int64)
+        lptr[1:] = np.cumsum([len(x) for x in lists])
+        self.lptr = _i32(lptr, device)
+        ent = np.concatenate([np.asarray(x, dtype=np.int32) for x in lists]) if lptr[-1] else \
+            np.zeros(1, np.int32)
+        self.lent = _i32(ent, device)
+
+
+class HMatrixGPU(object):
+    """One ACA-compressed matrix (complex64 factors, FP64 products)."""
+
+    def __init__(self, topo, A, lda, htol, scratch=None, stream=None):
+        """Compress the dense complex128 column-major matrix at ``A`` (a
+        torch tensor whose storage holds A[i + j*lda]) with ACA tolerance
+        ``htol``.  ``scratch``: optional FP64 tensor reused between matrices."""
+        self.topo = topo
+        dev = topo.device
+        sh = _lib.stream_handle(stream)
+        self.D = torch.empty(max(1, 2 * topo.dense_entries), dtype=torch.float32, device=dev)
+        call('mnpb_hmat_gather_dense', sh, ptr(A), lda, ptr(topo.c2p), topo.ndense,
+             ptr(topo.dense), ptr(topo.offD), ptr(self.D))
+        self.rank = torch.zeros(max(1, topo.nlr), dtype=torch.int32, device=dev)
+        if topo.nlr:
+            need = 2 * topo.scratch_entries
+            if scratch is None or scratch.numel() < need:
+                scratch = torch.empty(need, dtype=torch.float64, device=dev)
+            call('mnpb_hmat_aca', sh, topo.n, ptr(A), lda, ptr(topo.c2p), topo.nlr,
+                 ptr(topo.lowrank), ptr(topo.scr_offU), ptr(topo.scr_offV), topo.max_mn,
+                 topo.kmax, float(htol), ptr(scratch), ptr(self.rank))
+            rank = self.rank.cpu().numpy()[:topo.nlr].astype(np.int64)
+            lr = topo.part.lowrank
+            su = lr[:, 1].astype(np.int64) * rank
+            sv = lr[:, 3].astype(np.int64) * rank
+            offU = np.concatenate([[0], np.cumsum(su)[:-1]]).astype(np.int64)
+            offV = np.concatenate([[0], np.cumsum(sv)[:-1]]).astype(np.int64)
+            offT = np.concatenate([[0], np.cumsum(rank)[:-1]]).astype(np.int64)
+            self.rank_h = rank
+            self.offU = _i64(offU, dev)
+            self.offV = _i64(offV, dev)
+            self.offT = _i64(offT, dev)
+            self.U = torch.empty(max(1, 2 * int(su.sum())), dtype=torch.float32, device=dev)
+            self.V = torch.empty(max(1, 2 * int(sv.sum())), dtype=torch.float32, device=dev)
+            self.sum_rank = int(rank.sum())
+            call('mnpb_hmat_compact', sh, topo.nlr, ptr(topo.lowrank), ptr(self.rank),
+                 ptr(topo.scr_offU), ptr(topo.scr_offV), ptr(scratch), ptr(self.offU),
+                 ptr(self.offV), ptr(self.U), ptr(self.V))
+        else:
+            self.rank_h = np.zeros(0, np.int64)
+            z = _i64(np.zeros(1), dev)
+            self.offU = self.offV = self.offT = z
+            self.U = self.V = torch.empty(2, dtype=torch.float32, device=dev)
+            self.sum_rank = 0
+        self.scratch = scratch
+
+    def stored_bytes(self):
+        """Bytes read by one product (complex64 dense blocks and factors)."""
+        return 4 * (self.D.numel() + self.U.numel() + self.V.numel()) if self.topo.nlr else \
+            4 * self.D.numel()
+
+    def compression(self):
+        n = self.topo.n
+        return (self.topo.dense_entries + self.U.numel() // 2 + self.V.numel() // 2) / float(n * n)
+
+    def factors(self, b):
+        """(U, V) of low-rank block b as complex128 numpy arrays (for tests)."""
+        r = int(self.rank_h[b])
+        m, k = int(self.topo.part.lowrank[b, 1]), int(self.topo.part.lowrank[b, 3])
+        ou = int(self.offU[b].item())
+        ov = int(self.offV[b].item())
+        U = self.U[2 * ou:2 * (ou + m * r)].double().cpu().numpy().view(complex)
+        V = self.V[2 * ov:2 * (ov + k * r)].double().cpu().numpy().view(complex)
+        return U.reshape(r, m).T, V.reshape(r, k).T
+
+
+def hmat_matvec(hms, xs, ys, nc, stream=None):
+    """ys[i] = hms[i] @ xs[i] for up to 4 H-matrices of one topology; x, y are
+    complex128 (nc, n) tensors (column c contiguous) in face order."""
+    if not 1 <= len(hms) <= 4:
+        raise ValueError("hmat_matvec: 1 to 4 matrices per call")
+    topo = hms[0].topo
+    dev = topo.device
+    n = topo.n
+    # one V^T x scratch per matrix (the matrices run in the same launch)
+    per = 2 * max(1, max(h.sum_rank for h in hms)) * min(nc, 8)
+    T = torch.empty(per * len(hms), dtype=torch.float64, device=dev)
+    desc = np.zeros((len(hms), 11), dtype=np.uint64)
+    keep = []
+    for i, (h, x, y) in enumerate(zip(hms, xs, ys)):
+        if h.topo is not topo:
+            raise ValueError("hmat_matvec: all matrices must share one topology")
+        if x.dtype != torch.complex128 or y.dtype != torch.complex128 or not x.is_contiguous() \
+                or not y.is_contiguous() or x.numel() < n * nc or y.numel() < n * nc:
+            raise ValueError("hmat_matvec: x, y must be contiguous complex128 (nc, n)")
+        desc[i] = [h.D.data_ptr(), h.U.data_ptr(), h.V.data_ptr(), h.rank.data_ptr(),
+                   topo.offD.data_ptr(), h.offU.data_ptr(), h.offV.data_ptr(),
+                   h.offT.data_ptr(), x.data_ptr(), y.data_ptr(), T[i * per:].data_ptr()]
+        keep.append((x, y))
+    call('mnpb_hmat_matvec', _lib.stream_handle(stream), n, nc, len(hms), ptr(desc),
+         ptr(topo.c2p), topo.ndense, ptr(topo.dense), topo.nlr, ptr(topo.lowrank), topo.nleaf,
+         ptr(topo.leaf_rows), ptr(topo.lptr), ptr(topo.lent))
+    return ys
