@@ -413,6 +413,36 @@ int mnpb_gmres_update(void *stream, int64_t L, int64_t m, const double *H, int64
 int mnpb_vec_norms(void *stream, int64_t L, int64_t nvec, const double *x, int64_t ldx,
                    double *partial, double *out);
 
+/* ---------------------------------------------------------------------------
+ * Warm-start network (per-face MLP predicting the next wavelength's
+ * solution; no counterpart in the reference, which has no learned part).
+ * Activations row-major FP32, weights [out][in] bf16 + FP32 master copy.
+ * ------------------------------------------------------------------------- */
+
+/* C (M x N) = A B with element strides (A(m,k) = A[m*sam + k*sak], B(k,n) =
+ * B[k*sbk + n*sbn], C(m,n) = C[m*scm + n*scn]); b_bf16 != 0: B holds bf16.
+ * mode 0: plain product (nsplit > 1 splits K; work holds nsplit*M*N floats
+ * and C must be row-major dense); mode 1: C = SiLU(AB + bias), Z = AB +
+ * bias; mode 2: C = Z = AB + bias (Z may be NULL). */
+int mnpb_mlp_gemm(void *stream, int64_t M, int64_t N, int64_t K, const float *A, int64_t sam,
+                  int64_t sak, const void *B, int64_t sbk, int64_t sbn, int32_t b_bf16, float *C,
+                  int64_t scm, int64_t scn, const float *bias, int32_t mode, float *Z,
+                  int64_t nsplit, float *work);
+/* dZ = dY * SiLU'(Z) element-wise. */
+int mnpb_mlp_silu_back(void *stream, int64_t len, const float *dY, const float *Z, float *dZ);
+/* out[c] = sum over rows of X[r*ld + c]. */
+int mnpb_mlp_colsum(void *stream, int64_t rows, int64_t cols, const float *X, int64_t ld,
+                    float *out);
+/* dY = 2 (Y - T) / len; part[ceil(len/256)] partial sums of (Y - T)^2. */
+int mnpb_mlp_mse(void *stream, int64_t len, const float *Y, const float *T, float *dY,
+                 float *part);
+/* Adam step (bias correction in the step size) on FP32 w with gradient g,
+ * moments m, v; wb (bf16, may be NULL) receives the rounded weights. */
+int mnpb_mlp_adam(void *stream, int64_t len, float *w, void *wb, const float *g, float *m,
+                  float *v, double lr, double b1, double b2, double eps, int64_t step);
+/* wb = bf16(w), round to nearest even. */
+int mnpb_mlp_to_bf16(void *stream, int64_t len, const float *w, void *wb);
+
 #ifdef __cplusplus
 }
 #endif

@@ -70,6 +70,13 @@ SIGNATURES = {
     'mnpb_gmres_givens': [_P, _I64, _P, _I64, _P, _P, _P, _P],
     'mnpb_gmres_update': [_P, _I64, _I64, _P, _I64, _P, _P, _I64, _P, _P],
     'mnpb_vec_norms': [_P, _I64, _I64, _P, _I64, _P, _P],
+    'mnpb_mlp_gemm': [_P, _I64, _I64, _I64, _P, _I64, _I64, _P, _I64, _I64, C.c_int32, _P, _I64,
+                      _I64, _P, C.c_int32, _P, _I64, _P],
+    'mnpb_mlp_silu_back': [_P, _I64, _P, _P, _P],
+    'mnpb_mlp_colsum': [_P, _I64, _I64, _P, _I64, _P],
+    'mnpb_mlp_mse': [_P, _I64, _P, _P, _P, _P],
+    'mnpb_mlp_adam': [_P, _I64, _P, _P, _P, _P, _P, _D, _D, _D, _D, _I64],
+    'mnpb_mlp_to_bf16': [_P, _I64, _P, _P],
     'mnpb_stat_matrix': [_P, _I64, _I64, _P, _I64, _P, _P, _I64, _I64],
     'mnpb_planewave_potential': [_P, _I64, _I64, _I64, _P, _P, _P, _P, _P, _P, _P, _P, _P],
     'mnpb_farfield': [_P, _I64, _I64, _I64, _I64, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P],

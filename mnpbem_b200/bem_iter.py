@@ -53,13 +53,14 @@ def _norm(v, stream=None):
 
 
 def gmres(apply_A, b, tol=1e-6, maxit=200, restart=None, x0=None, apply_M=None,
-          stream=None, counter=None):
+          stream=None, counter=None, r0=None):
     """Restarted, right-preconditioned GMRES on complex128 device vectors.
 
     ``apply_A(v) -> A v`` and ``apply_M(v) -> M v`` take and return flat
     complex128 device tensors.  Stops when |b - A x| <= tol |b| (scipy
     semantics, bem_iter.py:79-89: restart = min(n, maxit), at most ``maxit``
-    restart cycles).  Returns (x, flag, relres, [cycles, iterations]).
+    restart cycles).  ``r0``: b - A x0 when the caller already has it.
+    Returns (x, flag, relres, [cycles, iterations]).
     """
     dev = b.device
     L = b.numel()
@@ -77,7 +78,10 @@ def gmres(apply_A, b, tol=1e-6, maxit=200, restart=None, x0=None, apply_M=None,
     if bnorm == 0.0:
         return torch.zeros_like(b), 0, 0.0, [0, 0]
     x = torch.zeros_like(b) if x0 is None else x0.reshape(-1).clone()
-    r = b.clone() if x0 is None else b - A(x)
+    if x0 is None:
+        r = b.clone()
+    else:
+        r = r0.clone() if r0 is not None else b - A(x)
     V = torch.empty((restart + 1, L), dtype=torch.complex128, device=dev)
     H = torch.zeros((restart, restart + 1), dtype=torch.complex128, device=dev)
     cs = torch.zeros(restart, dtype=torch.float64, device=dev)
@@ -318,6 +322,60 @@ class BEMRetIter(object):
             print('gmres: flag {}, relres {:.3e}, {} iterations, {} operator applications'.format(
                 flag, relres, it[1], cnt.matvecs))
         return x, flag, relres, it
+
+    def solve_spectrum(self, exc, eneis, warm=None, deflate=False):
+        """Solve a wavelength sweep with GMRES warm starts.
+
+        ``warm``: None (zero start, the reference's behaviour), 'previous'
+        (x_{i-1}), 'extrapolate' (quadratic: 3 x_{i-1} - 3 x_{i-2} + x_{i-3})
+        or a trained ``mnpbem_b200.learned.LearnedWarmStart`` (which corrects
+        the quadratic extrapolation).  The first wavelengths fall back to the
+        previous solution / linear extrapolation until the history is long
+        enough.  ``deflate``: start from
+        the minimal-residual point of span{start, x_{i-1}, x_{i-2}}.
+        Returns (list of CompStruct, list of per-wavelength statistics dicts,
+        list of packed device solutions).
+        """
+        from .learned import LearnedWarmStart, face_geometry, minres_start
+        n = self.tables.n
+        learned = isinstance(warm, LearnedWarmStart)
+        geo = face_geometry(self.p, self.device) if learned else None
+        xs, sols, stats = [], [], []
+        for i, enei in enumerate(eneis):
+            self._init_matrices(enei)
+            b, K = self._excitation(exc.potential(self.p, enei))
+            cnt = _Counter()
+            A = lambda v: self._afun(v, K)
+            x0 = r0 = None
+            if warm is not None and i >= 1:
+                if warm == 'previous' or i < 2:
+                    x0 = xs[i - 1]
+                elif i < 3:
+                    x0 = 2.0 * xs[i - 1] - xs[i - 2]
+                elif warm == 'extrapolate':
+                    x0 = 3.0 * xs[i - 1] - 3.0 * xs[i - 2] + xs[i - 3]
+                elif learned:
+                    x0 = warm.predict(self.p, [eneis[i - j] for j in range(4)],
+                                      [xs[i - 1], xs[i - 2], xs[i - 3]], K, geo)
+                else:
+                    raise ValueError("solve_spectrum: unknown warm start {!r}".format(warm))
+                if deflate and i >= 2:
+                    basis = [x0, xs[i - 1], xs[i - 2]] if warm != 'previous' else \
+                        [xs[i - 1], xs[i - 2]]
+                    x0, r0 = minres_start(A, b, basis, counter=cnt)
+            M = (lambda v: self._apply_precond(v, K)) if self._pre is not None else None
+            x, flag, relres, it = gmres(A, b, tol=self.tol, maxit=self.maxit,
+                                        restart=self.restart, x0=x0, apply_M=M, counter=cnt,
+                                        r0=r0)
+            self._flag.append(flag)
+            self._relres.append(relres)
+            self._iter.append(np.array(it))
+            self._matvecs.append(cnt.matvecs)
+            stats.append(dict(enei=enei, flag=flag, relres=relres, iters=it[1],
+                              matvecs=cnt.matvecs))
+            xs.append(x)
+            sols.append(self._to_compstruct(x.reshape(8, K, n).cpu().numpy(), K, enei))
+        return sols, stats, xs
 
     def _pack_solution(self, sig, K):
         n = self.tables.n
