@@ -365,23 +365,39 @@ int mnpb_hmat_aca(void *stream, int64_t n, const double *A, int64_t lda, const i
 int mnpb_hmat_gather_dense(void *stream, const double *A, int64_t lda, const int32_t *c2p,
                            int64_t nblk, const int32_t *blocks, const int64_t *offD, float *out);
 
-/* ACA factors from the FP64 scratch of mnpb_hmat_aca to complex64 storage
- * with rank columns each: U of block b at U + 2*outU[b], V at V + 2*outV[b]. */
+/* ACA factors from the FP64 scratch of mnpb_hmat_aca to complex64 storage:
+ * U of block b (rows x rank, column-major) at U + 2*outU[b]; V stored
+ * transposed (element (j, q) at q + j*rank) at V + 2*outV[b]. */
 int mnpb_hmat_compact(void *stream, int64_t nblk, const int32_t *blocks, const int32_t *rank,
                       const int64_t *offU, const int64_t *offV, const double *UV,
                       const int64_t *outU, const int64_t *outV, float *U, float *V);
 
 /* Y_i = H_i X_i for nmat (<= 4) H-matrices of one block partition; descs
- * points to nmat host records of 11 pointers each: D, U, V, rank, offD,
- * offU, offV, offT, X, Y, T (X, Y: complex128 n x nc, column stride n, face
- * order; T: FP64 scratch of 2 * min(nc, 8) * sum(rank) doubles).  leaf_rows:
+ * points to nmat host records of 14 pointers each: D, U, V, rank, offD,
+ * offU, offV, offT, X, Y, T, Xc, offTP, TP (X, Y: complex128 n x nc, column
+ * stride n, face order; T: FP64 scratch of 2 * min(nc, 4) * sum(rank)
+ * doubles; Xc: FP64 scratch of 2 * n * min(nc, 4) doubles for X in cluster
+ * order; offTP (int64 per low-rank block) and TP (FP64 scratch, 8 doubles
+ * per entry) hold the per-segment partials of V^T x: block b's segments
+ * start at TP + 8 * offTP[b], rank entries per segment).  vitems: nvitem
+ * int32 quadruples (block, first column, end column, segment) covering
+ * every low-rank block's columns; vptr (nlr + 1) the items of each block.
+ * leaf_rows:
  * int32 (start, rows) per leaf cluster; lptr/lent: CSR list per leaf of
- * contributing blocks (e >= 0 dense block e, e < 0 low-rank block -e-1).
+ * contributing blocks (e >= 0 dense block e, e < 0 low-rank block -e-1);
+ * chunks: nchunk int32 pairs (leaf, first row) covering every leaf in
+ * 32-row pieces; items: nitem int32 quadruples (chunk, first entry, end
+ * entry, 0) splitting each chunk's list into short segments, cptr (nchunk +
+ * 1) the items of each chunk; partial: FP64 scratch of nmat * nitem * 256
+ * doubles.
  * Replaces HMatrix.mtimes_vec (mnpbem/greenfun/hmatrix.py:450-541). */
 int mnpb_hmat_matvec(void *stream, int64_t n, int64_t nc, int64_t nmat, const void *descs,
                      const int32_t *c2p, int64_t ndense, const int32_t *dense, int64_t nlr,
                      const int32_t *lowrank, int64_t nleaf, const int32_t *leaf_rows,
-                     const int32_t *lptr, const int32_t *lent);
+                     const int32_t *lptr, const int32_t *lent, int64_t nchunk,
+                     const int32_t *chunks, int64_t nitem, const int32_t *items,
+                     const int32_t *cptr, double *partial, int64_t nvitem,
+                     const int32_t *vitems, const int32_t *vptr);
 
 /* y = A x of the packed retarded operator from the four products P1 = G1 v1,
  * P2 = G2 v2, Q1 = H1 v1, Q2 = H2 v2 (n x 4*nrhs each, columns sig then h

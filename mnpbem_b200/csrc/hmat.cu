@@ -216,9 +216,11 @@ __global__ void compact_kernel(const int4 *__restrict__ blk, const int *__restri
         const cd v = UV[offU[b] + e];
         fU[outU[b] + e] = make_float2((float)v.x, (float)v.y);
     }
+    // V transposed: (j, q) -> q + j * r
     for (int64_t e = threadIdx.x; e < nv; e += blockDim.x) {
+        const int64_t j = e % bk.w, q = e / bk.w;
         const cd v = UV[offV[b] + e];
-        fV[outV[b] + e] = make_float2((float)v.x, (float)v.y);
+        fV[outV[b] + q + j * r] = make_float2((float)v.x, (float)v.y);
     }
 }
 
@@ -234,115 +236,201 @@ struct HMat {
     const cd *X;          // n x nc input (face order), column stride n
     cd *Y;                // n x nc output (face order)
     cd *T;                // scratch V^T x
+    cd *Xc;               // scratch: X in cluster order (n x nc)
+    const int64_t *offTP; // per low-rank block: start of its segment partials (entries / NC)
+    cd *TP;               // scratch: segment partials of V^T x
 };
 struct HMats {
     HMat h[4];
 };
 
-// t_b = V_b^T x[cols]: one CTA per low-rank block, one warp per factor column.
+// t_b = V_b^T x[cols] in two steps.  Work items vitems[i] = (block, first
+// column, end column, segment index within the block) cover every low-rank
+// block in segments of at most a few hundred columns; one warp per item,
+// lane = factor column q (V is stored transposed: element (j, q) at
+// V[q + j * rank], so the lanes of one j read consecutive words), x in
+// cluster order read as a broadcast.  The item's partial t goes to
+// TP + (offTP[block] + segment * rank) * NC; hm_vtx_reduce_kernel adds a
+// block's segments in order (deterministic).
 template <int NC>
-__global__ void __launch_bounds__(256) hm_vtx_kernel(HMats P, int n, int nc,
-                                                     const int4 *__restrict__ lr,
-                                                     const int *__restrict__ c2p) {
+__global__ void __launch_bounds__(256, 3) hm_vtx_kernel(HMats P, int n, int nc, int nvitem,
+                                                     const int4 *__restrict__ vitems,
+                                                     const int4 *__restrict__ lr) {
+    const int it = blockIdx.x * 8 + (threadIdx.x >> 5);
+    if (it >= nvitem) return;
     const HMat &H = P.h[blockIdx.y];
-    const int b = blockIdx.x;
+    const int l = threadIdx.x & 31;
+    const int4 vi = vitems[it];
+    const int b = vi.x;
     const int4 bk = lr[b];
     const int r = H.rank[b];
     const float2 *V = H.V + H.offV[b];
-    cd *T = H.T + H.offT[b] * nc;
-    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
-    for (int q = w; q < r; q += 8) {
+    cd *out = H.TP + (H.offTP[b] + (int64_t)vi.w * r) * NC;
+    const cd *xc = H.Xc + bk.z;
+    constexpr int UN = 8;
+    for (int q0 = 0; q0 < r; q0 += 32) {
+        const int q = q0 + l;
+        const bool live = q < r;
         cd acc[NC];
 #pragma unroll
         for (int c = 0; c < NC; ++c) acc[c] = cmk(0, 0);
-        const float2 *vq = V + (int64_t)q * bk.w;
-        for (int j = l; j < bk.w; j += 32) {
-            const float2 v = vq[j];
-            const cd vv = cmk(v.x, v.y);
-            const int64_t row = c2p[bk.z + j];
+        int j = vi.y;
+        for (; j + UN <= vi.z; j += UN) {
+            float2 v[UN];
+#pragma unroll
+            for (int u = 0; u < UN; ++u)
+                v[u] = live ? V[(int64_t)(j + u) * r + q] : make_float2(0.f, 0.f);
+#pragma unroll
+            for (int u = 0; u < UN; ++u)
+#pragma unroll
+                for (int c = 0; c < NC; ++c)
+                    if (c < nc) acc[c] = cfma(cmk(v[u].x, v[u].y), xc[(int64_t)c * n + j + u], acc[c]);
+        }
+        for (; j < vi.z; ++j) {
+            const float2 v = live ? V[(int64_t)j * r + q] : make_float2(0.f, 0.f);
 #pragma unroll
             for (int c = 0; c < NC; ++c)
-                if (c < nc) acc[c] = cfma(vv, H.X[row + (int64_t)c * n], acc[c]);
+                if (c < nc) acc[c] = cfma(cmk(v.x, v.y), xc[(int64_t)c * n + j], acc[c]);
         }
+        if (live)
 #pragma unroll
-        for (int c = 0; c < NC; ++c) {
-            for (int o = 16; o > 0; o >>= 1) {
-                acc[c].x += __shfl_xor_sync(0xffffffffu, acc[c].x, o);
-                acc[c].y += __shfl_xor_sync(0xffffffffu, acc[c].y, o);
-            }
-        }
-        if (l == 0)
-            for (int c = 0; c < nc; ++c) T[(int64_t)q * nc + c] = acc[c];
+            for (int c = 0; c < NC; ++c) out[(int64_t)q * NC + c] = acc[c];
     }
 }
 
-// One CTA per leaf cluster (rows leaf_rows[L].x .. +leaf_rows[L].y): 64 rows
-// x 4 lanes over the columns of each contributing block.  Contribution list
-// (CSR over leaves): entry e >= 0 is dense block e, entry e < 0 low-rank block
-// -e-1.
-constexpr int HM_ROWS = 64, HM_KL = 4;
+// T[offT[b] * nc + q * nc + c] = sum over the block's segments (in order);
+// one warp per low-rank block, lane = q; vptr: items of block b are
+// vptr[b] .. vptr[b+1]-1 (segments 0, 1, ...).
 template <int NC>
-__global__ void __launch_bounds__(256) hm_rows_kernel(HMats P, int n, int nc,
-                                                      const int2 *__restrict__ leaf_rows,
-                                                      const int *__restrict__ lptr,
-                                                      const int *__restrict__ lent,
-                                                      const int4 *__restrict__ dn,
-                                                      const int4 *__restrict__ lr,
-                                                      const int *__restrict__ c2p) {
-    __shared__ cd part[HM_KL][HM_ROWS][NC];
+__global__ void __launch_bounds__(256) hm_vtx_reduce_kernel(HMats P, int nc, int nblk,
+                                                            const int *__restrict__ vptr) {
+    const int b = blockIdx.x * 8 + (threadIdx.x >> 5);
+    if (b >= nblk) return;
     const HMat &H = P.h[blockIdx.y];
-    const int2 lf = leaf_rows[blockIdx.x];
-    const int rl = threadIdx.x % HM_ROWS, kl = threadIdx.x / HM_ROWS;
-    for (int rbase = 0; rbase < lf.y; rbase += HM_ROWS) {
-        const int row = lf.x + rbase + rl;     // cluster position
-        const bool live = rbase + rl < lf.y;
+    const int l = threadIdx.x & 31;
+    const int r = H.rank[b];
+    const int nseg = vptr[b + 1] - vptr[b];
+    const cd *in = H.TP + H.offTP[b] * NC;
+    cd *T = H.T + H.offT[b] * nc;
+    for (int q = l; q < r; q += 32) {
         cd acc[NC];
 #pragma unroll
         for (int c = 0; c < NC; ++c) acc[c] = cmk(0, 0);
-        for (int e = lptr[blockIdx.x]; e < lptr[blockIdx.x + 1]; ++e) {
-            const int id = lent[e];
-            if (id >= 0) {
-                const int4 bk = dn[id];
-                const float2 *D = H.D + H.offD[id] + (row - bk.x);
-                if (live)
-                    for (int j = kl; j < bk.w; j += HM_KL) {
-                        const float2 a = D[(int64_t)j * bk.y];
-                        const cd aa = cmk(a.x, a.y);
-                        const int64_t xr = c2p[bk.z + j];
+        for (int sg = 0; sg < nseg; ++sg)
 #pragma unroll
-                        for (int c = 0; c < NC; ++c)
-                            if (c < nc) acc[c] = cfma(aa, H.X[xr + (int64_t)c * n], acc[c]);
-                    }
-            } else {
-                const int b = -id - 1;
-                const int4 bk = lr[b];
-                const int r = H.rank[b];
-                const float2 *U = H.U + H.offU[b] + (row - bk.x);
-                const cd *T = H.T + H.offT[b] * nc;
-                if (live)
-                    for (int q = kl; q < r; q += HM_KL) {
-                        const float2 a = U[(int64_t)q * bk.y];
-                        const cd aa = cmk(a.x, a.y);
+            for (int c = 0; c < NC; ++c) acc[c] = cadd(acc[c], in[((int64_t)sg * r + q) * NC + c]);
 #pragma unroll
-                        for (int c = 0; c < NC; ++c)
-                            if (c < nc) acc[c] = cfma(aa, T[(int64_t)q * nc + c], acc[c]);
-                    }
-            }
-        }
-#pragma unroll
-        for (int c = 0; c < NC; ++c) part[kl][rl][c] = acc[c];
-        __syncthreads();
-        for (int e = threadIdx.x; e < HM_ROWS * nc; e += blockDim.x) {
-            const int r = e % HM_ROWS, c = e / HM_ROWS;
-            if (rbase + r < lf.y) {
-                cd v = part[0][r][c];
-#pragma unroll
-                for (int q = 1; q < HM_KL; ++q) v = cadd(v, part[q][r][c]);
-                H.Y[c2p[lf.x + rbase + r] + (int64_t)c * n] = v;
-            }
-        }
-        __syncthreads();
+        for (int c = 0; c < NC; ++c)
+            if (c < nc) T[(int64_t)q * nc + c] = acc[c];
     }
+}
+
+// Row sums in two steps.  Work items: (32-row chunk of a leaf, segment of at
+// most a few entries of the leaf's contribution list); items[i] = (chunk,
+// first entry, end entry), chunks[k] = (leaf, first row offset).  One warp
+// per item, lane = row: the warp sums its entries (entry e >= 0 dense block
+// e, e < 0 low-rank block -e-1) in registers and writes a 32 x NC partial;
+// hm_reduce_kernel adds the partials of each chunk in item order (so the
+// result is deterministic) and scatters the rows to face order.
+template <int NC, int UN>
+__device__ __forceinline__ void rows_accumulate(const float2 *__restrict__ A, int64_t lda, int cnt,
+                                                const cd *__restrict__ B, int64_t bj, int64_t bc,
+                                                bool live, cd (&acc)[NC]) {
+    // acc += sum_j A[j * lda] * B[j * bj + c * bc]   (A per lane, B broadcast)
+    int j = 0;
+    for (; j + UN <= cnt; j += UN) {
+        float2 a[UN];
+#pragma unroll
+        for (int u = 0; u < UN; ++u) a[u] = live ? A[(int64_t)(j + u) * lda] : make_float2(0.f, 0.f);
+#pragma unroll
+        for (int u = 0; u < UN; ++u) {
+            const cd av = cmk(a[u].x, a[u].y);
+#pragma unroll
+            for (int c = 0; c < NC; ++c) acc[c] = cfma(av, B[(int64_t)(j + u) * bj + c * bc], acc[c]);
+        }
+    }
+    for (; j < cnt; ++j) {
+        const float2 a = live ? A[(int64_t)j * lda] : make_float2(0.f, 0.f);
+        const cd av = cmk(a.x, a.y);
+#pragma unroll
+        for (int c = 0; c < NC; ++c) acc[c] = cfma(av, B[(int64_t)j * bj + c * bc], acc[c]);
+    }
+}
+
+template <int NC>
+__global__ void __launch_bounds__(256, 3) hm_rows_kernel(HMats P, int n, int nitem,
+                                                         const int4 *__restrict__ items,
+                                                         const int2 *__restrict__ chunks,
+                                                         const int2 *__restrict__ leaf_rows,
+                                                         const int *__restrict__ lent,
+                                                         const int4 *__restrict__ dn,
+                                                         const int4 *__restrict__ lr,
+                                                         cd *__restrict__ partial) {
+    const int it = blockIdx.x * 8 + (threadIdx.x >> 5);
+    if (it >= nitem) return;
+    const HMat &H = P.h[blockIdx.y];
+    const int l = threadIdx.x & 31;
+    const int4 item = items[it];
+    const int2 ch = chunks[item.x];
+    const int2 lf = leaf_rows[ch.x];
+    const bool live = ch.y + l < lf.y;
+    const int row = lf.x + ch.y + l;          // cluster position
+    cd acc[NC];
+#pragma unroll
+    for (int c = 0; c < NC; ++c) acc[c] = cmk(0, 0);
+    for (int e = item.y; e < item.z; ++e) {
+        const int id = lent[e];
+        if (id >= 0) {
+            const int4 bk = dn[id];
+            rows_accumulate<NC, 8>(H.D + H.offD[id] + (row - bk.x), bk.y, bk.w, H.Xc + bk.z, 1, n,
+                                   live, acc);
+        } else {
+            const int b = -id - 1;
+            const int4 bk = lr[b];
+            rows_accumulate<NC, 8>(H.U + H.offU[b] + (row - bk.x), bk.y, H.rank[b],
+                                   H.T + H.offT[b] * NC, NC, 1, live, acc);
+        }
+    }
+    cd *out = partial + ((int64_t)blockIdx.y * nitem + it) * 32 * 4;
+#pragma unroll
+    for (int c = 0; c < NC; ++c) out[c * 32 + l] = acc[c];
+}
+
+// y rows of chunk k = sum of the partials of items cptr[k] .. cptr[k+1]-1
+template <int NC>
+__global__ void __launch_bounds__(256) hm_reduce_kernel(HMats P, int n, int nc, int nchunk,
+                                                        int nitem, const int *__restrict__ cptr,
+                                                        const int2 *__restrict__ chunks,
+                                                        const int2 *__restrict__ leaf_rows,
+                                                        const int *__restrict__ c2p,
+                                                        const cd *__restrict__ partial) {
+    const int k = blockIdx.x * 8 + (threadIdx.x >> 5);
+    if (k >= nchunk) return;
+    const HMat &H = P.h[blockIdx.y];
+    const int l = threadIdx.x & 31;
+    const int2 ch = chunks[k];
+    const int2 lf = leaf_rows[ch.x];
+    if (ch.y + l >= lf.y) return;
+    cd acc[NC];
+#pragma unroll
+    for (int c = 0; c < NC; ++c) acc[c] = cmk(0, 0);
+    const cd *base = partial + (int64_t)blockIdx.y * nitem * 32 * 4;
+    for (int i = cptr[k]; i < cptr[k + 1]; ++i)
+#pragma unroll
+        for (int c = 0; c < NC; ++c) acc[c] = cadd(acc[c], base[((int64_t)i * 4 + c) * 32 + l]);
+    const int64_t yr = c2p[lf.x + ch.y + l];
+#pragma unroll
+    for (int c = 0; c < NC; ++c)
+        if (c < nc) H.Y[yr + (int64_t)c * n] = acc[c];
+}
+
+// Xc[c + col*n] = X[c2p[c] + col*n] for every matrix of the launch (blockIdx.y)
+__global__ void permute_kernel(HMats P, int n, int nc, const int *__restrict__ c2p) {
+    const HMat &H = P.h[blockIdx.y];
+    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= (int64_t)n * nc) return;
+    const int c = (int)(e % n), col = (int)(e / n);
+    H.Xc[e] = H.X[c2p[c] + (int64_t)col * n];
 }
 
 // y = A x for the packed operator.  P1 = G1 [sig1|h1], P2 = G2 [sig2|h2],
@@ -441,53 +529,73 @@ struct mnpb_hmat_desc {
     const int32_t *rank;
     const int64_t *offD, *offU, *offV, *offT;
     const double *X;
-    double *Y, *T;
+    double *Y, *T, *Xc;
+    const int64_t *offTP;
+    double *TP;
 };
 
 extern "C" int mnpb_hmat_matvec(void *stream, int64_t n, int64_t nc, int64_t nmat,
                                 const void *descs, const int32_t *c2p, int64_t ndense,
                                 const int32_t *dense, int64_t nlr, const int32_t *lowrank,
                                 int64_t nleaf, const int32_t *leaf_rows, const int32_t *lptr,
-                                const int32_t *lent) {
+                                const int32_t *lent, int64_t nchunk, const int32_t *chunks,
+                                int64_t nitem, const int32_t *items, const int32_t *cptr,
+                                double *partial, int64_t nvitem, const int32_t *vitems,
+                                const int32_t *vptr) {
     clear_error();
     MNPB_REQUIRE(n > 0 && nc > 0 && nc <= 64 && nmat >= 1 && nmat <= 4 && nleaf > 0,
                  "hmat_matvec: bad sizes (nc <= 64, nmat <= 4)");
-    MNPB_REQUIRE(descs && c2p && leaf_rows && lptr && lent, "hmat_matvec: null pointer");
+    MNPB_REQUIRE(descs && c2p && leaf_rows && lptr && lent && chunks && nchunk > 0 && items &&
+                     nitem > 0 && cptr && partial && (nlr == 0 || (vitems && vptr && nvitem > 0)),
+                 "hmat_matvec: null pointer");
     cudaStream_t s = as_stream(stream);
     const mnpb_hmat_desc *d = (const mnpb_hmat_desc *)descs;
     hm::HMats P;
     for (int q = 0; q < 4; ++q) {
         const mnpb_hmat_desc &e = d[q < nmat ? q : 0];
         P.h[q] = hm::HMat{(const float2 *)e.D, (const float2 *)e.U, (const float2 *)e.V, e.rank,
-                          e.offD, e.offU, e.offV, e.offT, (const cd *)e.X, (cd *)e.Y, (cd *)e.T};
+                          e.offD, e.offU, e.offV, e.offT, (const cd *)e.X, (cd *)e.Y, (cd *)e.T,
+                          (cd *)e.Xc, e.offTP, (cd *)e.TP};
     }
     ProfScope ps(s, PC_HMATVEC, 0.0);
-    // columns in chunks of at most 8 (shared-memory bound of the row kernel);
-    // T holds sum(rank) x 8 entries and is reused by every chunk
-    for (int64_t c0 = 0; c0 < nc; c0 += 8) {
-        const int ncc = (int)(nc - c0 < 8 ? nc - c0 : 8);
+    // columns in chunks of at most 4 (register bound of the kernels); T
+    // holds sum(rank) x 4 entries and is reused by every chunk
+    for (int64_t c0 = 0; c0 < nc; c0 += 4) {
+        const int ncc = (int)(nc - c0 < 4 ? nc - c0 : 4);
         hm::HMats Q = P;
         for (int q = 0; q < 4; ++q) {
             Q.h[q].X = P.h[q].X + c0 * n;
             Q.h[q].Y = P.h[q].Y + c0 * n;
         }
+        hm::permute_kernel<<<dim3((unsigned)ceil_div(n * ncc, 256), (unsigned)nmat), 256, 0, s>>>(
+            Q, (int)n, ncc, c2p);
+        MNPB_LAUNCH_CHECK("hm permute_kernel");
         if (nlr > 0) {
-            dim3 g((unsigned)nlr, (unsigned)nmat);
-            if (ncc <= 4)
-                hm::hm_vtx_kernel<4><<<g, 256, 0, s>>>(Q, (int)n, ncc, (const int4 *)lowrank, c2p);
-            else
-                hm::hm_vtx_kernel<8><<<g, 256, 0, s>>>(Q, (int)n, ncc, (const int4 *)lowrank, c2p);
+            dim3 g((unsigned)ceil_div(nvitem, 8), (unsigned)nmat);
+            hm::hm_vtx_kernel<4><<<g, 256, 0, s>>>(Q, (int)n, ncc, (int)nvitem,
+                                                   (const int4 *)vitems, (const int4 *)lowrank);
             MNPB_LAUNCH_CHECK("hm_vtx_kernel");
+            dim3 gr((unsigned)ceil_div(nlr, 8), (unsigned)nmat);
+            hm::hm_vtx_reduce_kernel<4><<<gr, 256, 0, s>>>(Q, ncc, (int)nlr, vptr);
+            MNPB_LAUNCH_CHECK("hm_vtx_reduce_kernel");
         }
-        dim3 g((unsigned)nleaf, (unsigned)nmat);
-        if (ncc <= 4)
-            hm::hm_rows_kernel<4><<<g, 256, 0, s>>>(Q, (int)n, ncc, (const int2 *)leaf_rows, lptr,
-                                                    lent, (const int4 *)dense,
-                                                    (const int4 *)lowrank, c2p);
-        else
-            hm::hm_rows_kernel<8><<<g, 256, 0, s>>>(Q, (int)n, ncc, (const int2 *)leaf_rows, lptr,
-                                                    lent, (const int4 *)dense,
-                                                    (const int4 *)lowrank, c2p);
+        dim3 g((unsigned)ceil_div(nitem, 8), (unsigned)nmat);
+        dim3 gr((unsigned)ceil_div(nchunk, 8), (unsigned)nmat);
+#define MNPB_HM_ROWS(NCV)                                                                       \
+    hm::hm_rows_kernel<NCV><<<g, 256, 0, s>>>(Q, (int)n, (int)nitem, (const int4 *)items,       \
+                                              (const int2 *)chunks, (const int2 *)leaf_rows,    \
+                                              lent, (const int4 *)dense, (const int4 *)lowrank, \
+                                              (cd *)partial);                                   \
+    hm::hm_reduce_kernel<NCV><<<gr, 256, 0, s>>>(Q, (int)n, NCV, (int)nchunk, (int)nitem, cptr,  \
+                                                 (const int2 *)chunks, (const int2 *)leaf_rows,  \
+                                                 c2p, (const cd *)partial)
+        switch (ncc) {
+        case 1: MNPB_HM_ROWS(1); break;
+        case 2: MNPB_HM_ROWS(2); break;
+        case 3: MNPB_HM_ROWS(3); break;
+        default: MNPB_HM_ROWS(4); break;
+        }
+#undef MNPB_HM_ROWS
         MNPB_LAUNCH_CHECK("hm_rows_kernel");
     }
     return MNPB_OK;

@@ -79,6 +79,37 @@ class HTopology(object):
         ent = np.concatenate([np.asarray(x, dtype=np.int32) for x in lists]) if lptr[-1] else \
             np.zeros(1, np.int32)
         self.lent = _i32(ent, device)
+        # 32-row chunks of the leaves, and work items (chunk, segment of at
+        # most SEG entries of the leaf's list): one warp per item
+        SEG = 6
+        ch, items, cptr = [], [], [0]
+        for L in range(self.nleaf):
+            for r0 in range(0, int(lsize[L]), 32):
+                k = len(ch)
+                ch.append((L, r0))
+                for e in range(int(lptr[L]), int(lptr[L + 1]), SEG):
+                    items.append((k, e, min(e + SEG, int(lptr[L + 1])), 0))
+                if lptr[L + 1] == lptr[L]:
+                    items.append((k, 0, 0, 0))
+                cptr.append(len(items))
+        self.nchunk = len(ch)
+        self.chunks = _i32(np.asarray(ch, dtype=np.int64).reshape(-1, 2), device)
+        # V^T x work items: (block, first column, end column, segment)
+        VSEG = 128
+        vit, vptr = [], [0]
+        for b in range(self.nlr):
+            ncol = int(lr[b, 3])
+            for sg, j0 in enumerate(range(0, ncol, VSEG)):
+                vit.append((b, j0, min(j0 + VSEG, ncol), sg))
+            vptr.append(len(vit))
+        self.vseg_count = np.diff(np.asarray(vptr, dtype=np.int64))
+        self.nvitem = max(1, len(vit))
+        self.vitems = _i32(np.asarray(vit if vit else [(0, 0, 0, 0)], dtype=np.int64).reshape(-1, 4),
+                           device)
+        self.vptr = _i32(np.asarray(vptr, dtype=np.int64), device)
+        self.nitem = len(items)
+        self.items = _i32(np.asarray(items, dtype=np.int64).reshape(-1, 4), device)
+        self.cptr = _i32(np.asarray(cptr, dtype=np.int64), device)
 
 
 class HMatrixGPU(object):
@@ -109,6 +140,10 @@ class HMatrixGPU(object):
             offU = np.concatenate([[0], np.cumsum(su)[:-1]]).astype(np.int64)
             offV = np.concatenate([[0], np.cumsum(sv)[:-1]]).astype(np.int64)
             offT = np.concatenate([[0], np.cumsum(rank)[:-1]]).astype(np.int64)
+            tp = topo.vseg_count * rank
+            offTP = np.concatenate([[0], np.cumsum(tp)[:-1]]).astype(np.int64)
+            self.offTP = _i64(offTP, dev)
+            self.tp_entries = int(tp.sum())
             self.rank_h = rank
             self.offU = _i64(offU, dev)
             self.offV = _i64(offV, dev)
@@ -122,7 +157,8 @@ class HMatrixGPU(object):
         else:
             self.rank_h = np.zeros(0, np.int64)
             z = _i64(np.zeros(1), dev)
-            self.offU = self.offV = self.offT = z
+            self.offU = self.offV = self.offT = self.offTP = z
+            self.tp_entries = 0
             self.U = self.V = torch.empty(2, dtype=torch.float32, device=dev)
             self.sum_rank = 0
         self.scratch = scratch
@@ -144,7 +180,7 @@ class HMatrixGPU(object):
         ov = int(self.offV[b].item())
         U = self.U[2 * ou:2 * (ou + m * r)].double().cpu().numpy().view(complex)
         V = self.V[2 * ov:2 * (ov + k * r)].double().cpu().numpy().view(complex)
-        return U.reshape(r, m).T, V.reshape(r, k).T
+        return U.reshape(r, m).T, V.reshape(k, r)       # V is stored transposed
 
 
 def hmat_matvec(hms, xs, ys, nc, stream=None):
@@ -156,9 +192,14 @@ def hmat_matvec(hms, xs, ys, nc, stream=None):
     dev = topo.device
     n = topo.n
     # one V^T x scratch per matrix (the matrices run in the same launch)
-    per = 2 * max(1, max(h.sum_rank for h in hms)) * min(nc, 8)
+    per = 2 * max(1, max(h.sum_rank for h in hms)) * min(nc, 4)
     T = torch.empty(per * len(hms), dtype=torch.float64, device=dev)
-    desc = np.zeros((len(hms), 11), dtype=np.uint64)
+    pxc = 2 * n * min(nc, 4)
+    Xc = torch.empty(pxc * len(hms), dtype=torch.float64, device=dev)
+    partial = torch.empty(len(hms) * topo.nitem * 32 * 4 * 2, dtype=torch.float64, device=dev)
+    ptp = 2 * 4 * max(1, max(h.tp_entries for h in hms))
+    TP = torch.empty(ptp * len(hms), dtype=torch.float64, device=dev)
+    desc = np.zeros((len(hms), 14), dtype=np.uint64)
     keep = []
     for i, (h, x, y) in enumerate(zip(hms, xs, ys)):
         if h.topo is not topo:
@@ -168,9 +209,12 @@ def hmat_matvec(hms, xs, ys, nc, stream=None):
             raise ValueError("hmat_matvec: x, y must be contiguous complex128 (nc, n)")
         desc[i] = [h.D.data_ptr(), h.U.data_ptr(), h.V.data_ptr(), h.rank.data_ptr(),
                    topo.offD.data_ptr(), h.offU.data_ptr(), h.offV.data_ptr(),
-                   h.offT.data_ptr(), x.data_ptr(), y.data_ptr(), T[i * per:].data_ptr()]
+                   h.offT.data_ptr(), x.data_ptr(), y.data_ptr(), T[i * per:].data_ptr(),
+                   Xc[i * pxc:].data_ptr(), h.offTP.data_ptr(), TP[i * ptp:].data_ptr()]
         keep.append((x, y))
     call('mnpb_hmat_matvec', _lib.stream_handle(stream), n, nc, len(hms), ptr(desc),
          ptr(topo.c2p), topo.ndense, ptr(topo.dense), topo.nlr, ptr(topo.lowrank), topo.nleaf,
-         ptr(topo.leaf_rows), ptr(topo.lptr), ptr(topo.lent))
+         ptr(topo.leaf_rows), ptr(topo.lptr), ptr(topo.lent), topo.nchunk, ptr(topo.chunks),
+         topo.nitem, ptr(topo.items), ptr(topo.cptr), ptr(partial), topo.nvitem,
+         ptr(topo.vitems), ptr(topo.vptr))
     return ys
