@@ -53,7 +53,66 @@ def parse():
     ap.add_argument('--nlam', type=int, default=81)
     ap.add_argument('--no-cpu-baseline', action='store_true')
     ap.add_argument('--prof-dump', default=None, help='CSV of every timed launch')
+    ap.add_argument('--no-iterative', action='store_true',
+                    help='skip the H-matrix / GMRES measurement on the 25k-face rod')
+    ap.add_argument('--iter-nlam', type=int, default=6)
     return ap.parse_args()
+
+
+ITER_WORKLOAD = ("BEMRetIter H-matrix sweep: trirod(20 nm, 80 nm, [97, 47, 171]) = 25152 flat "
+                 "faces, Drude Au in vacuum, plane wave along the rod axis (pol x, dir z), ACA "
+                 "cleaf 64 htol 1e-6 (complex64 factors), GMRES tol 1e-6 unpreconditioned, "
+                 "wavelengths 500 nm + 2.5 nm steps (the 201-point 500-1000 nm grid)")
+
+
+def iterative_section(args):
+    """Solves/s, operator applications, ACA time and H-matrix product
+    bandwidth of the iterative path on the 25k-face rod (a short sweep of
+    the 201-wavelength grid, zero-start and extrapolated-start GMRES)."""
+    import torch
+    import mnpbem_b200 as M
+    from mnpbem_b200 import _lib
+    from mnpbem_b200.bem_iter import BEMRetIter
+    from mnpbem_b200.excitation import PlaneWaveRet
+    cp = M.ComParticle([M.EpsConst(1.0), M.EpsDrude(*DRUDE)],
+                       [M.trirod(20.0, 80.0, (97, 47, 171))], [[2, 1]], 1)
+    exc = PlaneWaveRet(pol=[[1.0, 0, 0]], dir=[[0, 0, 1.0]])
+    eneis = list(500.0 + 2.5 * np.arange(args.iter_nlam))
+    t0 = time.time()
+    bem = BEMRetIter(cp, hmatrix=True, cleaf=64, htol=1e-6, preconditioner='none', tol=1e-6,
+                     maxit=200)
+    bem._init_matrices(eneis[0] - 2.5)          # warm-up: topology, kernels
+    torch.cuda.synchronize()
+    ctor = time.time() - t0
+    out = {"workload": ITER_WORKLOAD, "n_faces": cp.n, "constructor_s": ctor}
+    for mode, warm in (("zero_start", None), ("extrapolated_start", "extrapolate")):
+        bem.enei = None
+        _lib.prof_begin()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        sols, stats, _ = bem.solve_spectrum(exc, eneis, warm=warm)
+        e1.record()
+        torch.cuda.synchronize()
+        prof = _lib.prof_end()
+        ms = e0.elapsed_time(e1)
+        mv = [s['matvecs'] for s in stats]
+        out[mode] = {"lambda_solves_per_s": len(eneis) / (ms / 1000.0),
+                     "operator_applications_per_lambda": float(np.mean(mv)),
+                     "all_converged": all(s['flag'] == 0 for s in stats),
+                     "ms_by_class": {k: round(v[0] / len(eneis), 3) for k, v in prof.items()}}
+        if 'hmat_matvec' in prof:
+            hms = (bem.G1, bem.G2, bem.H1, bem.H2)
+            nbytes = sum(h.stored_bytes() for h in hms)
+            hm_ms, _, cnt = prof['hmat_matvec']
+            out["hmat_product"] = {"bytes_per_application": nbytes,
+                                   "ms_per_application": hm_ms / cnt,
+                                   "achieved_GBs": nbytes / (hm_ms / cnt) / 1e6}
+    out["compression"] = [round(c, 4) for c in bem.compression()]
+    out["wavelengths"] = [float(e) for e in eneis]
+    del bem
+    torch.cuda.empty_cache()
+    return out
 
 
 # ---------------------------------------------------------------------------
@@ -338,6 +397,14 @@ def main():
                          "reference, LAPACK LU, %d BLAS threads); constructor %.1f s "
                          "excluded" % (cores, ctor)}
 
+    iterative = None
+    if rank == 0 and not args.no_iterative:
+        iterative = iterative_section(args)
+        if iterative.get("hmat_product"):
+            iterative["hmat_product"]["peak_GBs"] = peaks['hbm_gbs']
+            iterative["hmat_product"]["frac"] = (iterative["hmat_product"]["achieved_GBs"] /
+                                                 peaks['hbm_gbs'])
+
     if rank == 0:
         out = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
@@ -356,6 +423,7 @@ def main():
             "roofline": roof,
             "cpu_baseline": cpu,
             "clocks": ck,
+            "iterative": iterative,
         }
         print(json.dumps(out))
     if world > 1:
