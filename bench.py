@@ -10,9 +10,10 @@ Metric: wavelength-solves per second.
     python bench.py [--gpus N] [--steps K] [--warmup W] [--path fp64|mixed]
     python bench.py --impl reference ...   # CPU oracle of the same workload
 
-Multi-GPU: one process per GPU (torchrun); each rank sweeps its own spectrum
-(weak scaling, replicas -- the wavelengths are independent, no collective on
-the data path); the time is the max over ranks.
+Multi-GPU: one process per GPU (torchrun); N GPUs sweep an 81*N-point
+spectrum, each rank an interleaved 81 of its wavelengths (weak scaling -- the
+wavelengths are independent, no collective on the data path); the spectrum
+is all-gathered once at the end and the time is the max over ranks.
 
 The timed region starts with the geometry tables resident in HBM; every
 wavelength's matrices (4 x 133 MB per wavelength) exceed L2 many times over,
@@ -261,7 +262,12 @@ def main():
     exc = excitation.PlaneWaveRet(pol=[[1.0, 0, 0]], dir=[[0, 0, 1.0]])
     global NLAM
     NLAM = args.nlam
-    eneis = list(np.linspace(400, 800, NLAM))
+    # N GPUs: a weak-scaled sweep of NLAM * N wavelengths over 400-800 nm,
+    # dealt out interleaved; every rank solves NLAM of them
+    from mnpbem_b200 import replicas
+    eneis_all = np.linspace(400, 800, NLAM * world)
+    local_idx = replicas.shard(len(eneis_all), rank, world) if world > 1 else np.arange(NLAM)
+    eneis = list(eneis_all[local_idx])
     n = solver.tables.n
     B = args.batch
 
@@ -314,10 +320,12 @@ def main():
     launches = _lib.launch_count() - launches0
     ck = clocks.stop()
     ms = ev0.elapsed_time(ev1)
+    gathered = None
     if world > 1:
-        t = torch.tensor([ms], device='cuda')
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+        ms = replicas.max_over_ranks(ms)
+        # the one collective of the sweep: the full extinction spectrum on every rank
+        spec = replicas.gather_rows(ext_of(device_step())[:, None], local_idx, len(eneis_all))
+        gathered = int(np.isfinite(spec).all(axis=1).sum())
     value = world * NLAM * args.steps / (ms / 1000.0)
 
     # end to end through the public API with host buffers
@@ -331,9 +339,7 @@ def main():
     torch.cuda.synchronize()
     e2e_ms = e0.elapsed_time(e1)
     if world > 1:
-        t = torch.tensor([e2e_ms], device='cuda')
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
+        e2e_ms = replicas.max_over_ranks(e2e_ms)
     e2e_value = world * NLAM * args.steps / (e2e_ms / 1000.0)
     K = 1
     h2d = NLAM * (4 * 8 + 8 + 2 * 2 * 16 + 16 * 8)     # eps/k tables, block k tables, pol/dir
@@ -398,7 +404,7 @@ def main():
                          "excluded" % (cores, ctor)}
 
     iterative = None
-    if rank == 0 and not args.no_iterative:
+    if rank == 0 and world == 1 and not args.no_iterative:
         iterative = iterative_section(args)
         if iterative.get("hmat_product"):
             iterative["hmat_product"]["peak_GBs"] = peaks['hbm_gbs']
@@ -415,7 +421,10 @@ def main():
             "config": {"workload": WORKLOAD, "path": args.path, "batch_wavelengths": B,
                        "n_faces": n, "wavelengths": NLAM,
                        "l2": "inputs larger than L2 (4 x 133 MB per wavelength)",
-                       "parallelism": "replicas over wavelengths" if world > 1 else "1 GPU"},
+                       "parallelism": ("%d ranks, interleaved wavelengths of a %d-point "
+                                       "sweep, one all-gather of the spectrum"
+                                       % (world, NLAM * world)) if world > 1 else "1 GPU",
+                       "spectrum_points_gathered": gathered},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
             "gpu_launches": launches,
