@@ -126,6 +126,160 @@ __global__ void __launch_bounds__(PANEL_THREADS) panel_kernel(int n, int k0, int
     }
 }
 
+// LU leaf in shared memory: columns [k0, k0+kb) factored as kb/SW slabs of SW
+// columns.  A slab (rows cs..n-1, SW columns, planar) is loaded into shared
+// memory and factored there column by column (partial pivoting on |re|+|im|,
+// as the global-memory leaf); row swaps are mirrored into the panel's other
+// columns in global memory.  The panel's columns right of the slab then get
+// one block update: U12 = L11^{-1} A12 on the slab's SW rows, A22 -= L21 U12
+// below.  Compared with the global-memory leaf, each panel column is read and
+// written once per slab instead of once per column.  Dynamic shared memory:
+// SW * (n - k0) * 8 bytes.
+constexpr int SLAB_THREADS = 512;
+template <int SW>
+__global__ void __launch_bounds__(SLAB_THREADS) panel_slab_kernel(int n, int k0, int kb, float *A,
+                                                                 int64_t lda, int64_t plane,
+                                                                 int64_t sA, int32_t *ipiv,
+                                                                 int64_t sP, int32_t *info) {
+    extern __shared__ float slab_sm[];
+    __shared__ float red_v[SLAB_THREADS / 32];
+    __shared__ int red_i[SLAB_THREADS / 32];
+    __shared__ cf u12[SW][TS];
+    __shared__ int s_piv;
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    const int64_t b = blockIdx.x;
+    A += b * sA;
+    ipiv += b * sP;
+    const int mmax = n - k0;
+    float *sre = slab_sm, *sim = slab_sm + (int64_t)SW * mmax;
+    for (int cs = k0; cs < k0 + kb; cs += SW) {
+        const int ms = n - cs;                         // slab rows cs .. n-1
+        for (int e = tid; e < SW * ms; e += SLAB_THREADS) {
+            const int j = e / ms, i = e - j * ms;
+            const int64_t o = (int64_t)(cs + j) * lda + cs + i;
+            sre[j * mmax + i] = A[o];
+            sim[j * mmax + i] = A[o + plane];
+        }
+        __syncthreads();
+        for (int jj = 0; jj < SW; ++jj) {
+            const int c = cs + jj;
+            const float *cre = sre + jj * mmax, *cim = sim + jj * mmax;
+            float best = -1.f;
+            int bi = ms;
+            for (int i = jj + tid; i < ms; i += SLAB_THREADS) {
+                const float v = fabsf(cre[i]) + fabsf(cim[i]);
+                if (v > best) { best = v; bi = i; }
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                const float ov = __shfl_xor_sync(0xffffffffu, best, o);
+                const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+                if (ov > best || (ov == best && oi < bi)) { best = ov; bi = oi; }
+            }
+            if (lane == 0) { red_v[wid] = best; red_i[wid] = bi; }
+            __syncthreads();
+            if (wid == 0) {
+                best = (lane < SLAB_THREADS / 32) ? red_v[lane] : -1.f;
+                bi = (lane < SLAB_THREADS / 32) ? red_i[lane] : ms;
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) {
+                    const float ov = __shfl_xor_sync(0xffffffffu, best, o);
+                    const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+                    if (ov > best || (ov == best && oi < bi)) { best = ov; bi = oi; }
+                }
+                if (lane == 0) {
+                    int ip = bi;
+                    if (!(best > 0.f)) {
+                        ip = jj;
+                        if (info && info[b] == 0) info[b] = c + 1;
+                    }
+                    s_piv = ip;
+                    ipiv[c] = cs + ip;
+                }
+            }
+            __syncthreads();
+            const int ip = s_piv;
+            if (ip != jj) {
+                for (int j = tid; j < SW; j += SLAB_THREADS) {
+                    float t = sre[j * mmax + jj];
+                    sre[j * mmax + jj] = sre[j * mmax + ip];
+                    sre[j * mmax + ip] = t;
+                    t = sim[j * mmax + jj];
+                    sim[j * mmax + jj] = sim[j * mmax + ip];
+                    sim[j * mmax + ip] = t;
+                }
+                for (int cc = tid; cc < kb; cc += SLAB_THREADS) {
+                    const int col = k0 + cc;
+                    if (col >= cs && col < cs + SW) continue;
+                    const int64_t o = (int64_t)col * lda;
+                    const cf t = ld(A, plane, o + c);
+                    st(A, plane, o + c, ld(A, plane, o + cs + ip));
+                    st(A, plane, o + cs + ip, t);
+                }
+            }
+            __syncthreads();
+            const cf pv = fmk(sre[jj * mmax + jj], sim[jj * mmax + jj]);
+            const bool nz = (pv.x != 0.f || pv.y != 0.f);
+            const cf inv = nz ? frcp(pv) : fmk(0.f, 0.f);
+            for (int i = jj + 1 + tid; i < ms; i += SLAB_THREADS) {
+                cf l = fmk(sre[jj * mmax + i], sim[jj * mmax + i]);
+                if (nz) l = fmul(l, inv);
+                sre[jj * mmax + i] = l.x;
+                sim[jj * mmax + i] = l.y;
+                for (int j = jj + 1; j < SW; ++j) {
+                    const cf u = fmk(sre[j * mmax + jj], sim[j * mmax + jj]);
+                    cf a = fmk(sre[j * mmax + i], sim[j * mmax + i]);
+                    a = ffms(l, u, a);
+                    sre[j * mmax + i] = a.x;
+                    sim[j * mmax + i] = a.y;
+                }
+            }
+            __syncthreads();
+        }
+        for (int e = tid; e < SW * ms; e += SLAB_THREADS) {
+            const int j = e / ms, i = e - j * ms;
+            const int64_t o = (int64_t)(cs + j) * lda + cs + i;
+            A[o] = sre[j * mmax + i];
+            A[o + plane] = sim[j * mmax + i];
+        }
+        const int c1 = cs + SW, R = k0 + kb - c1;
+        if (R > 0) {
+            // U12 = L11^{-1} A12 (unit lower SW x SW from the slab's top rows)
+            for (int q = tid; q < R; q += SLAB_THREADS) {
+                const int64_t o = (int64_t)(c1 + q) * lda + cs;
+                cf x[SW];
+#pragma unroll
+                for (int r = 0; r < SW; ++r) x[r] = ld(A, plane, o + r);
+#pragma unroll
+                for (int r = 1; r < SW; ++r)
+#pragma unroll
+                    for (int t = 0; t < r; ++t)
+                        x[r] = ffms(fmk(sre[t * mmax + r], sim[t * mmax + r]), x[t], x[r]);
+#pragma unroll
+                for (int r = 0; r < SW; ++r) {
+                    st(A, plane, o + r, x[r]);
+                    u12[r][q] = x[r];
+                }
+            }
+            __syncthreads();
+            // A22 -= L21 U12 on rows cs+SW .. n-1
+            for (int i = SW + tid; i < ms; i += SLAB_THREADS) {
+                cf l[SW];
+#pragma unroll
+                for (int t = 0; t < SW; ++t) l[t] = fmk(sre[t * mmax + i], sim[t * mmax + i]);
+                for (int q = 0; q < R; ++q) {
+                    const int64_t o = (int64_t)(c1 + q) * lda + cs + i;
+                    cf a = ld(A, plane, o);
+#pragma unroll
+                    for (int t = 0; t < SW; ++t) a = ffms(l[t], u12[t][q], a);
+                    st(A, plane, o, a);
+                }
+            }
+        }
+        __syncthreads();
+    }
+}
+
 __global__ void laswp_kernel(float *A, int64_t lda, int64_t plane, int64_t sA, int j0, int j1,
                              const int32_t *ipiv, int64_t sP, int c0, int c1, int forward) {
     const int64_t b = blockIdx.y;
@@ -599,6 +753,24 @@ static int rgetrf(Ctx &c, int n, int off, int w, CMatF A, int32_t *ipiv, int64_t
     if (w <= TS) {
         ProfScope ps(c.s, PC_PANEL, 8.0 * w * w * (double)(n - off) * c.batch / 2);
         prof_tag("off=%d w=%d B=%d", off, w, c.batch);
+        constexpr int SW = 8;
+        const int64_t slab_bytes = (int64_t)SW * (n - off) * 8;
+        if (w % SW == 0 && w <= TS && slab_bytes <= 200 * 1024) {
+            static bool attr = false;
+            if (!attr) {
+                if (cudaFuncSetAttribute(panel_slab_kernel<SW>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         200 * 1024) != cudaSuccess) {
+                    set_error("panel_slab_kernel: cannot reserve shared memory");
+                    return MNPB_ECUDA;
+                }
+                attr = true;
+            }
+            panel_slab_kernel<SW><<<c.batch, SLAB_THREADS, (size_t)slab_bytes, c.s>>>(
+                n, off, w, A.p, A.ld, A.plane, A.stride, ipiv, sP, info);
+            MNPB_LAUNCH_CHECK("panel_slab_kernel(f32)");
+            return MNPB_OK;
+        }
         panel_kernel<<<c.batch, PANEL_THREADS, 0, c.s>>>(n, off, w, A.p, A.ld, A.plane, A.stride,
                                                          ipiv, sP, info);
         MNPB_LAUNCH_CHECK("panel_kernel(f32)");
