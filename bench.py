@@ -51,13 +51,98 @@ def parse():
     ap.add_argument('--path', default='mixed', choices=['fp64', 'mixed'])
     ap.add_argument('--no-accuracy', action='store_true')
     ap.add_argument('--batch', type=int, default=81)
+    ap.add_argument('--streams', type=int, default=1,
+                    help='sub-batches of --batch wavelengths solved concurrently')
     ap.add_argument('--nlam', type=int, default=81)
     ap.add_argument('--no-cpu-baseline', action='store_true')
     ap.add_argument('--prof-dump', default=None, help='CSV of every timed launch')
     ap.add_argument('--no-iterative', action='store_true',
                     help='skip the H-matrix / GMRES measurement on the 25k-face rod')
     ap.add_argument('--iter-nlam', type=int, default=6)
+    ap.add_argument('--probe', default=None, choices=['tc_gemm', 'hmat', 'lu'],
+                    help='run one representative kernel on a small case (profiling target) '
+                         'and print its timing instead of the benchmark')
     return ap.parse_args()
+
+
+def run_probe(args):
+    """Small, self-contained kernel cases for ncu captures (a few GB on the
+    device at most, a handful of launches):
+
+    * tc_gemm: C = C - A B, planar complex FP32, M = 2884, N = 1440,
+      K = 1444, batch 4 (the largest trailing update of the 2884-face LU);
+    * hmat: the four-matrix H-matrix product of trirod(20, 80, [61, 31, 101])
+      (9600 faces) at 600 nm, ACA cleaf 64 htol 1e-6, 4 right-hand sides;
+    * lu: mixed-precision LU (recursive, tensor-core updates, shared-memory
+      slab leaves) of 8 random 2884 x 2884 complex matrices."""
+    import torch
+    from mnpbem_b200 import _lib
+    from mnpbem_b200._lib import call, ptr
+    torch.manual_seed(0)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    out = {"probe": args.probe}
+    if args.probe == 'tc_gemm':
+        M, N, K, B = 2884, 1440, 1444, 4
+        ld, ldb = 2884, 1444
+        A = torch.randn((B, 2, K, ld), device='cuda')
+        Bm = torch.randn((B, 2, N, ldb), device='cuda')
+        C = torch.randn((B, 2, N, ld), device='cuda')
+        wb = int(_lib.lib().mnpb_cgemm_tf32_workspace(M, K, B))
+        W = torch.empty(wb, dtype=torch.uint8, device='cuda')
+
+        def f():
+            call('mnpb_cgemm_tf32', _lib.stream_handle(), M, N, K, B, -1.0, ptr(A), ld, K * ld,
+                 2 * K * ld, ptr(Bm), ldb, N * ldb, 2 * N * ldb, 1.0, ptr(C), ld, N * ld,
+                 2 * N * ld, ptr(W), wb)
+        flops = 8.0 * M * N * K * B
+    elif args.probe == 'hmat':
+        import mnpbem_b200 as Mb
+        from mnpbem_b200.bem_iter import BEMRetIter
+        from mnpbem_b200.hmatrix import hmat_matvec
+        cp = Mb.ComParticle([Mb.EpsConst(1.0), Mb.EpsDrude(*DRUDE)],
+                            [Mb.trirod(20.0, 80.0, (61, 31, 101))], [[2, 1]], 1)
+        bem = BEMRetIter(cp, hmatrix=True, cleaf=64, htol=1e-6, preconditioner='none')
+        bem._init_matrices(600.0)
+        bem._scratch = None                 # ACA scratch: not needed for products
+        torch.cuda.empty_cache()
+        n = cp.n
+        hms = [bem.G1, bem.G2, bem.H1, bem.H2]
+        xs = [torch.randn((4, n), dtype=torch.complex128, device='cuda') for _ in range(4)]
+        ys = [torch.empty_like(x) for x in xs]
+
+        def f():
+            hmat_matvec(hms, xs, ys, 4)
+        out["bytes"] = sum(h.stored_bytes() for h in hms)
+        flops = None
+    else:
+        n, B = 2884, 8
+        ld = 2884
+        A0 = torch.randn((B, 2, n, ld), device='cuda')
+        A = A0.clone()
+        piv = torch.empty((B, n), dtype=torch.int32, device='cuda')
+        info = torch.zeros(B, dtype=torch.int32, device='cuda')
+        wb = int(_lib.lib().mnpb_f32_workspace(n, B))
+        W = torch.empty(wb, dtype=torch.uint8, device='cuda')
+
+        def f():
+            A.copy_(A0)
+            call('mnpb_getrf_c32p', _lib.stream_handle(), n, B, ptr(A), ld, n * ld, 2 * n * ld,
+                 ptr(piv), n, ptr(info), ptr(W), wb)
+        flops = 8.0 / 3.0 * n ** 3 * B
+    for _ in range(2):
+        f()
+    torch.cuda.synchronize()
+    e0.record()
+    f()
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    out["ms"] = ms
+    if flops:
+        out["tflops"] = flops / ms / 1e9
+    if "bytes" in out:
+        out["GBs"] = out["bytes"] / ms / 1e6
+    print(json.dumps(out))
 
 
 ITER_WORKLOAD = ("BEMRetIter H-matrix sweep: trirod(20 nm, 80 nm, [97, 47, 171]) = 25152 flat "
@@ -238,6 +323,9 @@ def run_reference(args, rank):
 # ---------------------------------------------------------------------------
 def main():
     args = parse()
+    if args.probe:
+        run_probe(args)
+        return
     rank = int(os.environ.get('RANK', '0'))
     world = int(os.environ.get('WORLD_SIZE', '1'))
     local = int(os.environ.get('LOCAL_RANK', '0'))
@@ -276,18 +364,19 @@ def main():
     def device_step(slv=None):
         """One spectrum sweep with every array resident on the GPU."""
         slv = slv or solver
-        exts = []
-        for s0 in range(0, NLAM, B):
-            chunk = eneis[s0:s0 + B]
-            bt = slv._factor(chunk)
-            pots, K = exc.potential_device(cp, slv.tables, chunk)
-            xout = slv._solve_batch(bt, pots, K)
-            e, _ = exc.farfield_device(cp, slv.tables, xout, chunk, exc.dir)
-            exts.append(e)
+
+        def work(chunk, st):
+            bt = slv._factor(chunk, stream=st)
+            pots, K = exc.potential_device(cp, slv.tables, chunk, stream=st)
+            xout = slv._solve_batch(bt, pots, K, stream=st)
+            e, _ = exc.farfield_device(cp, slv.tables, xout, chunk, exc.dir, stream=st)
             if getattr(bt, 'iters', None) is not None:
                 refine_iters.extend(int(v) for v in bt.iters)
             del bt
-        return exts
+            return e
+
+        chunks = [eneis[s0:s0 + B] for s0 in range(0, NLAM, B)]
+        return bem.BEMRet.pipeline(chunks, work, args.streams)
 
     def ext_of(exts):
         kk = np.array([complex(*exc._wavenumbers(cp, [l])[0][0]) for l in eneis])
@@ -334,7 +423,7 @@ def main():
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record()
     for _ in range(args.steps):
-        sols = solver.solve_spectrum(exc, eneis, batch=B)
+        sols = solver.solve_spectrum(exc, eneis, batch=B, streams=args.streams)
     e1.record()
     torch.cuda.synchronize()
     e2e_ms = e0.elapsed_time(e1)
@@ -419,6 +508,7 @@ def main():
             "dtype": "f64" if args.path == 'fp64' else "tf32/bf16x3+f64-refine",
             "data": "synthetic",
             "config": {"workload": WORKLOAD, "path": args.path, "batch_wavelengths": B,
+                       "concurrent_batches": args.streams,
                        "n_faces": n, "wavelengths": NLAM,
                        "l2": "inputs larger than L2 (4 x 133 MB per wavelength)",
                        "parallelism": ("%d ranks, interleaved wavelengths of a %d-point "

@@ -276,19 +276,67 @@ class BEMRet(object):
         return self.solve(exc)
 
     # ------------------------------------------------------- spectrum sweeps
-    def solve_spectrum(self, exc, eneis, batch=16, stream=None):
+    @staticmethod
+    def pipeline(chunks, work, streams):
+        """Run ``work(chunk, stream)`` for every chunk on ``streams`` CUDA
+        streams, chunks dealt out round-robin, each stream driven by its own
+        host thread; results in chunk order.  While one stream's refinement
+        waits on the host between corrections, the other streams'
+        factorisations keep the GPU busy.  The caller's current stream waits
+        for all of them before returning."""
+        import threading
+        cur = torch.cuda.current_stream()
+        if streams <= 1 or len(chunks) <= 1:
+            return [work(c, cur) for c in chunks]
+        streams = min(streams, len(chunks))
+        sts = [torch.cuda.Stream() for _ in range(streams)]
+        for st in sts:
+            st.wait_stream(cur)
+        results = [None] * len(chunks)
+        errors = []
+
+        def run(k):
+            try:
+                with torch.cuda.stream(sts[k]):
+                    for i in range(k, len(chunks), streams):
+                        results[i] = work(chunks[i], sts[k])
+            except BaseException as e:       # re-raised in the caller's thread
+                errors.append(e)
+
+        threads = [threading.Thread(target=run, args=(k,)) for k in range(streams)]
+        for t in threads:
+            t.start()
+        for t in threads:
+            t.join()
+        for st in sts:
+            cur.wait_stream(st)
+        if errors:
+            raise errors[0]
+        return results
+
+    def solve_spectrum(self, exc, eneis, batch=16, stream=None, streams=1):
         """Solutions for every wavelength of ``eneis`` (host CompStructs).
 
         ``exc`` is a plane-wave excitation of this package (its potentials
         are generated on the GPU) or any object with ``potential(p, enei)``.
+        Wavelengths are solved ``batch`` at a time; ``streams`` > 1 runs that
+        many batches concurrently (see ``pipeline``).
         """
+        chunks = [list(eneis[s:s + batch]) for s in range(0, len(eneis), batch)]
+
+        def work(chunk, st):
+            bt = self._factor(chunk, stream=st)
+            pots, K = self._spectrum_pots(exc, chunk, st)
+            xout = self._solve_batch(bt, pots, K, stream=st)
+            return xout.cpu().numpy(), K
+
+        if streams > 1:
+            res = self.pipeline(chunks, work, streams)
+        else:
+            cur = stream if stream is not None else torch.cuda.current_stream()
+            res = [work(c, cur) for c in chunks]
         out = []
-        for s in range(0, len(eneis), batch):
-            chunk = list(eneis[s:s + batch])
-            bt = self._factor(chunk, stream=stream)
-            pots, K = self._spectrum_pots(exc, chunk, stream)
-            xout = self._solve_batch(bt, pots, K, stream=stream)
-            x = xout.cpu().numpy()
+        for chunk, (x, K) in zip(chunks, res):
             for b, enei in enumerate(chunk):
                 out.append(self._to_compstruct(x[b], K, enei))
         return out

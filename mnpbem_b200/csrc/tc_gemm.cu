@@ -314,6 +314,218 @@ __global__ void __launch_bounds__(128)
     }
 }
 
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+
+// Persistent variant for large GEMMs: one CTA per SM walks the output tiles
+// (t = blockIdx.x, blockIdx.x + gridDim.x, ...; M fastest, then N, then the
+// batch).  Warp 0 issues the TMA loads of a stage ring that runs on across
+// tiles, warp 1 allocates all 512 TMEM columns and issues the MMAs into two
+// accumulator buffers (re + im, 2 x BN columns each), warps 2-5 drain a
+// finished buffer into C (warp w owns TMEM lanes 32 (w % 4) ..) while the MMAs
+// of the next tile fill the other one.  acc_full[b] (MMA -> epilogue, one
+// commit) and acc_empty[b] (epilogue -> MMA, 128 arrivals) hand the buffers
+// over.  Every wait is bounded as in cgemm_tf32_kernel.
+template <int BN>
+__global__ void __launch_bounds__(192, 1)
+    cgemm_tf32_persistent(const __grid_constant__ CUtensorMap tmA,
+                          const __grid_constant__ CUtensorMap tmBr,
+                          const __grid_constant__ CUtensorMap tmBi, Epi ep, int STAGES, int MT,
+                          int NT, int ntiles) {
+    using TL = Tile<BN>;
+    constexpr int STAGE_BYTES = TL::STAGE_BYTES;
+    constexpr int TILE_BYTES = TILE_A_BYTES;
+    constexpr int ACC_COLS = 2 * BN;
+    constexpr int TMEM_COLS = 2 * ACC_COLS;
+    static_assert(TMEM_COLS <= 512, "two accumulator buffers must fit in TMEM");
+    extern __shared__ __align__(1024) uint8_t smem_raw[];
+    uint8_t *smem = (uint8_t *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+    uint64_t *bars = (uint64_t *)(smem + STAGES * STAGE_BYTES);
+    // bars: full [0, S), empty [S, 2S), acc_full 2S + {0,1}, acc_empty 2S + {2,3}
+    uint32_t *tmem_slot = (uint32_t *)(bars + 2 * MAX_STAGES + 4);
+    volatile int *abort_flag = (volatile int *)(tmem_slot + 1);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int TPB = MT * NT;   // tiles per batch entry
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < STAGES; ++s) {
+            mbar_init(smem_u32(&bars[s]), 1);
+            mbar_init(smem_u32(&bars[STAGES + s]), 1);
+        }
+        mbar_init(smem_u32(&bars[2 * STAGES + 0]), 1);
+        mbar_init(smem_u32(&bars[2 * STAGES + 1]), 1);
+        mbar_init(smem_u32(&bars[2 * STAGES + 2]), 128);
+        mbar_init(smem_u32(&bars[2 * STAGES + 3]), 128);
+        *abort_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                         smem_u32(tmem_slot)),
+                     "r"(TMEM_COLS)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    fence_before();
+    __syncthreads();
+    fence_after();
+    const uint32_t tmem = *tmem_slot;
+    const int KT = ep.ktiles;
+
+    if (warp == 0) {
+        if (lane == 0) {
+            // TMA producer
+            uint32_t g = 0;
+            for (int t = blockIdx.x; t < ntiles && !*abort_flag; t += gridDim.x) {
+                const int b = t / TPB, rem = t - b * TPB;
+                const int nt = rem / MT, mt = rem - nt * MT;
+                const int m0 = mt * BM, n0 = nt * BN;
+                bool ok = true;
+                for (int kt = 0; kt < KT; ++kt, ++g) {
+                    const int s = g % STAGES;
+                    if (g >= (uint32_t)STAGES &&
+                        !mbar_wait(smem_u32(&bars[STAGES + s]), ((g / STAGES) - 1) & 1)) {
+                        atomicCAS(&g_tc_error, 0, 1);
+                        *abort_flag = 1;
+                        ok = false;
+                        break;
+                    }
+                    if (*abort_flag) {
+                        ok = false;
+                        break;
+                    }
+                    uint8_t *st = smem + s * STAGE_BYTES;
+                    const uint32_t full = smem_u32(&bars[s]);
+                    mbar_expect_tx(full, STAGE_BYTES);
+                    const int k0 = kt * BK;
+                    tma_load_3d(smem_u32(st), &tmA, full, k0, m0, 2 * b);
+                    tma_load_3d(smem_u32(st + TILE_BYTES), &tmA, full, k0, m0, 2 * b + 1);
+                    tma_load_3d(smem_u32(st + 2 * TILE_BYTES), &tmBr, full, k0, n0, b);
+                    tma_load_3d(smem_u32(st + 2 * TILE_BYTES + TL::B_BYTES), &tmBi, full, k0, n0,
+                                b);
+                }
+                if (!ok) break;
+            }
+        }
+    } else if (warp == 1) {
+        if (lane == 0) {
+            // MMA issuer
+            constexpr uint32_t ID = idesc_tf32(false, BN), IDN = idesc_tf32(true, BN);
+            uint32_t g = 0;
+            int i = 0;
+            for (int t = blockIdx.x; t < ntiles && !*abort_flag; t += gridDim.x, ++i) {
+                const int buf = i & 1;
+                if (i >= 2 && !mbar_wait(smem_u32(&bars[2 * STAGES + 2 + buf]), ((i >> 1) - 1) & 1)) {
+                    atomicCAS(&g_tc_error, 0, 4);
+                    *abort_flag = 1;
+                    break;
+                }
+                fence_after();
+                const uint32_t d_re = tmem + buf * ACC_COLS, d_im = d_re + BN;
+                bool ok = true;
+                for (int kt = 0; kt < KT; ++kt, ++g) {
+                    const int s = g % STAGES;
+                    if (!mbar_wait(smem_u32(&bars[s]), (g / STAGES) & 1)) {
+                        atomicCAS(&g_tc_error, 0, 2);
+                        *abort_flag = 1;
+                        ok = false;
+                        break;
+                    }
+                    fence_after();
+                    const uint32_t st = smem_u32(smem + s * STAGE_BYTES);
+#pragma unroll
+                    for (int j = 0; j < BK / 8; ++j) {
+                        const uint32_t off = 32 * j;
+                        const uint64_t ar = smem_desc_k128(st + off);
+                        const uint64_t ai = smem_desc_k128(st + TILE_BYTES + off);
+                        const uint64_t br = smem_desc_k128(st + 2 * TILE_BYTES + off);
+                        const uint64_t bi = smem_desc_k128(st + 2 * TILE_BYTES + TL::B_BYTES + off);
+                        const uint32_t acc = (kt > 0 || j > 0) ? 1u : 0u;
+                        mma_tf32(d_re, ar, br, ID, acc);
+                        mma_tf32(d_re, ai, bi, IDN, 1u);
+                        mma_tf32(d_im, ar, bi, ID, acc);
+                        mma_tf32(d_im, ai, br, ID, 1u);
+                    }
+                    mma_commit(smem_u32(&bars[STAGES + s]));
+                }
+                mma_commit(smem_u32(&bars[2 * STAGES + buf]));
+                if (!ok) break;
+            }
+        }
+    } else {
+        // epilogue warps 2..5
+        const int q = warp & 3;
+        const uint32_t lane_base = (uint32_t)(q * 32) << 16;
+        int i = 0;
+        for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++i) {
+            const int buf = i & 1;
+            const bool acc_ok = mbar_wait(smem_u32(&bars[2 * STAGES + buf]), (i >> 1) & 1);
+            if (!acc_ok) {
+                atomicCAS(&g_tc_error, 0, 3);
+                *abort_flag = 1;
+                break;
+            }
+            fence_after();
+            if (*abort_flag) break;
+            const int b = t / TPB, rem = t - b * TPB;
+            const int nt = rem / MT, mt = rem - nt * MT;
+            const int m0 = mt * BM, n0 = nt * BN;
+            const uint32_t d_re = tmem + buf * ACC_COLS, d_im = d_re + BN;
+            const int row = m0 + q * 32 + lane;
+            float *Cr = ep.C + (int64_t)b * ep.strideC;
+            float *Ci = Cr + ep.planeC;
+            const bool row_ok = row < ep.M;
+            constexpr int CH = 16;
+#pragma unroll 1
+            for (int c0 = 0; c0 < BN; c0 += CH) {
+                float vr[CH], vi[CH];
+                tmem_ld16(d_re + lane_base + c0, vr);
+                tmem_ld16(d_im + lane_base + c0, vi);
+                const int ncol = min(CH, ep.N - (n0 + c0));
+                if (!row_ok || ncol <= 0) continue;
+                const int64_t o0 = (int64_t)(n0 + c0) * ep.ldc + row;
+                if (ep.beta != 0.f) {
+                    float cr[CH], ci[CH];
+#pragma unroll
+                    for (int c = 0; c < CH; ++c) {
+                        cr[c] = c < ncol ? __ldg(Cr + o0 + (int64_t)c * ep.ldc) : 0.f;
+                        ci[c] = c < ncol ? __ldg(Ci + o0 + (int64_t)c * ep.ldc) : 0.f;
+                    }
+#pragma unroll
+                    for (int c = 0; c < CH; ++c) {
+                        vr[c] = fmaf(ep.beta, cr[c], ep.alpha * vr[c]);
+                        vi[c] = fmaf(ep.beta, ci[c], ep.alpha * vi[c]);
+                    }
+                } else {
+#pragma unroll
+                    for (int c = 0; c < CH; ++c) {
+                        vr[c] *= ep.alpha;
+                        vi[c] *= ep.alpha;
+                    }
+                }
+#pragma unroll
+                for (int c = 0; c < CH; ++c) {
+                    if (c < ncol) {
+                        Cr[o0 + (int64_t)c * ep.ldc] = vr[c];
+                        Ci[o0 + (int64_t)c * ep.ldc] = vi[c];
+                    }
+                }
+            }
+            fence_before();
+            mbar_arrive(smem_u32(&bars[2 * STAGES + 2 + buf]));
+        }
+    }
+    fence_before();
+    __syncthreads();
+    if (warp == 1) {
+        fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                     "r"(TMEM_COLS)
+                     : "memory");
+    }
+}
+
 // Pack a column-major planar complex A (M x K) into K-major TF32 tiles:
 // out[b][plane][Mp][Kp], zero outside M x K, round to nearest TF32.
 __global__ void pack_a_tf32_kernel(const float *__restrict__ A, int64_t lda, int64_t planeA,
@@ -389,6 +601,19 @@ static int make_map(CUtensorMap *map, const float *base, uint64_t d0, uint64_t d
     return MNPB_OK;
 }
 
+static int num_sms() {
+    static int n = 0;
+    if (n == 0) {
+        int dev = 0, v = 0;
+        if (cudaGetDevice(&dev) == cudaSuccess &&
+            cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess && v > 0)
+            n = v;
+        else
+            n = 148;
+    }
+    return n;
+}
+
 int64_t cgemm_tf32_workspace(int M, int K, int batch) {
     const int64_t Mp = (M + BM - 1) / BM * BM, Kp = (K + BK - 1) / BK * BK;
     return (int64_t)batch * 2 * Mp * Kp * 4;
@@ -419,7 +644,28 @@ static int launch_tf32(cudaStream_t s, const CUtensorMap &mA, const CMatF &B, in
     int dyn = TL::smem_bytes(nst);
     const int floor_bytes = (228 * 1024) / (max_ctas_tmem + 1) + 1024;
     if (dyn < floor_bytes) dyn = floor_bytes;
-    dim3 grid(Mp / BM, (N + BN - 1) / BN, batch);
+    const int MT = Mp / BM, NT = (N + BN - 1) / BN;
+    const int64_t ntiles = (int64_t)MT * NT * batch;
+    if (BN == 128 && ntiles >= 2 * num_sms()) {
+        // persistent: one CTA per SM, double-buffered accumulators
+        static bool pattr = false;
+        if (!pattr) {
+            if (cudaFuncSetAttribute(cgemm_tf32_persistent<BN>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     TL::smem_bytes(TL::MAX_ST)) != cudaSuccess) {
+                set_error("tc_gemm: cannot set shared memory size (persistent)");
+                return MNPB_ECUDA;
+            }
+            pattr = true;
+        }
+        const int pst = TL::MAX_ST;
+        const int grid = (int)(ntiles < num_sms() ? ntiles : num_sms());
+        cgemm_tf32_persistent<BN><<<grid, 192, TL::smem_bytes(pst), s>>>(mA, mBr, mBi, ep, pst, MT,
+                                                                        NT, (int)ntiles);
+        MNPB_LAUNCH_CHECK("cgemm_tf32_persistent");
+        return MNPB_OK;
+    }
+    dim3 grid(MT, NT, batch);
     cgemm_tf32_kernel<BN><<<grid, 128, dyn, s>>>(mA, mBr, mBi, ep, nst);
     MNPB_LAUNCH_CHECK("cgemm_tf32_kernel");
     return MNPB_OK;
