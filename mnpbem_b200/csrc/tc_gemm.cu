@@ -646,6 +646,7 @@ static int launch_tf32(cudaStream_t s, const CUtensorMap &mA, const CMatF &B, in
     if (dyn < floor_bytes) dyn = floor_bytes;
     const int MT = Mp / BM, NT = (N + BN - 1) / BN;
     const int64_t ntiles = (int64_t)MT * NT * batch;
+    // (narrower tiles already overlap epilogues across several CTAs per SM)
     if (BN == 128 && ntiles >= 2 * num_sms()) {
         // persistent: one CTA per SM, double-buffered accumulators
         static bool pattr = false;

@@ -26,7 +26,8 @@ def _cplx(P, rows, cols):
     (128, 128, 32, 1, 1.0, 0.0), (256, 256, 256, 2, 1.0, 0.0), (200, 100, 50, 3, -1.0, 1.0),
     (37, 300, 130, 1, -1.0, 1.0), (384, 64, 1000, 2, 1.0, 1.0),
     # enough 128 x 128 tiles (>= 2 per SM) for the persistent kernel; ragged M, N
-    (1000, 400, 300, 16, -1.0, 1.0), (777, 260, 96, 16, 1.0, 0.0)])
+    (1000, 400, 300, 16, -1.0, 1.0), (777, 260, 96, 16, 1.0, 0.0),
+    (2000, 32, 64, 24, -1.0, 1.0), (1500, 60, 200, 30, 1.0, 1.0)])
 def test_cgemm_tf32(gpu_ok, m, n, k, batch, alpha, beta):
     lda, ldb, ldc = (m + 3) // 4 * 4, (k + 3) // 4 * 4, (m + 3) // 4 * 4
     A = _planar(batch, m, k, lda, 1)
