@@ -342,6 +342,10 @@ __global__ void __launch_bounds__(128) trsm_small_kernel(int mode, int kb, const
                                       : fmk(r == c ? 1.f : 0.f, 0.f);
     }
     __syncthreads();
+    // non-unit modes: keep 1 / diagonal on the diagonal, so that no thread's
+    // substitution chain contains a division
+    if ((mode == 1 || mode == 2) && threadIdx.x < TS) Ts[threadIdx.x][threadIdx.x] = frcp(Ts[threadIdx.x][threadIdx.x]);
+    __syncthreads();
     const int v = blockIdx.x * blockDim.x + threadIdx.x;
     if (v >= nvec) return;
     cf x[TS];
@@ -360,14 +364,14 @@ __global__ void __launch_bounds__(128) trsm_small_kernel(int mode, int kb, const
         for (int r = TS - 1; r >= 0; --r) {
 #pragma unroll
             for (int c = r + 1; c < TS; ++c) x[r] = ffms(Ts[r][c], x[c], x[r]);
-            x[r] = fmul(x[r], frcp(Ts[r][r]));
+            x[r] = fmul(x[r], Ts[r][r]);
         }
     } else if (mode == 2) {
 #pragma unroll
         for (int c = 0; c < TS; ++c) {
 #pragma unroll
             for (int r = 0; r < c; ++r) x[c] = ffms(x[r], Ts[r][c], x[c]);
-            x[c] = fmul(x[c], frcp(Ts[c][c]));
+            x[c] = fmul(x[c], Ts[c][c]);
         }
     } else {
 #pragma unroll
