@@ -227,10 +227,12 @@ int64_t mnpb_bemret_refine_workspace(int64_t n, int64_t batch, int64_t nrhs);
 
 /* Solve with the mixed factorisation and refine in FP64 against the exact
  * operator of mnpbem/bem/bem_ret_iter.py:1362-1501 (c128 G1, G2, H1, H2 with
- * the same ld): x = M^-1 b, then x += M^-1 (b - A x) until |b - A x| / |b| <
- * tol or max_iter corrections (MNPB_ENOCONV then).  b: excitation layout
- * (phi, a, De, alpha), x: solution layout (sig1, h1, sig2, h2), both
- * [batch][8][nrhs][n] c128, nrhs <= 4.  iters, relres: host arrays (batch). */
+ * the same ld): x = M^-1 b, then dx = M^-1 (b - A x), x += dx, per batch
+ * entry until |dx| / |x| < tol (a forward-error test) or max_iter
+ * corrections (MNPB_ENOCONV then).  b: excitation layout (phi, a, De,
+ * alpha), x: solution layout (sig1, h1, sig2, h2), both [batch][8][nrhs][n]
+ * c128, nrhs <= 4.  iters (corrections applied) and relres (final
+ * |b - A x| / |b|): host arrays (batch). */
 int mnpb_bemret_solve_refine(void *stream, int64_t n, int64_t batch, int64_t nrhs,
                              const float *G1p, const float *G2p, const float *S1p,
                              const float *Sp, const float *Dp, int64_t ld, const int32_t *piv,

@@ -100,11 +100,12 @@ class _MixedBatch(object):
 class BEMRet(object):
     """Retarded BEM solver (full Maxwell equations), dense, on the GPU."""
 
-    def __init__(self, p, enei=None, precision='fp64', refine_tol=1e-11, refine_maxit=12,
+    def __init__(self, p, enei=None, precision='fp64', refine_tol=1e-11, refine_maxit=20,
                  **options):
         """``precision``: 'fp64' (the reference's arithmetic) or 'mixed' (FP32
         storage, TF32 tensor-core factorisations, FP64 iterative refinement
-        of the solution to ``refine_tol`` relative residual)."""
+        of every wavelength's solution until its last correction is below
+        ``refine_tol`` relative to the solution)."""
         _check_particle(p, 'BEMRet')
         if precision not in ('fp64', 'mixed'):
             raise ValueError("BEMRet: precision must be 'fp64' or 'mixed'")

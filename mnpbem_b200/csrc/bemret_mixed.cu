@@ -216,9 +216,30 @@ __global__ void axpy_kernel(int64_t len, const cd *d, cd *x) {
 struct Factors {
     float *G1, *G2, *S1, *S, *D;
     int64_t ld, plane, stride;
-    const int32_t *piv;   // [3][batch][n]: G1, G2, Sigma
-    const float *dinv;    // diagonal-block inverses, see dinv_offsets
+    const int32_t *pivG1, *pivG2, *pivS;            // n per batch entry
+    const float *iG1L, *iG1U, *iG2L, *iG2U, *iSL, *iSU;   // diagonal-block inverses
+    int64_t n, dinv_per;                            // dinv_per: floats per entry
     int *trsv_state;      // flags + ticket of the one-launch triangular solves
+    // the same factors for batch entries b0, b0 + 1, ...
+    Factors at(int b0) const {
+        Factors f = *this;
+        const int64_t o = (int64_t)b0 * stride, op = (int64_t)b0 * n, oi = (int64_t)b0 * dinv_per;
+        f.G1 += o;
+        f.G2 += o;
+        f.S1 += o;
+        f.S += o;
+        f.D += o;
+        f.pivG1 += op;
+        f.pivG2 += op;
+        f.pivS += op;
+        f.iG1L += oi;
+        f.iG1U += oi;
+        f.iG2L += oi;
+        f.iG2U += oi;
+        f.iSL += oi;
+        f.iSU += oi;
+        return f;
+    }
 };
 
 // Offsets (floats) into the diagonal-block-inverse buffer: G1/G2 unit-lower
@@ -282,7 +303,6 @@ static int msolve(f32::Ctx &c, int n, int K, const Factors &F, const double *eps
     cd *R = V + (int64_t)B * nn * 3 * K;
     float *t1 = fscr, *t2 = fscr + (int64_t)B * nn * 16 * K;
     const int64_t sT = nn * 4 * K, sAP = nn * 3 * K, sR = nn * K, sx = nn * 8 * K;
-    const int32_t *piv = F.piv;
     dim3 g(ceil_div(n, 128), B);
     solve_prep_kernel<<<g, 128, 0, s>>>(n, K, xin, sx, T, sT, eps, kvac);
     MNPB_LAUNCH_CHECK("solve_prep_kernel");
@@ -292,18 +312,14 @@ static int msolve(f32::Ctx &c, int n, int K, const Factors &F, const double *eps
     MNPB_TRY(mgemm(c, n, 3 * K, F.D, F, AP, sAP, V, sAP, t1, t2));
     solve_rhs_kernel<<<g, 128, 0, s>>>(n, K, V, sAP, R, sR, eps, kvac, nvec);
     MNPB_LAUNCH_CHECK("solve_rhs_kernel");
-    const DinvOff dv{f32::diag_inv_floats(n, 1)};
-    MNPB_TRY(mgetrs(c, n, K, F.S, F, piv + 2 * (int64_t)B * nn, F.dinv + dv.sL(B),
-                    F.dinv + dv.sU(B), R, sR, t1));
+    MNPB_TRY(mgetrs(c, n, K, F.S, F, F.pivS, F.iSL, F.iSU, R, sR, t1));
     solve_h2pre_kernel<<<g, 128, 0, s>>>(n, K, AP, sAP, R, sR, eps, kvac, nvec);
     MNPB_LAUNCH_CHECK("solve_h2pre_kernel");
     MNPB_TRY(mgemm(c, n, 3 * K, F.D, F, AP, sAP, V, sAP, t1, t2));
     solve_out_kernel<<<g, 128, 0, s>>>(n, K, xin, sx, R, sR, V, sAP, xout, sx);
     MNPB_LAUNCH_CHECK("solve_out_kernel");
-    MNPB_TRY(mgetrs(c, n, 4 * K, F.G1, F, piv, F.dinv + dv.gL(0, B), F.dinv + dv.gU(0, B), xout,
-                    sx, t1));
-    return mgetrs(c, n, 4 * K, F.G2, F, piv + (int64_t)B * nn, F.dinv + dv.gL(1, B),
-                  F.dinv + dv.gU(1, B), xout + 4 * K * nn, sx, t1);
+    MNPB_TRY(mgetrs(c, n, 4 * K, F.G1, F, F.pivG1, F.iG1L, F.iG1U, xout, sx, t1));
+    return mgetrs(c, n, 4 * K, F.G2, F, F.pivG2, F.iG2L, F.iG2U, xout + 4 * K * nn, sx, t1);
 }
 
 }  // namespace mixed
@@ -412,8 +428,12 @@ extern "C" int mnpb_bemret_solve_refine(
     cudaStream_t s = as_stream(stream);
     const int N = (int)n, B = (int)batch, k = (int)K;
     const int64_t plane = ld * n;
+    const DinvOff dv{f32::diag_inv_floats(n, 1)};
+    const int64_t Bn = batch * n;
     Factors F{(float *)G1p, (float *)G2p, (float *)S1p, (float *)Sp, (float *)Dp, ld, plane,
-              2 * plane, piv, dinv, nullptr};
+              2 * plane, piv, piv + Bn, piv + 2 * Bn, dinv + dv.gL(0, batch),
+              dinv + dv.gU(0, batch), dinv + dv.gL(1, batch), dinv + dv.gU(1, batch),
+              dinv + dv.sL(batch), dinv + dv.sU(batch), n, dv.S, nullptr};
     const int64_t per = n * K;
     char *wp = (char *)work;
     auto take = [&](int64_t bytes) {
@@ -439,54 +459,88 @@ extern "C" int mnpb_bemret_solve_refine(
     std::vector<double> hn(2 * batch);
     std::vector<int> done(batch, 0);
     for (int b = 0; b < B; ++b) iters[b] = 0;
-    for (int it = 0; it <= max_iter; ++it) {
-        dim3 gz(ceil_div(n, 128), B);
-        dim3 gzs(ceil_div(n, ZS_ROWS), B);
-        const int64_t sG = ld * n;   // c128 matrices use the same leading dimension
-        {
-            ProfScope ps(s, PC_MATVEC, 4.0 * 16.0 * (double)n * n * batch);   // bytes of A read
-            const cd *mats[4] = {(const cd *)G1, (const cd *)G2, (const cd *)H1, (const cd *)H2};
-            const cd *xs[4] = {xx, xx + 4 * per, xx, xx + 4 * per};
-            cd *ys[4] = {P1, P2, Q1, Q2};
-            for (int q = 0; q < 4; ++q) {
-                // at most 8 columns per launch (shared-memory bound of the lane reduction)
-                for (int c0 = 0; c0 < 4 * k; c0 += 8) {
-                    const int mc = min(8, 4 * k - c0);
-                    const cd *xq = xs[q] + (int64_t)c0 * N;
-                    cd *yq = ys[q] + (int64_t)c0 * N;
-                    if (mc <= 4)
-                        zskinny_kernel<4><<<gzs, 256, 0, s>>>(N, mc, mats[q], ld, sG, xq, sx, yq, sP4);
-                    else
-                        zskinny_kernel<8><<<gzs, 256, 0, s>>>(N, mc, mats[q], ld, sG, xq, sx, yq, sP4);
-                }
+    const int64_t sG = ld * n;   // c128 matrices use the same leading dimension
+    // r = b - A x on entries [e0, B) (residual vectors at r + e0 * sx)
+    auto residual = [&](int e0) -> int {
+        const int Bp = B - e0;
+        dim3 gz(ceil_div(n, 128), Bp);
+        dim3 gzs(ceil_div(n, ZS_ROWS), Bp);
+        const cd *xa = xx + (int64_t)e0 * sx;
+        ProfScope ps(s, PC_MATVEC, 4.0 * 16.0 * (double)n * n * Bp);   // bytes of A read
+        const int64_t om = (int64_t)e0 * sG;
+        const cd *mats[4] = {(const cd *)G1 + om, (const cd *)G2 + om, (const cd *)H1 + om,
+                             (const cd *)H2 + om};
+        const cd *xs[4] = {xa, xa + 4 * per, xa, xa + 4 * per};
+        cd *ys[4] = {P1, P2, Q1, Q2};
+        for (int q = 0; q < 4; ++q) {
+            // at most 8 columns per launch (shared-memory bound of the lane reduction)
+            for (int c0 = 0; c0 < 4 * k; c0 += 8) {
+                const int mc = min(8, 4 * k - c0);
+                const cd *xq = xs[q] + (int64_t)c0 * N;
+                cd *yq = ys[q] + (int64_t)c0 * N;
+                if (mc <= 4)
+                    zskinny_kernel<4><<<gzs, 256, 0, s>>>(N, mc, mats[q], ld, sG, xq, sx, yq, sP4);
+                else
+                    zskinny_kernel<8><<<gzs, 256, 0, s>>>(N, mc, mats[q], ld, sG, xq, sx, yq, sP4);
             }
-            count_launch(3);
-            MNPB_LAUNCH_CHECK("zskinny_kernel");
         }
-        residual_kernel<<<gz, 128, 0, s>>>(N, k, P1, P2, Q1, Q2, sP4, bb, r, sx, eps, kvac, nvec);
+        count_launch(3);
+        MNPB_LAUNCH_CHECK("zskinny_kernel");
+        residual_kernel<<<gz, 128, 0, s>>>(N, k, P1, P2, Q1, Q2, sP4, bb + (int64_t)e0 * sx,
+                                           r + (int64_t)e0 * sx, sx, eps + 4 * (int64_t)e0,
+                                           kvac + e0, nvec);
         MNPB_LAUNCH_CHECK("residual_kernel");
-        norms_kernel<<<B, 256, 0, s>>>(sx, r, bb, sx, nrm);
+        return MNPB_OK;
+    };
+    // per entry of [e0, B): |u|^2 and |v|^2 to the host (hn[2 i], hn[2 i + 1])
+    auto norms = [&](int e0, const cd *u, const cd *v) -> int {
+        const int Bp = B - e0;
+        norms_kernel<<<Bp, 256, 0, s>>>(sx, u + (int64_t)e0 * sx, v + (int64_t)e0 * sx, sx, nrm);
         MNPB_LAUNCH_CHECK("norms_kernel");
-        if (cudaMemcpyAsync(hn.data(), nrm, sizeof(double) * 2 * batch, cudaMemcpyDeviceToHost,
-                            s) != cudaSuccess ||
+        if (cudaMemcpyAsync(hn.data(), nrm, sizeof(double) * 2 * Bp, cudaMemcpyDeviceToHost, s) !=
+                cudaSuccess ||
             cudaStreamSynchronize(s) != cudaSuccess) {
-            set_error("bemret_solve_refine: residual norm copy failed");
+            set_error("bemret_solve_refine: norm copy failed");
             return MNPB_ECUDA;
         }
-        bool all = true;
-        for (int b = 0; b < B; ++b) {
-            const double rel = hn[2 * b + 1] > 0 ? std::sqrt(hn[2 * b] / hn[2 * b + 1]) : 0.0;
-            relres[b] = rel;
-            if (!done[b] && rel < tol) done[b] = 1;
+        return MNPB_OK;
+    };
+    // Classical iterative refinement: r = b - A x (FP64), dx = M^-1 r (mixed),
+    // x += dx; an entry is finished when its last correction is below tol
+    // relative to the solution (a forward-error test: the residual alone
+    // under-states the error of ill-conditioned entries).  Entries finish at
+    // different rates; each pass works on [b0, B), b0 = the first entry not
+    // finished (the batch is a wavelength sweep whose slow entries gather at
+    // one end), through offset pointers.
+    int b0 = 0;
+    bool all = false;
+    for (int it = 0; it < max_iter && !all; ++it) {
+        const int Bp = B - b0;
+        MNPB_TRY(residual(b0));
+        f32::Ctx ca(s, Bp, (float *)wp, tcw);
+        MNPB_TRY(msolve(ca, N, k, F.at(b0), eps + 4 * (int64_t)b0, kvac + b0, nvec,
+                        r + (int64_t)b0 * sx, dx + (int64_t)b0 * sx, scr, fscr));
+        axpy_kernel<<<ceil_div((int64_t)Bp * sx, 256), 256, 0, s>>>((int64_t)Bp * sx,
+                                                                    dx + (int64_t)b0 * sx,
+                                                                    xx + (int64_t)b0 * sx);
+        MNPB_LAUNCH_CHECK("axpy_kernel");
+        MNPB_TRY(norms(b0, dx, xx));
+        all = true;
+        for (int i = 0; i < Bp; ++i) {
+            const int b = b0 + i;
+            if (done[b]) continue;
+            iters[b] = it + 1;
+            const double rel = hn[2 * i + 1] > 0 ? std::sqrt(hn[2 * i] / hn[2 * i + 1]) : 0.0;
+            if (rel < tol) done[b] = 1;
             if (!done[b]) all = false;
         }
-        if (all || it == max_iter) break;
-        MNPB_TRY(msolve(c, N, k, F, eps, kvac, nvec, r, dx, scr, fscr));
-        axpy_kernel<<<ceil_div(B * sx, 256), 256, 0, s>>>(B * sx, dx, xx);
-        MNPB_LAUNCH_CHECK("axpy_kernel");
-        for (int b = 0; b < B; ++b)
-            if (!done[b]) iters[b] = it + 1;
+        while (b0 < B && done[b0]) ++b0;
     }
+    // final relative residuals of every entry
+    MNPB_TRY(residual(0));
+    MNPB_TRY(norms(0, r, bb));
+    for (int b = 0; b < B; ++b)
+        relres[b] = hn[2 * b + 1] > 0 ? std::sqrt(hn[2 * b] / hn[2 * b + 1]) : 0.0;
     int terr = 0;
     MNPB_TRY(f32::trsv_error_read_and_clear(s, &terr));
     if (terr) {
@@ -495,9 +549,9 @@ extern "C" int mnpb_bemret_solve_refine(
     }
     for (int b = 0; b < B; ++b)
         if (!done[b]) {
-            set_error("bemret_solve_refine: batch entry %d stopped at relative residual %.3e "
-                      "(tolerance %.1e) after %d corrections",
-                      b, relres[b], tol, max_iter);
+            set_error("bemret_solve_refine: batch entry %d: the last of %d corrections was "
+                      "still above the tolerance %.1e (relative residual %.3e)",
+                      b, max_iter, tol, relres[b]);
             return MNPB_ENOCONV;
         }
     return MNPB_OK;
