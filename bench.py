@@ -458,10 +458,15 @@ def main():
         elif name in ('tc_gemm',):
             achieved = work / (dms / 1000.0) / 1e12
             peak = peaks['bf16_tflops_sustained']
+            # DRAM bytes of one representative launch from an ncu capture
+            # (ncu --set full -k regex:cgemm_tf32_persistent ... bench.py --probe tc_gemm)
             roof = {"kernel": name, "bound": "tensor", "achieved": achieved, "peak": peak,
-                    "unit": "TFLOP/s", "frac": achieved / peak, "traffic": None,
-                    "peak_source": peak_kind + " bf16 sustained", "launches": cnt,
-                    "share": dms / tot_ms}
+                    "unit": "TFLOP/s", "frac": achieved / peak, "traffic": 551.5e6,
+                    "traffic_launch": "cgemm_tf32_persistent<128>, M=2884 N=1440 K=1444 "
+                                      "batch 4 (algorithmic 466e6 B)",
+                    "peak_source": peak_kind + " bf16 sustained",
+                    "frac_of_tf32_ceiling": achieved / (peak / 2.0),
+                    "launches": cnt, "share": dms / tot_ms}
         else:
             achieved = work / (dms / 1000.0) / 1e9
             peak = peaks['hbm_gbs']
