@@ -243,7 +243,11 @@ int mnpb_bemret_solve_refine(void *stream, int64_t n, int64_t batch, int64_t nrh
                              int64_t work_bytes);
 
 /* Batched LU / LU solve of planar FP32 matrices with TF32 tensor-core
- * updates (recursive LU).  work: mnpb_f32_workspace(n, batch) bytes. */
+ * updates (recursive LU; triangular solves with >= 128 right-hand sides apply
+ * the 128 x 128 diagonal blocks through their inverses, also on the tensor
+ * cores).  Leading dimensions, planes and strides are multiples of 4 floats
+ * and base pointers 16-byte aligned (tensor-core operand rule).
+ * work: mnpb_f32_workspace(n, batch) bytes. */
 int64_t mnpb_f32_workspace(int64_t n, int64_t batch);
 int mnpb_getrf_c32p(void *stream, int64_t n, int64_t batch, float *A, int64_t ld, int64_t plane,
                     int64_t stride, int32_t *piv, int64_t pstride, int32_t *info, void *work,

@@ -4,7 +4,8 @@
 // LU is recursive (split the columns in halves; factor the left half; update
 // the right half with a triangular solve and a GEMM; factor the rest), so
 // nearly all flops land in large GEMMs that run on the tensor cores
-// (tc::cgemm_tf32); only the 32-column leaves run on CUDA cores.
+// (tc::cgemm_tf32); only the 32-column LU leaves, the 128 x 128 diagonal-block
+// inverses and the 32-row leaves of small triangular solves run on CUDA cores.
 #include "common.cuh"
 #include "dense_f32.cuh"
 
@@ -384,6 +385,108 @@ __global__ void __launch_bounds__(128) trsm_small_kernel(int mode, int kb, const
         if (e < kb) st(B, planeB, left ? (int64_t)v * ldb + e : (int64_t)e * ldb + v, x[e]);
 }
 
+// Inverses of the 128 x 128 diagonal blocks of a unit-lower (lower = 1) or
+// non-unit upper (lower = 0) triangle, one CTA per (block, matrix); the last
+// block may be short (kb < 128) and is padded with the identity.  The block
+// sits in shared memory column-major (k-th column contiguous), one warp
+// builds one column j of the inverse by column-oriented substitution
+// (T x = e_j): rows 32r + lane live in the lane's registers x[r], the newly
+// final entry x_k is broadcast by a shuffle and subtracted, times column k
+// of T, from the rows it feeds.  Output: out[b][blk][2][128][128] (planar,
+// column-major, leading dimension 128).
+constexpr int TL = 128;
+constexpr int TINV_THREADS = 512;
+
+__device__ __forceinline__ float tf32_rna(float v) {
+    uint32_t t;
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(t) : "f"(v));
+    return __uint_as_float(t);
+}
+
+__global__ void __launch_bounds__(TINV_THREADS) tri_inv_kernel(int n, int lower, const float *A,
+                                                               int64_t lda, int64_t plane,
+                                                               int64_t sA, float *out, int nb) {
+    extern __shared__ __align__(16) unsigned char tinv_smem[];
+    cf *Tc = reinterpret_cast<cf *>(tinv_smem);   // Tc[k * TL + i] = T(i, k)
+    __shared__ cf dinv[TL];
+    const int blk = blockIdx.x;
+    const int64_t b = blockIdx.y;
+    const int o = blk * TL, kb = min(TL, n - o);
+    A += b * sA;
+    for (int e = threadIdx.x; e < TL * TL; e += TINV_THREADS) {
+        const int i = e % TL, k = e / TL;
+        cf v = fmk(0.f, 0.f);
+        if (i < kb && k < kb) {
+            if (lower ? (i > k) : (i <= k)) v = ld(A, plane, (int64_t)(o + k) * lda + o + i);
+        } else if (i == k) {
+            v = fmk(1.f, 0.f);
+        }
+        Tc[e] = v;
+    }
+    __syncthreads();
+    if (!lower && threadIdx.x < TL) {
+        const cf d = Tc[threadIdx.x * TL + threadIdx.x];
+        dinv[threadIdx.x] = (d.x != 0.f || d.y != 0.f) ? frcp(d) : fmk(0.f, 0.f);
+    }
+    __syncthreads();
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    float *ob = out + ((b * nb + blk) * 2) * TL * TL;
+    for (int j = w; j < TL; j += TINV_THREADS / 32) {
+        cf x[4];
+#pragma unroll
+        for (int r = 0; r < 4; ++r) x[r] = fmk(32 * r + lane == j ? 1.f : 0.f, 0.f);
+        if (lower) {
+#pragma unroll
+            for (int r = 0; r < 4; ++r) {
+                if (32 * r + 31 < j) continue;
+                for (int kk = (32 * r < j ? j - 32 * r : 0); kk < 32; ++kk) {
+                    const int k = 32 * r + kk;
+                    const cf xk = fmk(__shfl_sync(0xffffffffu, x[r].x, kk),
+                                      __shfl_sync(0xffffffffu, x[r].y, kk));
+                    const cf *tk = Tc + k * TL + lane;
+#pragma unroll
+                    for (int r2 = r; r2 < 4; ++r2)
+                        if (r2 > r || lane > kk) x[r2] = ffms(tk[32 * r2], xk, x[r2]);
+                }
+            }
+        } else {
+#pragma unroll
+            for (int r = 3; r >= 0; --r) {
+                if (32 * r > j) continue;
+                for (int kk = min(31, j - 32 * r); kk >= 0; --kk) {
+                    const int k = 32 * r + kk;
+                    const cf xk = fmul(fmk(__shfl_sync(0xffffffffu, x[r].x, kk),
+                                           __shfl_sync(0xffffffffu, x[r].y, kk)),
+                                       dinv[k]);
+                    if (lane == kk) x[r] = xk;
+                    const cf *tk = Tc + k * TL + lane;
+#pragma unroll
+                    for (int r2 = 0; r2 <= r; ++r2)
+                        if (r2 < r || lane < kk) x[r2] = ffms(tk[32 * r2], xk, x[r2]);
+                }
+            }
+        }
+        // stored rounded to nearest TF32, the precision the leaf GEMM reads
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+            ob[j * TL + 32 * r + lane] = tf32_rna(x[r].x);
+            ob[TL * TL + j * TL + 32 * r + lane] = tf32_rna(x[r].y);
+        }
+    }
+}
+
+// Round rows [0, rows) of every column of a planar block to nearest TF32 in
+// place: the right-hand sides of a left leaf, read by the tensor cores as the
+// B operand (which would otherwise drop the low mantissa bits, a bias towards
+// zero) and overwritten by the leaf's result right after.
+__global__ void round_tf32_kernel(float *B, int64_t ldb, int64_t plane, int64_t sB, int rows) {
+    const int i = threadIdx.x;
+    if (i >= rows) return;
+    float *p = B + blockIdx.y * sB + (int64_t)blockIdx.x * ldb + i;
+    p[0] = tf32_rna(p[0]);
+    p[plane] = tf32_rna(p[plane]);
+}
+
 // Skinny GEMM C = alpha A B + beta C for at most NC (<= 16) columns (matrix
 // times a few vectors): one thread per row, A streamed once with coalesced
 // column reads, B broadcast from shared memory.  Real alpha, beta.
@@ -707,37 +810,109 @@ static int split_point(int n) {
     return h < TS ? TS : h;
 }
 
-int trsm_llu(Ctx &c, int n, int m, CMatF L, CMatF B) {
-    if (n <= TS) return trsm_small(c, 0, n, L, B, m);
-    const int n1 = split_point(n);
-    MNPB_TRY(trsm_llu(c, n1, m, L, B));
-    MNPB_TRY(gemm(c, n - n1, m, n1, -1.f, L.sub(n1, 0), B, 1.f, B.sub(n1, 0)));
-    return trsm_llu(c, n - n1, m, L.sub(n1, n1), B.sub(n1, 0));
+// Triangular solves with many right-hand sides, recursive: split the
+// triangle, solve one half, update the other half's right-hand sides with a
+// tensor-core GEMM, solve the other half.  Two leaf kinds:
+//  * 32-row leaves on CUDA cores (trsm_small) with splits at multiples of 32;
+//  * when there are at least TL right-hand sides and the workspace holds
+//    the inverses of the triangle's 128 x 128 diagonal blocks, 128-row
+//    leaves applied as one tensor-core GEMM with the block's inverse (splits
+//    at multiples of 128).  The leaf GEMM overwrites its own right-hand
+//    sides: for a left solve (inverse as A, the RHS rows as B, C = B) each
+//    output tile is a single 128-row tile whose columns no other tile reads,
+//    and its epilogue runs after all of its loads; for a right solve the RHS
+//    block is A and is copied into the packed operand before the GEMM.
+//  mode 0 left lower unit, 1 left upper non-unit, 2 right upper non-unit,
+//  3 right lower unit.
+struct InvSet {
+    const float *p;   // tri_inv_kernel output of the whole triangle
+    int nb;           // 128-blocks of that triangle
+};
+
+static CMatF inv_block(const InvSet &iv, int blk) {
+    return CMatF{(float *)iv.p + (int64_t)blk * 2 * TL * TL, TL, (int64_t)TL * TL,
+                 (int64_t)iv.nb * 2 * TL * TL};
 }
 
-int trsm_lun(Ctx &c, int n, int m, CMatF U, CMatF B) {
-    if (n <= TS) return trsm_small(c, 1, n, U, B, m);
-    const int n1 = split_point(n);
-    MNPB_TRY(trsm_lun(c, n - n1, m, U.sub(n1, n1), B.sub(n1, 0)));
-    MNPB_TRY(gemm(c, n1, m, n - n1, -1.f, U.sub(0, n1), B.sub(n1, 0), 1.f, B));
-    return trsm_lun(c, n1, m, U, B);
+static int split_tl(int n) {
+    int h = n / 2;
+    h = (h / TL) * TL;
+    return h < TL ? TL : h;
 }
 
-int trsm_run(Ctx &c, int n, int m, CMatF U, CMatF B) {
-    if (n <= TS) return trsm_small(c, 2, n, U, B, m);
-    const int n1 = split_point(n);
-    MNPB_TRY(trsm_run(c, n1, m, U, B));
-    MNPB_TRY(gemm(c, m, n - n1, n1, -1.f, B, U.sub(0, n1), 1.f, B.sub(0, n1)));
-    return trsm_run(c, n - n1, m, U.sub(n1, n1), B.sub(0, n1));
+static int trsm_rec(Ctx &c, int mode, int n, int m, CMatF T, CMatF B, const InvSet *iv,
+                    int blk0) {
+    if (!iv && n <= TS) return trsm_small(c, mode, n, T, B, m);
+    if (iv && n <= TL) {
+        const CMatF I = inv_block(*iv, blk0);
+        if (mode >= 2) return gemm(c, m, n, n, 1.f, B, I, 0.f, B);
+        round_tf32_kernel<<<dim3(m, c.batch), TL, 0, c.s>>>(B.p, B.ld, B.plane, B.stride, n);
+        MNPB_LAUNCH_CHECK("round_tf32_kernel");
+        return gemm(c, n, m, n, 1.f, I, B, 0.f, B);
+    }
+    const int n1 = iv ? split_tl(n) : split_point(n);
+    const int blk1 = blk0 + n1 / TL;
+    switch (mode) {
+    case 0:
+        MNPB_TRY(trsm_rec(c, 0, n1, m, T, B, iv, blk0));
+        MNPB_TRY(gemm(c, n - n1, m, n1, -1.f, T.sub(n1, 0), B, 1.f, B.sub(n1, 0)));
+        return trsm_rec(c, 0, n - n1, m, T.sub(n1, n1), B.sub(n1, 0), iv, blk1);
+    case 1:
+        MNPB_TRY(trsm_rec(c, 1, n - n1, m, T.sub(n1, n1), B.sub(n1, 0), iv, blk1));
+        MNPB_TRY(gemm(c, n1, m, n - n1, -1.f, T.sub(0, n1), B.sub(n1, 0), 1.f, B));
+        return trsm_rec(c, 1, n1, m, T, B, iv, blk0);
+    case 2:
+        MNPB_TRY(trsm_rec(c, 2, n1, m, T, B, iv, blk0));
+        MNPB_TRY(gemm(c, m, n - n1, n1, -1.f, B, T.sub(0, n1), 1.f, B.sub(0, n1)));
+        return trsm_rec(c, 2, n - n1, m, T.sub(n1, n1), B.sub(0, n1), iv, blk1);
+    default:
+        MNPB_TRY(trsm_rec(c, 3, n - n1, m, T.sub(n1, n1), B.sub(0, n1), iv, blk1));
+        MNPB_TRY(gemm(c, m, n1, n - n1, -1.f, B.sub(0, n1), T.sub(n1, 0), 1.f, B));
+        return trsm_rec(c, 3, n1, m, T, B, iv, blk0);
+    }
 }
 
-int trsm_rlu(Ctx &c, int n, int m, CMatF L, CMatF B) {
-    if (n <= TS) return trsm_small(c, 3, n, L, B, m);
-    const int n1 = split_point(n);
-    MNPB_TRY(trsm_rlu(c, n - n1, m, L.sub(n1, n1), B.sub(0, n1)));
-    MNPB_TRY(gemm(c, m, n1, n - n1, -1.f, B.sub(0, n1), L.sub(n1, 0), 1.f, B));
-    return trsm_rlu(c, n1, m, L, B);
+// Packed-operand bytes of the largest GEMM trsm_rec issues with 128-leaves.
+static int64_t trsm_pack_bytes(int mode, int n, int m, int batch) {
+    const int big = n - split_tl(n) > TL ? n - split_tl(n) : TL;
+    return mode < 2 ? tc::cgemm_tf32_workspace(big, big, batch)
+                    : tc::cgemm_tf32_workspace(m, big, batch);
 }
+
+static int trsm(Ctx &c, int mode, int n, int m, CMatF T, CMatF B) {
+    if (n <= 0 || m <= 0) return MNPB_OK;
+    const int nb = ceil_div(n, TL);
+    const int64_t inv_bytes = ((int64_t)c.batch * nb * 2 * TL * TL * 4 + 255) / 256 * 256;
+    const int64_t keep = (c.work_bytes - inv_bytes) / 256 * 256;
+    if (n <= TS || m < TL || keep < trsm_pack_bytes(mode, n, m, c.batch))
+        return trsm_rec(c, mode, n, m, T, B, nullptr, 0);
+    static bool attr = false;
+    if (!attr) {
+        if (cudaFuncSetAttribute(tri_inv_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 TL * TL * (int)sizeof(cf)) != cudaSuccess) {
+            set_error("tri_inv_kernel: cannot reserve shared memory");
+            return MNPB_ECUDA;
+        }
+        attr = true;
+    }
+    float *inv = (float *)((char *)c.work + keep);
+    {
+        dim3 grid(nb, c.batch);
+        ProfScope ps(c.s, PC_TRSM, 8.0 * TL * TL * TL / 3.0 * nb * c.batch);
+        prof_tag("tri_inv n=%d B=%d %s", n, c.batch, (mode == 0 || mode == 3) ? "L" : "U");
+        tri_inv_kernel<<<grid, TINV_THREADS, TL * TL * sizeof(cf), c.s>>>(
+            n, (mode == 0 || mode == 3) ? 1 : 0, T.p, T.ld, T.plane, T.stride, inv, nb);
+        MNPB_LAUNCH_CHECK("tri_inv_kernel");
+    }
+    Ctx c2(c.s, c.batch, c.work, keep);
+    const InvSet iv{inv, nb};
+    return trsm_rec(c2, mode, n, m, T, B, &iv, 0);
+}
+
+int trsm_llu(Ctx &c, int n, int m, CMatF L, CMatF B) { return trsm(c, 0, n, m, L, B); }
+int trsm_lun(Ctx &c, int n, int m, CMatF U, CMatF B) { return trsm(c, 1, n, m, U, B); }
+int trsm_run(Ctx &c, int n, int m, CMatF U, CMatF B) { return trsm(c, 2, n, m, U, B); }
+int trsm_rlu(Ctx &c, int n, int m, CMatF L, CMatF B) { return trsm(c, 3, n, m, L, B); }
 
 int laswp(Ctx &c, CMatF A, int j0, int j1, const int32_t *ipiv, int64_t sP, int c0, int c1,
           bool forward) {
@@ -899,6 +1074,9 @@ extern "C" int mnpb_getrf_c32p(void *stream, int64_t n, int64_t batch, float *A,
     clear_error();
     MNPB_REQUIRE(n > 0 && batch > 0 && batch < 65536 && ld >= n, "getrf_c32p: bad sizes");
     MNPB_REQUIRE(A && piv && work, "getrf_c32p: null pointer");
+    MNPB_REQUIRE(ld % 4 == 0 && plane % 4 == 0 && stride % 4 == 0 && ((uintptr_t)A & 15) == 0,
+                 "getrf_c32p: ld, plane and stride must be multiples of 4 floats and A 16-byte "
+                 "aligned");
     f32::Ctx c(as_stream(stream), (int)batch, (float *)work, work_bytes);
     return f32::getrf(c, (int)n, tc::CMatF{A, ld, plane, stride}, piv, pstride, info);
 }
@@ -909,6 +1087,11 @@ extern "C" int mnpb_getrs_c32p(void *stream, int64_t n, int64_t batch, int64_t n
                                int64_t planeB, int64_t bstride, void *work, int64_t work_bytes) {
     clear_error();
     MNPB_REQUIRE(n > 0 && batch > 0 && nrhs > 0 && ld >= n && ldb >= n, "getrs_c32p: bad sizes");
+    MNPB_REQUIRE(ld % 4 == 0 && plane % 4 == 0 && stride % 4 == 0 && ldb % 4 == 0 &&
+                     planeB % 4 == 0 && bstride % 4 == 0 && ((uintptr_t)LU & 15) == 0 &&
+                     ((uintptr_t)B & 15) == 0,
+                 "getrs_c32p: leading dimensions, planes and strides must be multiples of 4 "
+                 "floats and base pointers 16-byte aligned");
     MNPB_REQUIRE(LU && piv && B && work, "getrs_c32p: null pointer");
     f32::Ctx c(as_stream(stream), (int)batch, (float *)work, work_bytes);
     return f32::getrs(c, (int)n, (int)nrhs, tc::CMatF{(float *)LU, ld, plane, stride}, piv,

@@ -27,7 +27,8 @@ def rel(a, b):
     return np.abs(np.asarray(a) - np.asarray(b)).max() / np.abs(np.asarray(b)).max()
 
 
-@pytest.mark.parametrize('n,batch,nrhs', [(32, 1, 1), (100, 2, 3), (256, 3, 5), (300, 1, 40)])
+@pytest.mark.parametrize('n,batch,nrhs', [(32, 1, 1), (100, 2, 3), (256, 3, 5), (300, 1, 40),
+                                         (700, 2, 300), (130, 1, 130)])
 def test_getrf_getrs_c32p(gpu_ok, n, batch, nrhs):
     ld = (n + 3) // 4 * 4
     g = torch.Generator().manual_seed(7)
@@ -41,9 +42,9 @@ def test_getrf_getrs_c32p(gpu_ok, n, batch, nrhs):
     A = torch.zeros((batch, 2, n, ld), dtype=torch.float32)
     A[:, 0, :, :n] = Ac.real.transpose(1, 2).float()
     A[:, 1, :, :n] = Ac.imag.transpose(1, 2).float()
-    B = torch.zeros((batch, 2, nrhs, n), dtype=torch.float32)
-    B[:, 0] = Bc.real.transpose(1, 2).float()
-    B[:, 1] = Bc.imag.transpose(1, 2).float()
+    B = torch.zeros((batch, 2, nrhs, ld), dtype=torch.float32)
+    B[:, 0, :, :n] = Bc.real.transpose(1, 2).float()
+    B[:, 1, :, :n] = Bc.imag.transpose(1, 2).float()
     A, B = A.cuda(), B.cuda()
     piv = torch.zeros((batch, n), dtype=torch.int32, device='cuda')
     info = torch.zeros(batch, dtype=torch.int32, device='cuda')
@@ -53,10 +54,10 @@ def test_getrf_getrs_c32p(gpu_ok, n, batch, nrhs):
     call('mnpb_getrf_c32p', sh, n, batch, ptr(A), ld, n * ld, 2 * n * ld, ptr(piv), n, ptr(info),
          ptr(work), wb)
     call('mnpb_getrs_c32p', sh, n, batch, nrhs, ptr(A), ld, n * ld, 2 * n * ld, ptr(piv), n,
-         ptr(B), n, n * nrhs, 2 * n * nrhs, ptr(work), wb)
+         ptr(B), ld, ld * nrhs, 2 * ld * nrhs, ptr(work), wb)
     torch.cuda.synchronize()
     assert info.sum().item() == 0
-    Xg = (B[:, 0].double() + 1j * B[:, 1].double()).transpose(1, 2).cpu()
+    Xg = (B[:, 0, :, :n].double() + 1j * B[:, 1, :, :n].double()).transpose(1, 2).cpu()
     err = ((Xg - X).abs().pow(2).sum() / X.abs().pow(2).sum()).sqrt().item()
     assert err < 1e-2, err
 
