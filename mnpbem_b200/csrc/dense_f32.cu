@@ -40,6 +40,13 @@ __device__ __forceinline__ cf frcp(cf b) {
         return cf{r / d, -1.f / d};
     }
 }
+// nearest TF32 (10-bit mantissa), ties away from zero
+__device__ __forceinline__ float tf32_rna(float v) {
+    uint32_t t;
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(t) : "f"(v));
+    return __uint_as_float(t);
+}
+__device__ __forceinline__ cf rna(cf v) { return cf{tf32_rna(v.x), tf32_rna(v.y)}; }
 __device__ __forceinline__ cf ld(const float *p, int64_t plane, int64_t o) {
     return cf{p[o], p[o + plane]};
 }
@@ -109,14 +116,19 @@ __global__ void __launch_bounds__(PANEL_THREADS) panel_kernel(int n, int k0, int
         }
         __syncthreads();
         const int rest = kb - jj;
-        for (int cc = tid; cc < rest; cc += PANEL_THREADS) prow[cc] = ld(A, plane, (int64_t)(c + cc) * lda + c);
+        for (int cc = tid; cc < rest; cc += PANEL_THREADS) {
+            const int64_t o = (int64_t)(c + cc) * lda + c;
+            const cf u = rna(ld(A, plane, o));
+            prow[cc] = u;
+            st(A, plane, o, u);
+        }
         __syncthreads();
         const cf pv = prow[0];
         const bool nz = (pv.x != 0.f || pv.y != 0.f);
         const cf inv = nz ? frcp(pv) : fmk(0.f, 0.f);
         for (int r = c + 1 + tid; r < n; r += PANEL_THREADS) {
             cf l = ld(A, plane, co + r);
-            if (nz) l = fmul(l, inv);
+            if (nz) l = rna(fmul(l, inv));
             st(A, plane, co + r, l);
             for (int cc = 1; cc < rest; ++cc) {
                 const int64_t o = (int64_t)(c + cc) * lda + r;
@@ -218,13 +230,20 @@ __global__ void __launch_bounds__(SLAB_THREADS) panel_slab_kernel(int n, int k0,
                     st(A, plane, o + cs + ip, t);
                 }
             }
+            // the pivot row's U entries are final: store them as TF32 (same
+            // thread per column as the swap above)
+            for (int j = tid; j < SW; j += SLAB_THREADS) {
+                if (j < jj) continue;
+                sre[j * mmax + jj] = tf32_rna(sre[j * mmax + jj]);
+                sim[j * mmax + jj] = tf32_rna(sim[j * mmax + jj]);
+            }
             __syncthreads();
             const cf pv = fmk(sre[jj * mmax + jj], sim[jj * mmax + jj]);
             const bool nz = (pv.x != 0.f || pv.y != 0.f);
             const cf inv = nz ? frcp(pv) : fmk(0.f, 0.f);
             for (int i = jj + 1 + tid; i < ms; i += SLAB_THREADS) {
                 cf l = fmk(sre[jj * mmax + i], sim[jj * mmax + i]);
-                if (nz) l = fmul(l, inv);
+                if (nz) l = rna(fmul(l, inv));
                 sre[jj * mmax + i] = l.x;
                 sim[jj * mmax + i] = l.y;
                 for (int j = jj + 1; j < SW; ++j) {
@@ -258,6 +277,7 @@ __global__ void __launch_bounds__(SLAB_THREADS) panel_slab_kernel(int n, int k0,
                         x[r] = ffms(fmk(sre[t * mmax + r], sim[t * mmax + r]), x[t], x[r]);
 #pragma unroll
                 for (int r = 0; r < SW; ++r) {
+                    x[r] = rna(x[r]);
                     st(A, plane, o + r, x[r]);
                     u12[r][q] = x[r];
                 }
@@ -382,7 +402,7 @@ __global__ void __launch_bounds__(128) trsm_small_kernel(int mode, int kb, const
     }
 #pragma unroll
     for (int e = 0; e < TS; ++e)
-        if (e < kb) st(B, planeB, left ? (int64_t)v * ldb + e : (int64_t)e * ldb + v, x[e]);
+        if (e < kb) st(B, planeB, left ? (int64_t)v * ldb + e : (int64_t)e * ldb + v, rna(x[e]));
 }
 
 // Inverses of the 128 x 128 diagonal blocks of a unit-lower (lower = 1) or
@@ -397,11 +417,6 @@ __global__ void __launch_bounds__(128) trsm_small_kernel(int mode, int kb, const
 constexpr int TL = 128;
 constexpr int TINV_THREADS = 512;
 
-__device__ __forceinline__ float tf32_rna(float v) {
-    uint32_t t;
-    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(t) : "f"(v));
-    return __uint_as_float(t);
-}
 
 __global__ void __launch_bounds__(TINV_THREADS) tri_inv_kernel(int n, int lower, const float *A,
                                                                int64_t lda, int64_t plane,
@@ -499,7 +514,7 @@ __global__ void __launch_bounds__(128) skinny_kernel(int m, int n, int k, float 
                                                      const float *__restrict__ B, int64_t ldb,
                                                      int64_t planeB, int64_t sB, float beta,
                                                      float *__restrict__ C, int64_t ldc,
-                                                     int64_t planeC, int64_t sC) {
+                                                     int64_t planeC, int64_t sC, int rnd) {
     __shared__ cf Bs[SK_KT][NC];
     const int64_t b = blockIdx.y;
     A += b * sA;
@@ -539,7 +554,9 @@ __global__ void __launch_bounds__(128) skinny_kernel(int m, int n, int k, float 
         if (j < n) {
             const int64_t o = (int64_t)j * ldc + row;
             cf c = beta != 0.f ? ld(C, planeC, o) : fmk(0.f, 0.f);
-            st(C, planeC, o, fmk(alpha * acc[j].x + beta * c.x, alpha * acc[j].y + beta * c.y));
+            cf v = fmk(alpha * acc[j].x + beta * c.x, alpha * acc[j].y + beta * c.y);
+            if (rnd) v = fmk(tf32_rna(v.x), tf32_rna(v.y));
+            st(C, planeC, o, v);
         }
     }
 }
@@ -766,7 +783,8 @@ __global__ void set_identity_kernel(float *W, int64_t ldw, int64_t plane, int64_
 Ctx::Ctx(cudaStream_t s_, int batch_, float *work_, int64_t work_bytes_)
     : s(s_), batch(batch_), work(work_), work_bytes(work_bytes_) {}
 
-int gemm(Ctx &c, int m, int n, int k, float alpha, CMatF A, CMatF B, float beta, CMatF C) {
+int gemm(Ctx &c, int m, int n, int k, float alpha, CMatF A, CMatF B, float beta, CMatF C,
+         bool round_out) {
     if (m <= 0 || n <= 0) return MNPB_OK;
     if (k <= 0) {
         if (beta == 1.f) return MNPB_OK;
@@ -780,7 +798,7 @@ int gemm(Ctx &c, int m, int n, int k, float alpha, CMatF A, CMatF B, float beta,
 #define MNPB_SKINNY(NC)                                                                        \
     skinny_kernel<NC><<<grid, 128, 0, c.s>>>(m, n, k, alpha, A.p, A.ld, A.plane, A.stride, B.p, \
                                              B.ld, B.plane, B.stride, beta, C.p, C.ld, C.plane, \
-                                             C.stride)
+                                             C.stride, round_out ? 1 : 0)
         if (n <= 1) MNPB_SKINNY(1);
         else if (n <= 2) MNPB_SKINNY(2);
         else if (n <= 4) MNPB_SKINNY(4);
@@ -790,7 +808,8 @@ int gemm(Ctx &c, int m, int n, int k, float alpha, CMatF A, CMatF B, float beta,
         MNPB_LAUNCH_CHECK("skinny_kernel");
         return MNPB_OK;
     }
-    return tc::cgemm_tf32(c.s, m, n, k, c.batch, alpha, A, B, beta, C, c.work, c.work_bytes);
+    return tc::cgemm_tf32(c.s, m, n, k, c.batch, alpha, A, B, beta, C, c.work, c.work_bytes,
+                          round_out);
 }
 
 static int trsm_small(Ctx &c, int mode, int kb, CMatF T, CMatF B, int nvec) {
@@ -845,10 +864,10 @@ static int trsm_rec(Ctx &c, int mode, int n, int m, CMatF T, CMatF B, const InvS
     if (!iv && n <= TS) return trsm_small(c, mode, n, T, B, m);
     if (iv && n <= TL) {
         const CMatF I = inv_block(*iv, blk0);
-        if (mode >= 2) return gemm(c, m, n, n, 1.f, B, I, 0.f, B);
+        if (mode >= 2) return gemm(c, m, n, n, 1.f, B, I, 0.f, B, true);
         round_tf32_kernel<<<dim3(m, c.batch), TL, 0, c.s>>>(B.p, B.ld, B.plane, B.stride, n);
         MNPB_LAUNCH_CHECK("round_tf32_kernel");
-        return gemm(c, n, m, n, 1.f, I, B, 0.f, B);
+        return gemm(c, n, m, n, 1.f, I, B, 0.f, B, true);
     }
     const int n1 = iv ? split_tl(n) : split_point(n);
     const int blk1 = blk0 + n1 / TL;

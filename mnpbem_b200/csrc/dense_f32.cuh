@@ -16,7 +16,7 @@ struct Ctx {
 };
 
 int gemm(Ctx &c, int m, int n, int k, float alpha, tc::CMatF A, tc::CMatF B, float beta,
-         tc::CMatF C);
+         tc::CMatF C, bool round_out = false);
 int trsm_llu(Ctx &c, int n, int m, tc::CMatF L, tc::CMatF B);
 int trsm_lun(Ctx &c, int n, int m, tc::CMatF U, tc::CMatF B);
 int trsm_run(Ctx &c, int n, int m, tc::CMatF U, tc::CMatF B);

@@ -159,7 +159,14 @@ struct Epi {
     int64_t ldc, planeC, strideC;
     float alpha, beta;
     int M, N, ktiles;
+    int round_out;   // 1: store C rounded to nearest TF32
 };
+
+__device__ __forceinline__ float rna_tf32(float v) {
+    uint32_t t;
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(t) : "f"(v));
+    return __uint_as_float(t);
+}
 
 template <int BN>
 __global__ void __launch_bounds__(128)
@@ -294,6 +301,13 @@ __global__ void __launch_bounds__(128)
             for (int c = 0; c < CH; ++c) {
                 vr[c] *= ep.alpha;
                 vi[c] *= ep.alpha;
+            }
+        }
+        if (ep.round_out) {
+#pragma unroll
+            for (int c = 0; c < CH; ++c) {
+                vr[c] = rna_tf32(vr[c]);
+                vi[c] = rna_tf32(vi[c]);
             }
         }
 #pragma unroll
@@ -504,6 +518,13 @@ __global__ void __launch_bounds__(192, 1)
                         vi[c] *= ep.alpha;
                     }
                 }
+                if (ep.round_out) {
+#pragma unroll
+                    for (int c = 0; c < CH; ++c) {
+                        vr[c] = rna_tf32(vr[c]);
+                        vi[c] = rna_tf32(vi[c]);
+                    }
+                }
 #pragma unroll
                 for (int c = 0; c < CH; ++c) {
                     if (c < ncol) {
@@ -548,6 +569,59 @@ __global__ void pack_a_tf32_kernel(const float *__restrict__ A, int64_t lda, int
     for (int i = threadIdx.y; i < 32; i += blockDim.y) {
         const int m = mb + i, k = kb + threadIdx.x;
         if (m < Mp && k < Kp) dst[(int64_t)m * Kp + k] = tile[threadIdx.x][i];
+    }
+}
+
+// Same pack for 16-byte aligned operands (base, lda, plane and stride all
+// multiples of 4 floats): 64 x 64 tiles, 16-byte loads and stores, four
+// independent loads per thread in flight before any shared-memory traffic.
+constexpr int PK = 64;
+__global__ void __launch_bounds__(256) pack_a_tf32_vec_kernel(const float *__restrict__ A,
+                                                              int64_t lda, int64_t planeA,
+                                                              int64_t strideA, int M, int K,
+                                                              int Mp, int Kp,
+                                                              float *__restrict__ out) {
+    __shared__ float tile[PK][PK + 1];   // tile[k][m]
+    const int b = blockIdx.z >> 1, pl = blockIdx.z & 1;
+    const int mb = blockIdx.x * PK, kb = blockIdx.y * PK;
+    const float *src = A + (int64_t)b * strideA + (int64_t)pl * planeA;
+    const int tid = threadIdx.x;
+    float4 v[4];
+#pragma unroll
+    for (int p = 0; p < 4; ++p) {
+        const int idx = tid + 256 * p, kc = idx >> 4, m = mb + 4 * (idx & 15), k = kb + kc;
+        v[p] = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (k < K) {
+            const float *s = src + (int64_t)k * lda + m;
+            if (m + 3 < M) {
+                v[p] = __ldg(reinterpret_cast<const float4 *>(s));
+            } else {
+                if (m < M) v[p].x = s[0];
+                if (m + 1 < M) v[p].y = s[1];
+                if (m + 2 < M) v[p].z = s[2];
+            }
+        }
+    }
+#pragma unroll
+    for (int p = 0; p < 4; ++p) {
+        const int idx = tid + 256 * p, kc = idx >> 4, mm = 4 * (idx & 15);
+        const float e[4] = {v[p].x, v[p].y, v[p].z, v[p].w};
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            uint32_t t;
+            asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(t) : "f"(e[q]));
+            tile[kc][mm + q] = __uint_as_float(t);
+        }
+    }
+    __syncthreads();
+    float *dst = out + ((int64_t)b * 2 + pl) * (int64_t)Mp * Kp;
+#pragma unroll
+    for (int p = 0; p < 4; ++p) {
+        const int idx = tid + 256 * p, mr = idx >> 4, kq = 4 * (idx & 15);
+        const int m = mb + mr, k = kb + kq;
+        if (m < Mp && k < Kp)
+            *reinterpret_cast<float4 *>(dst + (int64_t)m * Kp + k) =
+                make_float4(tile[kq][mr], tile[kq + 1][mr], tile[kq + 2][mr], tile[kq + 3][mr]);
     }
 }
 
@@ -673,7 +747,7 @@ static int launch_tf32(cudaStream_t s, const CUtensorMap &mA, const CMatF &B, in
 }
 
 int cgemm_tf32(cudaStream_t s, int M, int N, int K, int batch, float alpha, CMatF A, CMatF B,
-               float beta, CMatF C, float *work, int64_t work_bytes) {
+               float beta, CMatF C, float *work, int64_t work_bytes, bool round_out) {
     if (M <= 0 || N <= 0 || batch <= 0) return MNPB_OK;
     if (K <= 0) {
         set_error("tc_gemm: K must be positive");
@@ -685,14 +759,21 @@ int cgemm_tf32(cudaStream_t s, int M, int N, int K, int batch, float alpha, CMat
         return MNPB_ENOMEM;
     }
     {
-        dim3 g(Mp / 32, Kp / 32, batch * 2), t(32, 8);
         ProfScope ps(s, PC_PACK, 8.0 * (double)M * K * batch);
-        pack_a_tf32_kernel<<<g, t, 0, s>>>(A.p, A.ld, A.plane, A.stride, M, K, Mp, Kp, work);
-        MNPB_LAUNCH_CHECK("pack_a_tf32_kernel");
+        if (((uintptr_t)A.p & 15) == 0 && A.ld % 4 == 0 && A.plane % 4 == 0 && A.stride % 4 == 0) {
+            dim3 g(Mp / PK, (Kp + PK - 1) / PK, batch * 2);
+            pack_a_tf32_vec_kernel<<<g, 256, 0, s>>>(A.p, A.ld, A.plane, A.stride, M, K, Mp, Kp,
+                                                     work);
+            MNPB_LAUNCH_CHECK("pack_a_tf32_vec_kernel");
+        } else {
+            dim3 g(Mp / 32, Kp / 32, batch * 2), t(32, 8);
+            pack_a_tf32_kernel<<<g, t, 0, s>>>(A.p, A.ld, A.plane, A.stride, M, K, Mp, Kp, work);
+            MNPB_LAUNCH_CHECK("pack_a_tf32_kernel");
+        }
     }
     CUtensorMap mA;
     MNPB_TRY(make_map(&mA, work, Kp, Mp, (uint64_t)batch * 2, Kp, (uint64_t)Mp * Kp, BM));
-    Epi ep{C.p, C.ld, C.plane, C.stride, alpha, beta, M, N, Kp / BK};
+    Epi ep{C.p, C.ld, C.plane, C.stride, alpha, beta, M, N, Kp / BK, round_out ? 1 : 0};
     ProfScope ps(s, PC_TCGEMM, 8.0 * M * N * (double)K * batch);
     prof_tag("M=%d N=%d K=%d B=%d", M, N, K, batch);
     if (N <= 32) return launch_tf32<32>(s, mA, B, M, N, K, Kp, Mp, batch, ep);

@@ -17,8 +17,10 @@ struct CMatF {
 
 int64_t cgemm_tf32_workspace(int M, int K, int batch);
 // C = beta C + alpha A B (A: M x K, B: K x N, C: M x N), work >= cgemm_tf32_workspace.
+// round_out: store C rounded to nearest TF32 (values that later GEMMs read as
+// operands then reach the tensor cores unchanged).
 int cgemm_tf32(cudaStream_t s, int M, int N, int K, int batch, float alpha, CMatF A, CMatF B,
-               float beta, CMatF C, float *work, int64_t work_bytes);
+               float beta, CMatF C, float *work, int64_t work_bytes, bool round_out = false);
 int tc_error_read_and_clear(cudaStream_t s, int *code);
 
 }  // namespace tc
