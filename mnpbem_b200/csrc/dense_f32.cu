@@ -765,6 +765,132 @@ __global__ void __launch_bounds__(256) trsv_kernel(int n, int m, int lower, cons
     }
 }
 
+// Few-RHS triangular solve, one CTA per matrix, right-looking: the whole
+// right-hand side lives in shared memory (r[i][c], n x NC), each 32-row block
+// is solved through its precomputed diagonal inverse, then every row the
+// block feeds (below it for L, above it for U) subtracts T[i, block] x_block,
+// streaming that column block of the triangle once.  Two rows per thread with
+// 8-byte loads, 16 columns in flight; the next block's diagonal inverse is
+// staged while the current block's update runs.  No inter-CTA waits.
+constexpr int RL_THREADS = 512;
+template <int NC>
+__global__ void __launch_bounds__(RL_THREADS) trsv_rl_kernel(int n, int m, int lower,
+                                                             const float *__restrict__ A,
+                                                             int64_t lda, int64_t plane,
+                                                             int64_t sA,
+                                                             const float *__restrict__ Dinv,
+                                                             float *X, int64_t ldx,
+                                                             int64_t planeX, int64_t sX, int nb) {
+    extern __shared__ __align__(16) unsigned char rl_smem[];
+    cf *r = reinterpret_cast<cf *>(rl_smem);   // r[i * NC + c]
+    __shared__ cf dsm[2][TB][TB + 1];
+    __shared__ cf xj[TB][NC];
+    const int tid = threadIdx.x;
+    const int64_t b = blockIdx.x;
+    A += b * sA;
+    X += b * sX;
+    const float *Db = Dinv + b * nb * 2 * TB * TB;
+    for (int e = tid; e < n * NC; e += RL_THREADS) {
+        const int i = e % n, c = e / n;
+        r[i * NC + c] = c < m ? ld(X, planeX, (int64_t)c * ldx + i) : fmk(0.f, 0.f);
+    }
+    {
+        const int j = lower ? 0 : nb - 1;
+        const float *Di = Db + (int64_t)j * 2 * TB * TB;
+        for (int e = tid; e < TB * TB; e += RL_THREADS) {
+            const int rr = e % TB, k = e / TB;
+            dsm[0][rr][k] = fmk(__ldg(Di + k * TB + rr), __ldg(Di + TB * TB + k * TB + rr));
+        }
+    }
+    __syncthreads();
+    for (int jj = 0; jj < nb; ++jj) {
+        const int j = lower ? jj : nb - 1 - jj, r0 = j * TB, rows = min(TB, n - r0);
+        const int buf = jj & 1;
+        // diagonal block: x_j = D_j^{-1} r_j
+        if (tid < TB * NC) {
+            const int rr = tid % TB, c = tid / TB;
+            cf y = fmk(0.f, 0.f);
+            if (rr < rows && c < m) {
+#pragma unroll 8
+                for (int k = 0; k < TB; ++k) {
+                    if (k < rows) {
+                        const cf d = dsm[buf][rr][k], v = r[(r0 + k) * NC + c];
+                        y.x = fmaf(d.x, v.x, y.x);
+                        y.x = fmaf(-d.y, v.y, y.x);
+                        y.y = fmaf(d.x, v.y, y.y);
+                        y.y = fmaf(d.y, v.x, y.y);
+                    }
+                }
+                st(X, planeX, (int64_t)c * ldx + r0 + rr, y);
+            }
+            xj[rr][c] = y;
+        }
+        __syncthreads();
+        // stage the next block's inverse while this block's update runs
+        if (jj + 1 < nb) {
+            const int jn = lower ? j + 1 : j - 1;
+            const float *Di = Db + (int64_t)jn * 2 * TB * TB;
+            for (int e = tid; e < TB * TB; e += RL_THREADS) {
+                const int rr = e % TB, k = e / TB;
+                dsm[buf ^ 1][rr][k] =
+                    fmk(__ldg(Di + k * TB + rr), __ldg(Di + TB * TB + k * TB + rr));
+            }
+        }
+        const int lo = lower ? r0 + rows : 0, hi = lower ? n : r0;
+        const float *Ac = A + (int64_t)r0 * lda;
+        for (int i = lo + 2 * tid; i < hi; i += 2 * RL_THREADS) {
+            const bool two = i + 1 < hi;
+            cf a0[NC], a1[NC];
+#pragma unroll
+            for (int c = 0; c < NC; ++c) a0[c] = a1[c] = fmk(0.f, 0.f);
+            for (int k0 = 0; k0 < rows; k0 += 16) {
+                float2 vr[16], vi[16];
+#pragma unroll
+                for (int k = 0; k < 16; ++k) {
+                    vr[k] = vi[k] = make_float2(0.f, 0.f);
+                    if (k0 + k < rows) {
+                        const float *p = Ac + (int64_t)(k0 + k) * lda + i;
+                        if (two) {
+                            vr[k] = __ldg(reinterpret_cast<const float2 *>(p));
+                            vi[k] = __ldg(reinterpret_cast<const float2 *>(p + plane));
+                        } else {
+                            vr[k].x = __ldg(p);
+                            vi[k].x = __ldg(p + plane);
+                        }
+                    }
+                }
+#pragma unroll
+                for (int k = 0; k < 16; ++k) {
+#pragma unroll
+                    for (int c = 0; c < NC; ++c) {
+                        const cf x = xj[(k0 + k) & (TB - 1)][c];
+                        a0[c].x = fmaf(vr[k].x, x.x, a0[c].x);
+                        a0[c].x = fmaf(-vi[k].x, x.y, a0[c].x);
+                        a0[c].y = fmaf(vr[k].x, x.y, a0[c].y);
+                        a0[c].y = fmaf(vi[k].x, x.x, a0[c].y);
+                        a1[c].x = fmaf(vr[k].y, x.x, a1[c].x);
+                        a1[c].x = fmaf(-vi[k].y, x.y, a1[c].x);
+                        a1[c].y = fmaf(vr[k].y, x.y, a1[c].y);
+                        a1[c].y = fmaf(vi[k].y, x.x, a1[c].y);
+                    }
+                }
+            }
+#pragma unroll
+            for (int c = 0; c < NC; ++c) {
+                cf &u = r[i * NC + c];
+                u.x -= a0[c].x;
+                u.y -= a0[c].y;
+                if (two) {
+                    cf &w = r[(i + 1) * NC + c];
+                    w.x -= a1[c].x;
+                    w.y -= a1[c].y;
+                }
+            }
+        }
+        __syncthreads();
+    }
+}
+
 __global__ void set_identity_kernel(float *W, int64_t ldw, int64_t plane, int64_t sW, int n) {
     const int64_t b = blockIdx.z;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -784,7 +910,7 @@ Ctx::Ctx(cudaStream_t s_, int batch_, float *work_, int64_t work_bytes_)
     : s(s_), batch(batch_), work(work_), work_bytes(work_bytes_) {}
 
 int gemm(Ctx &c, int m, int n, int k, float alpha, CMatF A, CMatF B, float beta, CMatF C,
-         bool round_out) {
+         bool round_out, bool a_tf32) {
     if (m <= 0 || n <= 0) return MNPB_OK;
     if (k <= 0) {
         if (beta == 1.f) return MNPB_OK;
@@ -809,7 +935,7 @@ int gemm(Ctx &c, int m, int n, int k, float alpha, CMatF A, CMatF B, float beta,
         return MNPB_OK;
     }
     return tc::cgemm_tf32(c.s, m, n, k, c.batch, alpha, A, B, beta, C, c.work, c.work_bytes,
-                          round_out);
+                          round_out, a_tf32);
 }
 
 static int trsm_small(Ctx &c, int mode, int kb, CMatF T, CMatF B, int nvec) {
@@ -864,29 +990,33 @@ static int trsm_rec(Ctx &c, int mode, int n, int m, CMatF T, CMatF B, const InvS
     if (!iv && n <= TS) return trsm_small(c, mode, n, T, B, m);
     if (iv && n <= TL) {
         const CMatF I = inv_block(*iv, blk0);
+        // right leaf: A is the not-yet-rounded right-hand side, packed with rounding
         if (mode >= 2) return gemm(c, m, n, n, 1.f, B, I, 0.f, B, true);
         round_tf32_kernel<<<dim3(m, c.batch), TL, 0, c.s>>>(B.p, B.ld, B.plane, B.stride, n);
         MNPB_LAUNCH_CHECK("round_tf32_kernel");
-        return gemm(c, n, m, n, 1.f, I, B, 0.f, B, true);
+        return gemm(c, n, m, n, 1.f, I, B, 0.f, B, true, true);
     }
     const int n1 = iv ? split_tl(n) : split_point(n);
     const int blk1 = blk0 + n1 / TL;
+    // the A operand of every update is TF32 already: a factor block (stored
+    // rounded by the LU) or right-hand-side rows a leaf has finished (stored
+    // rounded), so the tensor cores read it in place
     switch (mode) {
     case 0:
         MNPB_TRY(trsm_rec(c, 0, n1, m, T, B, iv, blk0));
-        MNPB_TRY(gemm(c, n - n1, m, n1, -1.f, T.sub(n1, 0), B, 1.f, B.sub(n1, 0)));
+        MNPB_TRY(gemm(c, n - n1, m, n1, -1.f, T.sub(n1, 0), B, 1.f, B.sub(n1, 0), false, true));
         return trsm_rec(c, 0, n - n1, m, T.sub(n1, n1), B.sub(n1, 0), iv, blk1);
     case 1:
         MNPB_TRY(trsm_rec(c, 1, n - n1, m, T.sub(n1, n1), B.sub(n1, 0), iv, blk1));
-        MNPB_TRY(gemm(c, n1, m, n - n1, -1.f, T.sub(0, n1), B.sub(n1, 0), 1.f, B));
+        MNPB_TRY(gemm(c, n1, m, n - n1, -1.f, T.sub(0, n1), B.sub(n1, 0), 1.f, B, false, true));
         return trsm_rec(c, 1, n1, m, T, B, iv, blk0);
     case 2:
         MNPB_TRY(trsm_rec(c, 2, n1, m, T, B, iv, blk0));
-        MNPB_TRY(gemm(c, m, n - n1, n1, -1.f, B, T.sub(0, n1), 1.f, B.sub(0, n1)));
+        MNPB_TRY(gemm(c, m, n - n1, n1, -1.f, B, T.sub(0, n1), 1.f, B.sub(0, n1), false, true));
         return trsm_rec(c, 2, n - n1, m, T.sub(n1, n1), B.sub(0, n1), iv, blk1);
     default:
         MNPB_TRY(trsm_rec(c, 3, n - n1, m, T.sub(n1, n1), B.sub(0, n1), iv, blk1));
-        MNPB_TRY(gemm(c, m, n1, n - n1, -1.f, B.sub(0, n1), T.sub(n1, 0), 1.f, B));
+        MNPB_TRY(gemm(c, m, n1, n - n1, -1.f, B.sub(0, n1), T.sub(n1, 0), 1.f, B, false, true));
         return trsm_rec(c, 3, n1, m, T, B, iv, blk0);
     }
 }
@@ -978,8 +1108,9 @@ static int rgetrf(Ctx &c, int n, int off, int w, CMatF A, int32_t *ipiv, int64_t
     MNPB_TRY(rgetrf(c, n, off, w1, A, ipiv, sP, info));
     MNPB_TRY(laswp(c, A, off + w1, off + w, ipiv, sP, off, off + w1, true));
     MNPB_TRY(trsm_llu(c, w1, w - w1, A.sub(off, off), A.sub(off, off + w1)));
+    // L21 is stored rounded to TF32 by the panels: read in place
     MNPB_TRY(gemm(c, n - off - w1, w - w1, w1, -1.f, A.sub(off + w1, off),
-                  A.sub(off, off + w1), 1.f, A.sub(off + w1, off + w1)));
+                  A.sub(off, off + w1), 1.f, A.sub(off + w1, off + w1), false, true));
     MNPB_TRY(rgetrf(c, n, off + w1, w - w1, A, ipiv, sP, info));
     return laswp(c, A, off, off + w1, ipiv, sP, off + w1, off + w, true);
 }
@@ -1024,8 +1155,42 @@ int diag_inv(Ctx &c, int n, CMatF LU, float *invL, float *invU) {
 
 // state: caller-provided device scratch of trsv_state_bytes(n, batch) bytes
 // (flags per block and the ticket counter), cleared before each launch.
+template <int NC>
+static int trsv_rl(Ctx &c, bool lower, int n, int m, CMatF T, const float *inv, CMatF X) {
+    const int nb = ceil_div(n, TB);
+    const int dyn = n * NC * (int)sizeof(cf);
+    static int attr_bytes = 0;
+    if (dyn > 48 * 1024 && dyn > attr_bytes) {
+        if (cudaFuncSetAttribute(trsv_rl_kernel<NC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 dyn) != cudaSuccess) {
+            set_error("trsv_rl_kernel: cannot reserve %d bytes of shared memory", dyn);
+            return MNPB_ECUDA;
+        }
+        attr_bytes = dyn;
+    }
+    ProfScope ps(c.s, PC_TRSV, 4.0 * (double)n * n * c.batch);   // bytes of the triangle
+    prof_tag("n=%d m=%d B=%d %s", n, m, c.batch, lower ? "L" : "U");
+    trsv_rl_kernel<NC><<<c.batch, RL_THREADS, dyn, c.s>>>(n, m, lower ? 1 : 0, T.p, T.ld, T.plane,
+                                                         T.stride, inv, X.p, X.ld, X.plane,
+                                                         X.stride, nb);
+    MNPB_LAUNCH_CHECK("trsv_rl_kernel");
+    return MNPB_OK;
+}
+
 static int trsv(Ctx &c, bool lower, int n, int m, CMatF T, const float *inv, CMatF X,
                 int *state) {
+    // one CTA per matrix when the right-hand sides fit in shared memory and
+    // the triangle allows 8-byte row-pair loads
+    const bool even = ((uintptr_t)T.p & 7) == 0 && T.ld % 2 == 0 && T.plane % 2 == 0 &&
+                      T.stride % 2 == 0;
+    if (even && m <= 8) {
+        const int nc = m <= 1 ? 1 : m <= 4 ? 4 : 8;
+        if ((int64_t)n * nc * (int64_t)sizeof(cf) <= 200 * 1024) {
+            if (nc == 1) return trsv_rl<1>(c, lower, n, m, T, inv, X);
+            if (nc == 4) return trsv_rl<4>(c, lower, n, m, T, inv, X);
+            return trsv_rl<8>(c, lower, n, m, T, inv, X);
+        }
+    }
     const int nb = ceil_div(n, TB);
     int *flags = state;
     unsigned *ticket = (unsigned *)(state + (int64_t)nb * c.batch);

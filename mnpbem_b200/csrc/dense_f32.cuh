@@ -15,8 +15,9 @@ struct Ctx {
     Ctx(cudaStream_t s_, int batch_, float *work_, int64_t work_bytes_);
 };
 
+// round_out / a_tf32: see tc::cgemm_tf32 (store C as TF32; A holds TF32 values).
 int gemm(Ctx &c, int m, int n, int k, float alpha, tc::CMatF A, tc::CMatF B, float beta,
-         tc::CMatF C, bool round_out = false);
+         tc::CMatF C, bool round_out = false, bool a_tf32 = false);
 int trsm_llu(Ctx &c, int n, int m, tc::CMatF L, tc::CMatF B);
 int trsm_lun(Ctx &c, int n, int m, tc::CMatF U, tc::CMatF B);
 int trsm_run(Ctx &c, int n, int m, tc::CMatF U, tc::CMatF B);

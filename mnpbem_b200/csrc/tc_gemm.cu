@@ -93,11 +93,28 @@ __device__ __forceinline__ uint64_t smem_desc_k128(uint32_t addr) {
     d |= (uint64_t)2 << 61;                          // swizzle: 128 B
     return d;
 }
-// Instruction descriptor: TF32 x TF32 -> F32, both K-major, M = 128, N = bn.
-__host__ __device__ constexpr uint32_t idesc_tf32(bool neg_a, int bn) {
+// MN-major operand tile (A read straight from a column-major matrix): four
+// TMA boxes of 32 M x 32 K, 4096 B apart, each K row 128 B with its four 32-B
+// chunks swizzled (TMA 128B_ATOM_32B mode, descriptor layout type 1 = 128-B
+// swizzle on a 32-B base).  Leading byte offset: the 4096-B step between
+// 32-element M groups; stride byte offset: the 512-B step between 4-row K
+// groups.  One MMA (K = 8) reads 8 K rows = 1024 B from addr.
+__device__ __forceinline__ uint64_t smem_desc_mn128_32b(uint32_t addr) {
+    uint64_t d = 0;
+    d |= (uint64_t)((addr >> 4) & 0x3FFF);          // start address
+    d |= (uint64_t)(4096 >> 4) << 16;               // leading byte offset: M group step
+    d |= (uint64_t)(512 >> 4) << 32;                // stride byte offset: 4-row K group step
+    d |= (uint64_t)1 << 46;                          // descriptor version (sm_100)
+    d |= (uint64_t)1 << 61;                          // layout: 128-B swizzle, 32-B atoms
+    return d;
+}
+// Instruction descriptor: TF32 x TF32 -> F32, B K-major, A K-major (a_mn = false)
+// or MN-major, M = 128, N = bn.
+__host__ __device__ constexpr uint32_t idesc_tf32(bool neg_a, int bn, bool a_mn = false) {
     return (1u << 4)                    // D format F32
          | (2u << 7) | (2u << 10)       // A, B format TF32
          | ((neg_a ? 1u : 0u) << 13)    // negate A
+         | ((a_mn ? 1u : 0u) << 15)     // A major-ness: 1 = MN-major
          | ((uint32_t)(bn >> 3) << 17)  // N / 8
          | ((uint32_t)(BM >> 4) << 24); // M / 16
 }
@@ -168,9 +185,10 @@ __device__ __forceinline__ float rna_tf32(float v) {
     return __uint_as_float(t);
 }
 
-template <int BN>
+template <int BN, bool AMN>
 __global__ void __launch_bounds__(128)
     cgemm_tf32_kernel(const __grid_constant__ CUtensorMap tmA,
+                      const __grid_constant__ CUtensorMap tmAi,
                       const __grid_constant__ CUtensorMap tmBr,
                       const __grid_constant__ CUtensorMap tmBi, Epi ep, int STAGES) {
     using TL = Tile<BN>;
@@ -227,14 +245,23 @@ __global__ void __launch_bounds__(128)
             const uint32_t full = smem_u32(&bars[s]);
             mbar_expect_tx(full, STAGE_BYTES);
             const int k0 = kt * BK;
-            tma_load_3d(smem_u32(st), &tmA, full, k0, m0, 2 * b);
-            tma_load_3d(smem_u32(st + TILE_BYTES), &tmA, full, k0, m0, 2 * b + 1);
+            if (AMN) {
+#pragma unroll
+                for (int a = 0; a < BM / 32; ++a) {
+                    tma_load_3d(smem_u32(st + a * 4096), &tmA, full, m0 + 32 * a, k0, b);
+                    tma_load_3d(smem_u32(st + TILE_BYTES + a * 4096), &tmAi, full, m0 + 32 * a,
+                                k0, b);
+                }
+            } else {
+                tma_load_3d(smem_u32(st), &tmA, full, k0, m0, 2 * b);
+                tma_load_3d(smem_u32(st + TILE_BYTES), &tmA, full, k0, m0, 2 * b + 1);
+            }
             tma_load_3d(smem_u32(st + 2 * TILE_BYTES), &tmBr, full, k0, n0, b);
             tma_load_3d(smem_u32(st + 2 * TILE_BYTES + TL::B_BYTES), &tmBi, full, k0, n0, b);
         }
     } else if (warp == 1 && lane == 0) {
         // MMA issuer
-        constexpr uint32_t ID = idesc_tf32(false, BN), IDN = idesc_tf32(true, BN);
+        constexpr uint32_t ID = idesc_tf32(false, BN, AMN), IDN = idesc_tf32(true, BN, AMN);
         for (int kt = 0; kt < KT; ++kt) {
             const int s = kt % STAGES;
             if (!mbar_wait(smem_u32(&bars[s]), (kt / STAGES) & 1)) {
@@ -247,8 +274,9 @@ __global__ void __launch_bounds__(128)
 #pragma unroll
             for (int j = 0; j < BK / 8; ++j) {      // 8 TF32 = 32 bytes per MMA
                 const uint32_t off = 32 * j;
-                const uint64_t ar = smem_desc_k128(st + off);
-                const uint64_t ai = smem_desc_k128(st + TILE_BYTES + off);
+                const uint64_t ar = AMN ? smem_desc_mn128_32b(st + 1024 * j) : smem_desc_k128(st + off);
+                const uint64_t ai = AMN ? smem_desc_mn128_32b(st + TILE_BYTES + 1024 * j)
+                                        : smem_desc_k128(st + TILE_BYTES + off);
                 const uint64_t br = smem_desc_k128(st + 2 * TILE_BYTES + off);
                 const uint64_t bi = smem_desc_k128(st + 2 * TILE_BYTES + TL::B_BYTES + off);
                 const uint32_t acc = (kt > 0 || j > 0) ? 1u : 0u;
@@ -341,9 +369,10 @@ __device__ __forceinline__ void mbar_arrive(uint32_t bar) {
 // of the next tile fill the other one.  acc_full[b] (MMA -> epilogue, one
 // commit) and acc_empty[b] (epilogue -> MMA, 128 arrivals) hand the buffers
 // over.  Every wait is bounded as in cgemm_tf32_kernel.
-template <int BN>
+template <int BN, bool AMN>
 __global__ void __launch_bounds__(192, 1)
     cgemm_tf32_persistent(const __grid_constant__ CUtensorMap tmA,
+                          const __grid_constant__ CUtensorMap tmAi,
                           const __grid_constant__ CUtensorMap tmBr,
                           const __grid_constant__ CUtensorMap tmBi, Epi ep, int STAGES, int MT,
                           int NT, int ntiles) {
@@ -413,8 +442,17 @@ __global__ void __launch_bounds__(192, 1)
                     const uint32_t full = smem_u32(&bars[s]);
                     mbar_expect_tx(full, STAGE_BYTES);
                     const int k0 = kt * BK;
-                    tma_load_3d(smem_u32(st), &tmA, full, k0, m0, 2 * b);
-                    tma_load_3d(smem_u32(st + TILE_BYTES), &tmA, full, k0, m0, 2 * b + 1);
+                    if (AMN) {
+#pragma unroll
+                        for (int a = 0; a < BM / 32; ++a) {
+                            tma_load_3d(smem_u32(st + a * 4096), &tmA, full, m0 + 32 * a, k0, b);
+                            tma_load_3d(smem_u32(st + TILE_BYTES + a * 4096), &tmAi, full,
+                                        m0 + 32 * a, k0, b);
+                        }
+                    } else {
+                        tma_load_3d(smem_u32(st), &tmA, full, k0, m0, 2 * b);
+                        tma_load_3d(smem_u32(st + TILE_BYTES), &tmA, full, k0, m0, 2 * b + 1);
+                    }
                     tma_load_3d(smem_u32(st + 2 * TILE_BYTES), &tmBr, full, k0, n0, b);
                     tma_load_3d(smem_u32(st + 2 * TILE_BYTES + TL::B_BYTES), &tmBi, full, k0, n0,
                                 b);
@@ -425,7 +463,7 @@ __global__ void __launch_bounds__(192, 1)
     } else if (warp == 1) {
         if (lane == 0) {
             // MMA issuer
-            constexpr uint32_t ID = idesc_tf32(false, BN), IDN = idesc_tf32(true, BN);
+            constexpr uint32_t ID = idesc_tf32(false, BN, AMN), IDN = idesc_tf32(true, BN, AMN);
             uint32_t g = 0;
             int i = 0;
             for (int t = blockIdx.x; t < ntiles && !*abort_flag; t += gridDim.x, ++i) {
@@ -451,8 +489,10 @@ __global__ void __launch_bounds__(192, 1)
 #pragma unroll
                     for (int j = 0; j < BK / 8; ++j) {
                         const uint32_t off = 32 * j;
-                        const uint64_t ar = smem_desc_k128(st + off);
-                        const uint64_t ai = smem_desc_k128(st + TILE_BYTES + off);
+                        const uint64_t ar = AMN ? smem_desc_mn128_32b(st + 1024 * j)
+                                                : smem_desc_k128(st + off);
+                        const uint64_t ai = AMN ? smem_desc_mn128_32b(st + TILE_BYTES + 1024 * j)
+                                                : smem_desc_k128(st + TILE_BYTES + off);
                         const uint64_t br = smem_desc_k128(st + 2 * TILE_BYTES + off);
                         const uint64_t bi = smem_desc_k128(st + 2 * TILE_BYTES + TL::B_BYTES + off);
                         const uint32_t acc = (kt > 0 || j > 0) ? 1u : 0u;
@@ -650,7 +690,8 @@ static EncodeFn get_encode() {
 // 3-D FP32 map: inner dim d0 (contiguous), rows d1 (stride s1 elements),
 // planes/batch d2 (stride s2 elements); box 32 x 128 x 1, 128-byte swizzle.
 static int make_map(CUtensorMap *map, const float *base, uint64_t d0, uint64_t d1, uint64_t d2,
-                    uint64_t s1, uint64_t s2, uint32_t box_rows) {
+                    uint64_t s1, uint64_t s2, uint32_t box_rows,
+                    CUtensorMapSwizzle swz = CU_TENSOR_MAP_SWIZZLE_128B) {
     EncodeFn enc = get_encode();
     if (!enc) {
         set_error("tc_gemm: cuTensorMapEncodeTiled unavailable");
@@ -666,7 +707,7 @@ static int make_map(CUtensorMap *map, const float *base, uint64_t d0, uint64_t d
     cuuint32_t box[3] = {BK, box_rows, 1};
     cuuint32_t estr[3] = {1, 1, 1};
     CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, (void *)base, dims, strides, box,
-                     estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                     estr, CU_TENSOR_MAP_INTERLEAVE_NONE, swz,
                      CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) {
         set_error("tc_gemm: cuTensorMapEncodeTiled failed (%d)", (int)r);
@@ -693,13 +734,14 @@ int64_t cgemm_tf32_workspace(int M, int K, int batch) {
     return (int64_t)batch * 2 * Mp * Kp * 4;
 }
 
-template <int BN>
-static int launch_tf32(cudaStream_t s, const CUtensorMap &mA, const CMatF &B, int M, int N,
-                       int K, int Kp, int Mp, int batch, Epi ep) {
+template <int BN, bool AMN>
+static int launch_tf32(cudaStream_t s, const CUtensorMap &mA, const CUtensorMap &mAi,
+                       const CMatF &B, int M, int N, int K, int Kp, int Mp, int batch, Epi ep) {
     using TL = Tile<BN>;
     static bool attr_set = false;
     if (!attr_set) {
-        if (cudaFuncSetAttribute(cgemm_tf32_kernel<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        if (cudaFuncSetAttribute(cgemm_tf32_kernel<BN, AMN>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  TL::smem_bytes(TL::MAX_ST)) != cudaSuccess) {
             set_error("tc_gemm: cannot set shared memory size");
             return MNPB_ECUDA;
@@ -725,7 +767,7 @@ static int launch_tf32(cudaStream_t s, const CUtensorMap &mA, const CMatF &B, in
         // persistent: one CTA per SM, double-buffered accumulators
         static bool pattr = false;
         if (!pattr) {
-            if (cudaFuncSetAttribute(cgemm_tf32_persistent<BN>,
+            if (cudaFuncSetAttribute(cgemm_tf32_persistent<BN, AMN>,
                                      cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      TL::smem_bytes(TL::MAX_ST)) != cudaSuccess) {
                 set_error("tc_gemm: cannot set shared memory size (persistent)");
@@ -735,32 +777,57 @@ static int launch_tf32(cudaStream_t s, const CUtensorMap &mA, const CMatF &B, in
         }
         const int pst = TL::MAX_ST;
         const int grid = (int)(ntiles < num_sms() ? ntiles : num_sms());
-        cgemm_tf32_persistent<BN><<<grid, 192, TL::smem_bytes(pst), s>>>(mA, mBr, mBi, ep, pst, MT,
-                                                                        NT, (int)ntiles);
+        cgemm_tf32_persistent<BN, AMN><<<grid, 192, TL::smem_bytes(pst), s>>>(
+            mA, mAi, mBr, mBi, ep, pst, MT, NT, (int)ntiles);
         MNPB_LAUNCH_CHECK("cgemm_tf32_persistent");
         return MNPB_OK;
     }
     dim3 grid(MT, NT, batch);
-    cgemm_tf32_kernel<BN><<<grid, 128, dyn, s>>>(mA, mBr, mBi, ep, nst);
+    cgemm_tf32_kernel<BN, AMN><<<grid, 128, dyn, s>>>(mA, mAi, mBr, mBi, ep, nst);
     MNPB_LAUNCH_CHECK("cgemm_tf32_kernel");
     return MNPB_OK;
 }
 
+template <bool AMN>
+static int launch_any(cudaStream_t s, const CUtensorMap &mA, const CUtensorMap &mAi,
+                      const CMatF &B, int M, int N, int K, int Kp, int Mp, int batch, Epi ep) {
+    if (N <= 32) return launch_tf32<32, AMN>(s, mA, mAi, B, M, N, K, Kp, Mp, batch, ep);
+    if (N <= 64) return launch_tf32<64, AMN>(s, mA, mAi, B, M, N, K, Kp, Mp, batch, ep);
+    return launch_tf32<128, AMN>(s, mA, mAi, B, M, N, K, Kp, Mp, batch, ep);
+}
+
+static bool aligned16(const CMatF &X) {
+    return ((uintptr_t)X.p & 15) == 0 && X.ld % 4 == 0 && X.plane % 4 == 0 && X.stride % 4 == 0;
+}
+
 int cgemm_tf32(cudaStream_t s, int M, int N, int K, int batch, float alpha, CMatF A, CMatF B,
-               float beta, CMatF C, float *work, int64_t work_bytes, bool round_out) {
+               float beta, CMatF C, float *work, int64_t work_bytes, bool round_out,
+               bool a_tf32) {
     if (M <= 0 || N <= 0 || batch <= 0) return MNPB_OK;
     if (K <= 0) {
         set_error("tc_gemm: K must be positive");
         return MNPB_EINVAL;
     }
     const int Mp = (M + BM - 1) / BM * BM, Kp = (K + BK - 1) / BK * BK;
+    Epi ep{C.p, C.ld, C.plane, C.stride, alpha, beta, M, N, Kp / BK, round_out ? 1 : 0};
+    if (a_tf32 && aligned16(A)) {
+        // A already holds TF32 values: the tensor cores read it in place (MN-major)
+        CUtensorMap mAr, mAi;
+        MNPB_TRY(make_map(&mAr, A.p, M, K, batch, A.ld, A.stride, 32,
+                          CU_TENSOR_MAP_SWIZZLE_128B_ATOM_32B));
+        MNPB_TRY(make_map(&mAi, A.p + A.plane, M, K, batch, A.ld, A.stride, 32,
+                          CU_TENSOR_MAP_SWIZZLE_128B_ATOM_32B));
+        ProfScope ps(s, PC_TCGEMM, 8.0 * M * N * (double)K * batch);
+        prof_tag("M=%d N=%d K=%d B=%d mn", M, N, K, batch);
+        return launch_any<true>(s, mAr, mAi, B, M, N, K, Kp, Mp, batch, ep);
+    }
     if (work_bytes < cgemm_tf32_workspace(M, K, batch)) {
         set_error("tc_gemm: workspace too small");
         return MNPB_ENOMEM;
     }
     {
         ProfScope ps(s, PC_PACK, 8.0 * (double)M * K * batch);
-        if (((uintptr_t)A.p & 15) == 0 && A.ld % 4 == 0 && A.plane % 4 == 0 && A.stride % 4 == 0) {
+        if (aligned16(A)) {
             dim3 g(Mp / PK, (Kp + PK - 1) / PK, batch * 2);
             pack_a_tf32_vec_kernel<<<g, 256, 0, s>>>(A.p, A.ld, A.plane, A.stride, M, K, Mp, Kp,
                                                      work);
@@ -773,12 +840,9 @@ int cgemm_tf32(cudaStream_t s, int M, int N, int K, int batch, float alpha, CMat
     }
     CUtensorMap mA;
     MNPB_TRY(make_map(&mA, work, Kp, Mp, (uint64_t)batch * 2, Kp, (uint64_t)Mp * Kp, BM));
-    Epi ep{C.p, C.ld, C.plane, C.stride, alpha, beta, M, N, Kp / BK, round_out ? 1 : 0};
     ProfScope ps(s, PC_TCGEMM, 8.0 * M * N * (double)K * batch);
     prof_tag("M=%d N=%d K=%d B=%d", M, N, K, batch);
-    if (N <= 32) return launch_tf32<32>(s, mA, B, M, N, K, Kp, Mp, batch, ep);
-    if (N <= 64) return launch_tf32<64>(s, mA, B, M, N, K, Kp, Mp, batch, ep);
-    return launch_tf32<128>(s, mA, B, M, N, K, Kp, Mp, batch, ep);
+    return launch_any<false>(s, mA, mA, B, M, N, K, Kp, Mp, batch, ep);
 }
 
 int tc_error_read_and_clear(cudaStream_t s, int *code) {
@@ -859,7 +923,8 @@ constexpr int kMaxDevices = 64;
 
 template <int BN> static cudaError_t opt_in_smem() {
     using TL = Tile<BN>;
-    return cudaFuncSetAttribute(cgemm_tf32_kernel<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    return cudaFuncSetAttribute(cgemm_tf32_kernel<BN, false>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 TL::smem_bytes(TL::MAX_ST));
 }
 

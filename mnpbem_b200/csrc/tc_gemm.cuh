@@ -19,8 +19,13 @@ int64_t cgemm_tf32_workspace(int M, int K, int batch);
 // C = beta C + alpha A B (A: M x K, B: K x N, C: M x N), work >= cgemm_tf32_workspace.
 // round_out: store C rounded to nearest TF32 (values that later GEMMs read as
 // operands then reach the tensor cores unchanged).
+// a_tf32: the caller guarantees every element of A is a TF32 value (low 13
+// mantissa bits zero); A is then read in place by the tensor cores (MN-major
+// TMA loads) instead of being packed, when it is 16-byte aligned.  Without
+// that guarantee A is packed with round-to-nearest conversion.
 int cgemm_tf32(cudaStream_t s, int M, int N, int K, int batch, float alpha, CMatF A, CMatF B,
-               float beta, CMatF C, float *work, int64_t work_bytes, bool round_out = false);
+               float beta, CMatF C, float *work, int64_t work_bytes, bool round_out = false,
+               bool a_tf32 = false);
 int tc_error_read_and_clear(cudaStream_t s, int *code);
 
 }  // namespace tc
