@@ -159,6 +159,7 @@ __global__ void __launch_bounds__(SLAB_THREADS) panel_slab_kernel(int n, int k0,
     __shared__ int red_i[SLAB_THREADS / 32];
     __shared__ cf u12[SW][TS];
     __shared__ int s_piv;
+    __shared__ int slab_piv[SW];   // local pivot row of each slab column
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
     const int64_t b = blockIdx.x;
     A += b * sA;
@@ -207,6 +208,7 @@ __global__ void __launch_bounds__(SLAB_THREADS) panel_slab_kernel(int n, int k0,
                         if (info && info[b] == 0) info[b] = c + 1;
                     }
                     s_piv = ip;
+                    slab_piv[jj] = ip;
                     ipiv[c] = cs + ip;
                 }
             }
@@ -220,14 +222,6 @@ __global__ void __launch_bounds__(SLAB_THREADS) panel_slab_kernel(int n, int k0,
                     t = sim[j * mmax + jj];
                     sim[j * mmax + jj] = sim[j * mmax + ip];
                     sim[j * mmax + ip] = t;
-                }
-                for (int cc = tid; cc < kb; cc += SLAB_THREADS) {
-                    const int col = k0 + cc;
-                    if (col >= cs && col < cs + SW) continue;
-                    const int64_t o = (int64_t)col * lda;
-                    const cf t = ld(A, plane, o + c);
-                    st(A, plane, o + c, ld(A, plane, o + cs + ip));
-                    st(A, plane, o + cs + ip, t);
                 }
             }
             // the pivot row's U entries are final: store them as TF32 (same
@@ -262,6 +256,42 @@ __global__ void __launch_bounds__(SLAB_THREADS) panel_slab_kernel(int n, int k0,
             A[o] = sre[j * mmax + i];
             A[o + plane] = sim[j * mmax + i];
         }
+        // the slab's SW row interchanges, applied to the panel's other columns
+        // in one gather / permute / scatter (at most 2 SW distinct rows)
+        for (int cc = tid; cc < kb; cc += SLAB_THREADS) {
+            const int col = k0 + cc;
+            if (col >= cs && col < cs + SW) continue;
+            const int64_t o = (int64_t)col * lda + cs;
+            int rows[2 * SW];
+            int nr = 0;
+#pragma unroll
+            for (int jj = 0; jj < SW; ++jj) {
+                const int r1 = jj, r2 = slab_piv[jj];
+                bool h1 = false, h2 = false;
+                for (int t = 0; t < nr; ++t) {
+                    h1 |= rows[t] == r1;
+                    h2 |= rows[t] == r2;
+                }
+                if (!h1) rows[nr++] = r1;
+                if (!h2 && r2 != r1) rows[nr++] = r2;
+            }
+            cf vals[2 * SW];
+            for (int t = 0; t < nr; ++t) vals[t] = ld(A, plane, o + rows[t]);
+            for (int jj = 0; jj < SW; ++jj) {
+                const int r2 = slab_piv[jj];
+                if (r2 == jj) continue;
+                int t1 = 0, t2 = 0;
+                for (int t = 0; t < nr; ++t) {
+                    if (rows[t] == jj) t1 = t;
+                    if (rows[t] == r2) t2 = t;
+                }
+                const cf x = vals[t1];
+                vals[t1] = vals[t2];
+                vals[t2] = x;
+            }
+            for (int t = 0; t < nr; ++t) st(A, plane, o + rows[t], vals[t]);
+        }
+        __syncthreads();
         const int c1 = cs + SW, R = k0 + kb - c1;
         if (R > 0) {
             // U12 = L11^{-1} A12 (unit lower SW x SW from the slab's top rows)
@@ -284,16 +314,29 @@ __global__ void __launch_bounds__(SLAB_THREADS) panel_slab_kernel(int n, int k0,
             }
             __syncthreads();
             // A22 -= L21 U12 on rows cs+SW .. n-1
+            // all of a row's loads issued before its stores (one memory
+            // round trip per row instead of one per column)
             for (int i = SW + tid; i < ms; i += SLAB_THREADS) {
                 cf l[SW];
 #pragma unroll
                 for (int t = 0; t < SW; ++t) l[t] = fmk(sre[t * mmax + i], sim[t * mmax + i]);
-                for (int q = 0; q < R; ++q) {
-                    const int64_t o = (int64_t)(c1 + q) * lda + cs + i;
-                    cf a = ld(A, plane, o);
+                float *col = A + (int64_t)c1 * lda + cs + i;
+                for (int q0 = 0; q0 < R; q0 += 8) {
+                    cf a[8];
 #pragma unroll
-                    for (int t = 0; t < SW; ++t) a = ffms(l[t], u12[t][q], a);
-                    st(A, plane, o, a);
+                    for (int q = 0; q < 8; ++q)
+                        if (q0 + q < R)
+                            a[q] = fmk(col[(int64_t)(q0 + q) * lda],
+                                       col[(int64_t)(q0 + q) * lda + plane]);
+#pragma unroll
+                    for (int q = 0; q < 8; ++q) {
+                        if (q0 + q < R) {
+#pragma unroll
+                            for (int t = 0; t < SW; ++t) a[q] = ffms(l[t], u12[t][q0 + q], a[q]);
+                            col[(int64_t)(q0 + q) * lda] = a[q].x;
+                            col[(int64_t)(q0 + q) * lda + plane] = a[q].y;
+                        }
+                    }
                 }
             }
         }
@@ -301,48 +344,79 @@ __global__ void __launch_bounds__(SLAB_THREADS) panel_slab_kernel(int n, int k0,
     }
 }
 
+// Row / column interchanges of a pivot range.  Pivoting on these matrices
+// rarely moves a row, so each CTA first compacts the range's non-trivial
+// interchanges (pivot p != c) into shared memory, in order, 1024 pivots at a
+// time (warp 0, ballot + popc), and its threads then apply only those to
+// their own column (laswp) or row (colswp).
+constexpr int SWP_CHUNK = 1024;
+
+__device__ int compact_swaps(const int32_t *pv, int lo, int hi, int2 *list) {
+    // warp 0 fills list[0..count) with (c, pv[c]) for pv[c] != c, c in [lo, hi)
+    __shared__ int s_count;
+    if (threadIdx.x < 32) {
+        const int lane = threadIdx.x;
+        int count = 0;
+        for (int c0 = lo; c0 < hi; c0 += 32) {
+            const int c = c0 + lane;
+            const int p = c < hi ? pv[c] : c;
+            const bool f = p != c;
+            const unsigned m = __ballot_sync(0xffffffffu, f);
+            if (f) list[count + __popc(m & ((1u << lane) - 1u))] = make_int2(c, p);
+            count += __popc(m);
+        }
+        if (lane == 0) s_count = count;
+    }
+    __syncthreads();
+    const int n = s_count;
+    __syncthreads();
+    return n;
+}
+
 __global__ void laswp_kernel(float *A, int64_t lda, int64_t plane, int64_t sA, int j0, int j1,
                              const int32_t *ipiv, int64_t sP, int c0, int c1, int forward) {
+    __shared__ int2 list[SWP_CHUNK];
     const int64_t b = blockIdx.y;
     const int j = j0 + blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= j1) return;
     float *col = A + b * sA + (int64_t)j * lda;
     const int32_t *pv = ipiv + b * sP;
-    if (forward) {
-        for (int c = c0; c < c1; ++c) {
-            const int p = pv[c];
-            if (p != c) {
-                cf t = ld(col, plane, c);
-                st(col, plane, c, ld(col, plane, p));
-                st(col, plane, p, t);
+    const int nch = (c1 - c0 + SWP_CHUNK - 1) / SWP_CHUNK;
+    for (int q = 0; q < nch; ++q) {
+        const int ch = forward ? q : nch - 1 - q;
+        const int lo = c0 + ch * SWP_CHUNK, hi = min(c1, lo + SWP_CHUNK);
+        const int cnt = compact_swaps(pv, lo, hi, list);
+        if (j < j1) {
+            for (int t = 0; t < cnt; ++t) {
+                const int2 e = list[forward ? t : cnt - 1 - t];
+                const cf x = ld(col, plane, e.x);
+                st(col, plane, e.x, ld(col, plane, e.y));
+                st(col, plane, e.y, x);
             }
         }
-    } else {
-        for (int c = c1 - 1; c >= c0; --c) {
-            const int p = pv[c];
-            if (p != c) {
-                cf t = ld(col, plane, c);
-                st(col, plane, c, ld(col, plane, p));
-                st(col, plane, p, t);
-            }
-        }
+        __syncthreads();
     }
 }
 
 __global__ void colswp_kernel(float *X, int64_t ldx, int64_t plane, int64_t sX, int m,
                               const int32_t *ipiv, int64_t sP, int n) {
+    __shared__ int2 list[SWP_CHUNK];
     const int64_t b = blockIdx.y;
     const int r = blockIdx.x * blockDim.x + threadIdx.x;
-    if (r >= m) return;
     float *x = X + b * sX + r;
     const int32_t *pv = ipiv + b * sP;
-    for (int c = n - 1; c >= 0; --c) {
-        const int p = pv[c];
-        if (p != c) {
-            cf t = ld(x, plane, (int64_t)c * ldx);
-            st(x, plane, (int64_t)c * ldx, ld(x, plane, (int64_t)p * ldx));
-            st(x, plane, (int64_t)p * ldx, t);
+    const int nch = (n + SWP_CHUNK - 1) / SWP_CHUNK;
+    for (int q = nch - 1; q >= 0; --q) {
+        const int lo = q * SWP_CHUNK, hi = min(n, lo + SWP_CHUNK);
+        const int cnt = compact_swaps(pv, lo, hi, list);
+        if (r < m) {
+            for (int t = cnt - 1; t >= 0; --t) {
+                const int2 e = list[t];
+                const cf v = ld(x, plane, (int64_t)e.x * ldx);
+                st(x, plane, (int64_t)e.x * ldx, ld(x, plane, (int64_t)e.y * ldx));
+                st(x, plane, (int64_t)e.y * ldx, v);
+            }
         }
+        __syncthreads();
     }
 }
 
@@ -949,6 +1023,18 @@ static int trsm_small(Ctx &c, int mode, int kb, CMatF T, CMatF B, int nvec) {
     return MNPB_OK;
 }
 
+static int dev_sms() {
+    static int n = 0;
+    if (n == 0) {
+        int dev = 0, v = 0;
+        n = (cudaGetDevice(&dev) == cudaSuccess &&
+             cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess && v > 0)
+                ? v
+                : 148;
+    }
+    return n;
+}
+
 static int split_point(int n) {
     int h = n / 2;
     h = (h / TS) * TS;
@@ -1081,20 +1167,30 @@ static int rgetrf(Ctx &c, int n, int off, int w, CMatF A, int32_t *ipiv, int64_t
     if (w <= TS) {
         ProfScope ps(c.s, PC_PANEL, 8.0 * w * w * (double)(n - off) * c.batch / 2);
         prof_tag("off=%d w=%d B=%d", off, w, c.batch);
-        constexpr int SW = 8;
-        const int64_t slab_bytes = (int64_t)SW * (n - off) * 8;
-        if (w % SW == 0 && w <= TS && slab_bytes <= 200 * 1024) {
-            static bool attr = false;
-            if (!attr) {
-                if (cudaFuncSetAttribute(panel_slab_kernel<SW>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         200 * 1024) != cudaSuccess) {
-                    set_error("panel_slab_kernel: cannot reserve shared memory");
-                    return MNPB_ECUDA;
-                }
-                attr = true;
+        static bool attr = false;
+        if (!attr) {
+            if (cudaFuncSetAttribute(panel_slab_kernel<8>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     200 * 1024) != cudaSuccess ||
+                cudaFuncSetAttribute(panel_slab_kernel<4>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     200 * 1024) != cudaSuccess) {
+                set_error("panel_slab_kernel: cannot reserve shared memory");
+                return MNPB_ECUDA;
             }
-            panel_slab_kernel<SW><<<c.batch, SLAB_THREADS, (size_t)slab_bytes, c.s>>>(
+            attr = true;
+        }
+        // more matrices than SMs: 4-column slabs, half the shared memory, so
+        // that two CTAs share an SM and the batch runs in one wave
+        const int64_t slab8 = (int64_t)8 * (n - off) * 8, slab4 = slab8 / 2;
+        if (c.batch > dev_sms() && w % 4 == 0 && w <= TS && slab4 <= 100 * 1024) {
+            panel_slab_kernel<4><<<c.batch, SLAB_THREADS, (size_t)slab4, c.s>>>(
+                n, off, w, A.p, A.ld, A.plane, A.stride, ipiv, sP, info);
+            MNPB_LAUNCH_CHECK("panel_slab_kernel<4>(f32)");
+            return MNPB_OK;
+        }
+        if (w % 8 == 0 && w <= TS && slab8 <= 200 * 1024) {
+            panel_slab_kernel<8><<<c.batch, SLAB_THREADS, (size_t)slab8, c.s>>>(
                 n, off, w, A.p, A.ld, A.plane, A.stride, ipiv, sP, info);
             MNPB_LAUNCH_CHECK("panel_slab_kernel(f32)");
             return MNPB_OK;

@@ -28,7 +28,7 @@ def rel(a, b):
 
 
 @pytest.mark.parametrize('n,batch,nrhs', [(32, 1, 1), (100, 2, 3), (256, 3, 5), (300, 1, 40),
-                                         (700, 2, 300), (130, 1, 130)])
+                                         (700, 2, 300), (130, 1, 130), (200, 150, 2)])
 def test_getrf_getrs_c32p(gpu_ok, n, batch, nrhs):
     ld = (n + 3) // 4 * 4
     g = torch.Generator().manual_seed(7)
