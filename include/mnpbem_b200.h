@@ -231,8 +231,9 @@ int64_t mnpb_bemret_refine_workspace(int64_t n, int64_t batch, int64_t nrhs);
  * entry until |dx| / |x| < tol (a forward-error test) or max_iter
  * corrections (MNPB_ENOCONV then).  b: excitation layout (phi, a, De,
  * alpha), x: solution layout (sig1, h1, sig2, h2), both [batch][8][nrhs][n]
- * c128, nrhs <= 4.  iters (corrections applied) and relres (final
- * |b - A x| / |b|): host arrays (batch). */
+ * c128, nrhs <= 4.  iters (corrections applied) and relres (|b - A x| / |b|
+ * of the iterate before the last correction, normally above the final
+ * one): host arrays (batch). */
 int mnpb_bemret_solve_refine(void *stream, int64_t n, int64_t batch, int64_t nrhs,
                              const float *G1p, const float *G2p, const float *S1p,
                              const float *Sp, const float *Dp, int64_t ld, const int32_t *piv,

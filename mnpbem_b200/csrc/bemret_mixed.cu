@@ -6,6 +6,9 @@
 // correction operator -- the structure the reference itself uses for its
 // preconditioned iterative solver (bem_ret_iter.py:1503-1634).
 #include "common.cuh"
+
+#include <mutex>
+#include <vector>
 #include "bemret_kernels.cuh"
 #include "dense_f32.cuh"
 
@@ -341,19 +344,10 @@ extern "C" int64_t mnpb_bemret_dinv_floats(int64_t n, int64_t batch) {
     return 6 * f32::diag_inv_floats((int)n, (int)batch);
 }
 
-extern "C" int mnpb_bemret_init_mixed(void *stream, int64_t n, int64_t batch, float *G1,
-                                      float *G2, float *H1, float *H2, float *D, int64_t ld,
-                                      const double *eps, const double *kvac, const double *nvec,
-                                      int32_t *piv, int32_t *info, float *dinv, void *work,
-                                      int64_t work_bytes) {
-    clear_error();
-    MNPB_REQUIRE(n > 0 && batch > 0 && batch < 65536 && n < 65536 && ld >= n && ld % 4 == 0,
-                 "bemret_init_mixed: bad sizes");
-    MNPB_REQUIRE(G1 && G2 && H1 && H2 && D && eps && kvac && nvec && piv && info && dinv && work,
-                 "bemret_init_mixed: null pointer");
-    MNPB_REQUIRE(work_bytes >= mnpb_bemret_workspace_mixed(n, batch),
-                 "bemret_init_mixed: workspace too small");
-    cudaStream_t s = as_stream(stream);
+static int init_mixed_body(cudaStream_t s, int64_t n, int64_t batch, float *G1, float *G2,
+                           float *H1, float *H2, float *D, int64_t ld, const double *eps,
+                           const double *kvac, const double *nvec, int32_t *piv, int32_t *info,
+                           float *dinv, void *work, int64_t work_bytes) {
     const int N = (int)n, B = (int)batch;
     const int64_t plane = ld * n, stride = 2 * plane;
     const int64_t tcw = align_up(tc::cgemm_tf32_workspace(N, N, 2 * B), 256);
@@ -394,6 +388,109 @@ extern "C" int mnpb_bemret_init_mixed(void *stream, int64_t n, int64_t batch, fl
     MNPB_TRY(f32::diag_inv(c, N, g1, dinv + dv.gL(0, B), dinv + dv.gU(0, B)));
     MNPB_TRY(f32::diag_inv(c, N, g2, dinv + dv.gL(1, B), dinv + dv.gU(1, B)));
     return f32::diag_inv(c, N, h2, dinv + dv.sL(B), dinv + dv.sU(B));
+}
+
+// The factorisation is ~2,000 launches whose arguments depend only on the
+// sizes and the buffer addresses, so it is replayed as a CUDA graph: the
+// first call with a given (sizes, addresses, device) runs normally, the
+// second is captured (thread-local capture mode), instantiated and launched,
+// later ones launch the instantiated graph.  Up to kGraphs such graphs are
+// kept (least recently used replaced).  Not used while the event profiler
+// records (its per-launch records come from the host-side launch sequence).
+namespace {
+struct InitKey {
+    const void *p[12];
+    int64_t n, batch, ld, work_bytes;
+    int dev;
+    bool operator==(const InitKey &o) const {
+        for (int i = 0; i < 12; ++i)
+            if (p[i] != o.p[i]) return false;
+        return n == o.n && batch == o.batch && ld == o.ld && work_bytes == o.work_bytes &&
+               dev == o.dev;
+    }
+};
+struct InitGraph {
+    InitKey key;
+    cudaGraphExec_t exec;   // null until captured
+    int64_t launches;       // kernels in the graph (for the launch counter)
+    uint64_t used;
+};
+constexpr int kGraphs = 4;
+std::mutex g_graph_mu;
+std::vector<InitGraph> g_graphs;
+uint64_t g_graph_clock = 0;
+}  // namespace
+
+extern "C" int mnpb_bemret_init_mixed(void *stream, int64_t n, int64_t batch, float *G1,
+                                      float *G2, float *H1, float *H2, float *D, int64_t ld,
+                                      const double *eps, const double *kvac, const double *nvec,
+                                      int32_t *piv, int32_t *info, float *dinv, void *work,
+                                      int64_t work_bytes) {
+    clear_error();
+    MNPB_REQUIRE(n > 0 && batch > 0 && batch < 65536 && n < 65536 && ld >= n && ld % 4 == 0,
+                 "bemret_init_mixed: bad sizes");
+    MNPB_REQUIRE(G1 && G2 && H1 && H2 && D && eps && kvac && nvec && piv && info && dinv && work,
+                 "bemret_init_mixed: null pointer");
+    MNPB_REQUIRE(work_bytes >= mnpb_bemret_workspace_mixed(n, batch),
+                 "bemret_init_mixed: workspace too small");
+    cudaStream_t s = as_stream(stream);
+    auto body = [&]() {
+        return init_mixed_body(s, n, batch, G1, G2, H1, H2, D, ld, eps, kvac, nvec, piv, info,
+                               dinv, work, work_bytes);
+    };
+    if (prof_on()) return body();
+    InitKey key{{G1, G2, H1, H2, D, eps, kvac, nvec, piv, info, dinv, work},
+                n, batch, ld, work_bytes, 0};
+    if (cudaGetDevice(&key.dev) != cudaSuccess) return body();
+    std::lock_guard<std::mutex> lk(g_graph_mu);
+    InitGraph *hit = nullptr;
+    for (auto &g : g_graphs)
+        if (g.key == key) hit = &g;
+    if (!hit) {
+        // first sighting: remember the key, run normally
+        if ((int)g_graphs.size() >= kGraphs) {
+            auto lru = g_graphs.begin();
+            for (auto it = g_graphs.begin(); it != g_graphs.end(); ++it)
+                if (it->used < lru->used) lru = it;
+            if (lru->exec) cudaGraphExecDestroy(lru->exec);
+            g_graphs.erase(lru);
+        }
+        g_graphs.push_back(InitGraph{key, nullptr, 0, ++g_graph_clock});
+        return body();
+    }
+    hit->used = ++g_graph_clock;
+    if (!hit->exec) {
+        if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+            cudaGetLastError();
+            return body();
+        }
+        const int64_t l0 = g_launches.load();
+        const int rc = body();
+        cudaGraph_t graph = nullptr;
+        const cudaError_t ec = cudaStreamEndCapture(s, &graph);
+        hit->launches = g_launches.load() - l0;
+        g_launches.fetch_sub(hit->launches);   // counted again when the graph runs
+        if (rc != MNPB_OK || ec != cudaSuccess || !graph) {
+            if (graph) cudaGraphDestroy(graph);
+            cudaGetLastError();
+            return rc != MNPB_OK ? rc : body();
+        }
+        cudaGraphExec_t exec = nullptr;
+        const cudaError_t ei = cudaGraphInstantiate(&exec, graph, 0);
+        cudaGraphDestroy(graph);
+        if (ei != cudaSuccess) {
+            cudaGetLastError();
+            return body();
+        }
+        hit->exec = exec;
+    }
+    if (cudaGraphLaunch(hit->exec, s) != cudaSuccess) {
+        set_error("bemret_init_mixed: graph launch failed: %s",
+                  cudaGetErrorString(cudaGetLastError()));
+        return MNPB_ECUDA;
+    }
+    count_launch(hit->launches);
+    return MNPB_OK;
 }
 
 extern "C" int64_t mnpb_bemret_refine_workspace(int64_t n, int64_t batch, int64_t nrhs) {
@@ -446,7 +543,7 @@ extern "C" int mnpb_bemret_solve_refine(
     cd *r = (cd *)take(batch * per * 8 * 16);
     cd *dx = (cd *)take(batch * per * 8 * 16);
     cd *P = (cd *)take(batch * per * 4 * 4 * 16);
-    double *nrm = (double *)take(batch * 2 * 8);
+    double *nrm = (double *)take(batch * 4 * 8);
     F.trsv_state = (int *)take(f32::trsv_state_bytes(N, B));
     const int64_t tcw = (int64_t)((char *)work + work_bytes - wp);
     f32::Ctx c(s, B, (float *)wp, tcw);
@@ -456,9 +553,12 @@ extern "C" int mnpb_bemret_solve_refine(
     cd *xx = (cd *)x;
 
     MNPB_TRY(msolve(c, N, k, F, eps, kvac, nvec, bb, xx, scr, fscr));
-    std::vector<double> hn(2 * batch);
+    std::vector<double> hn(4 * batch);
     std::vector<int> done(batch, 0);
-    for (int b = 0; b < B; ++b) iters[b] = 0;
+    for (int b = 0; b < B; ++b) {
+        iters[b] = 0;
+        relres[b] = 0.0;
+    }
     const int64_t sG = ld * n;   // c128 matrices use the same leading dimension
     // r = b - A x on entries [e0, B) (residual vectors at r + e0 * sx)
     auto residual = [&](int e0) -> int {
@@ -492,12 +592,15 @@ extern "C" int mnpb_bemret_solve_refine(
         MNPB_LAUNCH_CHECK("residual_kernel");
         return MNPB_OK;
     };
-    // per entry of [e0, B): |u|^2 and |v|^2 to the host (hn[2 i], hn[2 i + 1])
-    auto norms = [&](int e0, const cd *u, const cd *v) -> int {
+    // per entry of [e0, B): |dx|^2, |x|^2 (hn[2 i], hn[2 i + 1]) and |r|^2, |b|^2
+    // (hn[2 Bp + 2 i], hn[2 Bp + 2 i + 1]) to the host
+    auto norms = [&](int e0) -> int {
         const int Bp = B - e0;
-        norms_kernel<<<Bp, 256, 0, s>>>(sx, u + (int64_t)e0 * sx, v + (int64_t)e0 * sx, sx, nrm);
+        norms_kernel<<<Bp, 256, 0, s>>>(sx, dx + (int64_t)e0 * sx, xx + (int64_t)e0 * sx, sx, nrm);
+        norms_kernel<<<Bp, 256, 0, s>>>(sx, r + (int64_t)e0 * sx, bb + (int64_t)e0 * sx, sx,
+                                        nrm + 2 * Bp);
         MNPB_LAUNCH_CHECK("norms_kernel");
-        if (cudaMemcpyAsync(hn.data(), nrm, sizeof(double) * 2 * Bp, cudaMemcpyDeviceToHost, s) !=
+        if (cudaMemcpyAsync(hn.data(), nrm, sizeof(double) * 4 * Bp, cudaMemcpyDeviceToHost, s) !=
                 cudaSuccess ||
             cudaStreamSynchronize(s) != cudaSuccess) {
             set_error("bemret_solve_refine: norm copy failed");
@@ -524,23 +627,23 @@ extern "C" int mnpb_bemret_solve_refine(
                                                                     dx + (int64_t)b0 * sx,
                                                                     xx + (int64_t)b0 * sx);
         MNPB_LAUNCH_CHECK("axpy_kernel");
-        MNPB_TRY(norms(b0, dx, xx));
+        MNPB_TRY(norms(b0));
         all = true;
         for (int i = 0; i < Bp; ++i) {
             const int b = b0 + i;
             if (done[b]) continue;
             iters[b] = it + 1;
+            relres[b] = hn[2 * Bp + 2 * i + 1] > 0
+                            ? std::sqrt(hn[2 * Bp + 2 * i] / hn[2 * Bp + 2 * i + 1])
+                            : 0.0;
             const double rel = hn[2 * i + 1] > 0 ? std::sqrt(hn[2 * i] / hn[2 * i + 1]) : 0.0;
             if (rel < tol) done[b] = 1;
             if (!done[b]) all = false;
         }
         while (b0 < B && done[b0]) ++b0;
     }
-    // final relative residuals of every entry
-    MNPB_TRY(residual(0));
-    MNPB_TRY(norms(0, r, bb));
-    for (int b = 0; b < B; ++b)
-        relres[b] = hn[2 * b + 1] > 0 ? std::sqrt(hn[2 * b] / hn[2 * b + 1]) : 0.0;
+    // relres holds each entry's relative residual before its last correction
+    // (no extra pass over the FP64 operator just to report the final one)
     int terr = 0;
     MNPB_TRY(f32::trsv_error_read_and_clear(s, &terr));
     if (terr) {

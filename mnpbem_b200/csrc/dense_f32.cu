@@ -9,6 +9,8 @@
 #include "common.cuh"
 #include "dense_f32.cuh"
 
+#include <cuda.h>
+
 namespace mnpb {
 namespace f32 {
 
@@ -965,6 +967,325 @@ __global__ void __launch_bounds__(RL_THREADS) trsv_rl_kernel(int n, int m, int l
     }
 }
 
+// ---- few-RHS triangular solve with the triangle streamed by TMA ------------
+//
+// One CTA per matrix; the right-hand sides r (n x NC) stay in shared memory.
+// Warp 9 (one lane) streams the triangle block column by block column in the
+// order the solve consumes it: for 32-column block j, the inverse of its
+// diagonal block (8 KB, bulk copy) and then every 128-row tile the block
+// updates (below it for L, above it, bottom tile first, for U), through a
+// ring of S stages; it runs ahead of the arithmetic, bounded only by the
+// ring.  Warp 8 solves the diagonal blocks (x_j = D_j^{-1} r_j) into a double
+// buffer as soon as the first tile of the previous block has updated block
+// j's rows; warps 0-7 update r with each tile: thread t takes row t % 128 and
+// half of the tile's 32 columns (t / 128); the second half's partial sums
+// meet the first half's through a double buffer in shared memory.  Every
+// mbarrier wait is bounded; on a timeout the kernel records an error in
+// g_trsv_error and stops.
+constexpr int STR_ROWS = 128;                                  // rows per tile
+constexpr int STR_TILE_BYTES = 2 * TB * STR_ROWS * 4;          // re + im planes
+constexpr int STR_CONS = 256;                                  // consumer threads
+constexpr int STR_THREADS = STR_CONS + 64;
+constexpr uint64_t STR_WAIT_NS = 1000000000ull;
+
+__device__ __forceinline__ uint32_t s_u32(const void *p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void sbar_init(uint32_t bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count));
+}
+__device__ __forceinline__ void sbar_expect(uint32_t bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void sbar_arrive(uint32_t bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+__device__ __forceinline__ bool sbar_wait(uint32_t bar, uint32_t parity) {
+    const uint64_t t0 = gtimer();
+    while (true) {
+        uint32_t ok;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(ok)
+            : "r"(bar), "r"(parity)
+            : "memory");
+        if (ok) return true;
+        if (gtimer() - t0 > STR_WAIT_NS) return false;
+    }
+}
+__device__ __forceinline__ void s_tma3(uint32_t dst, const CUtensorMap *map, uint32_t bar, int c0,
+                                       int c1, int c2) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes "
+        "[%0], [%1, {%3, %4, %5}], [%2];" ::"r"(dst),
+        "l"((uint64_t)map), "r"(bar), "r"(c0), "r"(c1), "r"(c2)
+        : "memory");
+}
+__device__ __forceinline__ void s_bulk(uint32_t dst, const void *src, uint32_t bytes,
+                                       uint32_t bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
+            "r"(dst),
+        "l"((uint64_t)src), "r"(bytes), "r"(bar)
+        : "memory");
+}
+
+template <int NC>
+__global__ void __launch_bounds__(STR_THREADS, 1)
+    trsv_stream_kernel(const __grid_constant__ CUtensorMap tmRe,
+                       const __grid_constant__ CUtensorMap tmIm, int n, int m, int lower,
+                       const float *__restrict__ Dinv, float *X, int64_t ldx, int64_t planeX,
+                       int64_t sX, int nb, int S) {
+    extern __shared__ __align__(1024) unsigned char str_raw[];
+    unsigned char *sm = (unsigned char *)(((uintptr_t)str_raw + 1023) & ~(uintptr_t)1023);
+    float *ring = (float *)sm;                                        // S tiles
+    float *dsm = (float *)(sm + (size_t)S * STR_TILE_BYTES);          // 2 x [2][32][32]
+    cf *xb = (cf *)(dsm + 2 * 2 * TB * TB);                           // 2 x [32][NC]
+    cf *red = xb + 2 * TB * NC;                                       // 2 x [128][NC]
+    cf *r = red + 2 * STR_ROWS * NC;                                  // [n][NC]
+    uint64_t *bars = (uint64_t *)(r + (size_t)n * NC);
+    // bars: full[S], empty[S], dfull[2], dempty[2], rows_ready, xready[2],
+    // red_full[2], red_empty[2]
+    uint64_t *full = bars, *empty = bars + S, *dfull = bars + 2 * S, *dempty = dfull + 2;
+    uint64_t *rows_ready = dempty + 2, *xready = rows_ready + 1;
+    uint64_t *red_full = xready + 2, *red_empty = red_full + 2;
+    volatile int *abort_flag = (volatile int *)(red_empty + 2);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int64_t b = blockIdx.x;
+    X += b * sX;
+    const float *Db = Dinv + b * nb * 2 * TB * TB;
+
+    for (int e = tid; e < n * NC; e += STR_THREADS) {
+        const int i = e % n, c = e / n;
+        r[i * NC + c] = c < m ? ld(X, planeX, (int64_t)c * ldx + i) : fmk(0.f, 0.f);
+    }
+    if (tid == 0) {
+        for (int q = 0; q < S; ++q) {
+            sbar_init(s_u32(&full[q]), 1);
+            sbar_init(s_u32(&empty[q]), STR_CONS);
+        }
+        for (int q = 0; q < 2; ++q) {
+            sbar_init(s_u32(&dfull[q]), 1);
+            sbar_init(s_u32(&dempty[q]), 1);
+            sbar_init(s_u32(&xready[q]), 1);
+            sbar_init(s_u32(&red_full[q]), STR_CONS / 2);
+            sbar_init(s_u32(&red_empty[q]), STR_CONS / 2);
+        }
+        sbar_init(s_u32(rows_ready), STR_ROWS);
+        *abort_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+
+    // tile t of block j: first row and row range [lo, hi) that the block updates
+    auto range = [&](int j, int &lo, int &hi) {
+        if (lower) {
+            lo = (j + 1) * TB;
+            hi = n;
+        } else {
+            lo = 0;
+            hi = j * TB;
+        }
+        if (lo > hi) lo = hi;
+    };
+    auto tile_row = [&](int lo, int hi, int t) {
+        return lower ? lo + t * STR_ROWS : hi - (t + 1) * STR_ROWS;
+    };
+    auto fail = [&](int code) {
+        atomicCAS(&g_trsv_error, 0, code);
+        *abort_flag = 1;
+    };
+
+    if (warp == 9) {
+        if (lane == 0) {
+            uint32_t g = 0;
+            // the inverse of block jj's diagonal block; block jj + 1's is
+            // requested right after the first tile of block jj, so that the
+            // diagonal solve never waits for it
+            auto load_dinv = [&](int jj) -> bool {
+                const int j = lower ? jj : nb - 1 - jj, buf = jj & 1;
+                if (jj >= 2 && !sbar_wait(s_u32(&dempty[buf]), ((jj - 2) >> 1) & 1)) {
+                    fail(11);
+                    return false;
+                }
+                sbar_expect(s_u32(&dfull[buf]), 2 * TB * TB * 4);
+                s_bulk(s_u32(dsm + buf * 2 * TB * TB), Db + (int64_t)j * 2 * TB * TB,
+                       2 * TB * TB * 4, s_u32(&dfull[buf]));
+                return true;
+            };
+            bool ok = load_dinv(0);
+            for (int jj = 0; jj < nb && ok && !*abort_flag; ++jj) {
+                const int j = lower ? jj : nb - 1 - jj;
+                int lo, hi;
+                range(j, lo, hi);
+                const int nt = (hi - lo + STR_ROWS - 1) / STR_ROWS;
+                for (int t = 0; t < nt; ++t, ++g) {
+                    const int q = g % S;
+                    if (g >= (uint32_t)S && !sbar_wait(s_u32(&empty[q]), ((g / S) - 1) & 1)) {
+                        fail(12);
+                        ok = false;
+                        break;
+                    }
+                    const uint32_t dst = s_u32(ring) + q * STR_TILE_BYTES;
+                    sbar_expect(s_u32(&full[q]), STR_TILE_BYTES);
+                    s_tma3(dst, &tmRe, s_u32(&full[q]), tile_row(lo, hi, t), j * TB, (int)b);
+                    s_tma3(dst + STR_TILE_BYTES / 2, &tmIm, s_u32(&full[q]), tile_row(lo, hi, t),
+                           j * TB, (int)b);
+                    if (t == 0 && jj + 1 < nb && !load_dinv(jj + 1)) {
+                        ++g;
+                        ok = false;
+                        break;
+                    }
+                }
+            }
+            // copies still in flight (only after an abort): wait for them, bounded
+            if (*abort_flag) {
+                const uint32_t first = g > (uint32_t)S ? g - S : 0;
+                for (uint32_t h = first; h < g; ++h)
+                    sbar_wait(s_u32(&full[h % S]), (h / S) & 1);
+                for (int q = 0; q < 2 && q < nb; ++q) {
+                    // last use of each inverse buffer: jl = largest block index with jl % 2 == q
+                    const int jl = ((nb - 1 - q) / 2) * 2 + q;
+                    sbar_wait(s_u32(&dfull[q]), (jl >> 1) & 1);
+                }
+            }
+        }
+    } else if (warp == 8) {
+        for (int jj = 0; jj < nb && !*abort_flag; ++jj) {
+            const int j = lower ? jj : nb - 1 - jj, buf = jj & 1;
+            const int r0 = j * TB, rows = min(TB, n - r0);
+            if (jj >= 1 && !sbar_wait(s_u32(rows_ready), (jj - 1) & 1)) {
+                if (lane == 0) fail(13);
+                break;
+            }
+            if (!sbar_wait(s_u32(&dfull[buf]), (jj >> 1) & 1)) {
+                if (lane == 0) fail(14);
+                break;
+            }
+            const float *Dr = dsm + buf * 2 * TB * TB, *Di = Dr + TB * TB;
+            cf *xo = xb + buf * TB * NC;
+            cf y[NC];
+#pragma unroll
+            for (int c = 0; c < NC; ++c) y[c] = fmk(0.f, 0.f);
+            if (lane < rows) {
+#pragma unroll 4
+                for (int k = 0; k < rows; ++k) {
+                    const cf d = fmk(Dr[k * TB + lane], Di[k * TB + lane]);
+#pragma unroll
+                    for (int c = 0; c < NC; ++c) {
+                        const cf v = r[(r0 + k) * NC + c];
+                        y[c].x = fmaf(d.x, v.x, y[c].x);
+                        y[c].x = fmaf(-d.y, v.y, y[c].x);
+                        y[c].y = fmaf(d.x, v.y, y[c].y);
+                        y[c].y = fmaf(d.y, v.x, y[c].y);
+                    }
+                }
+            }
+#pragma unroll
+            for (int c = 0; c < NC; ++c) {
+                if (c >= m) y[c] = fmk(0.f, 0.f);
+                if (lane < rows && c < m) st(X, planeX, (int64_t)c * ldx + r0 + lane, y[c]);
+                xo[lane * NC + c] = y[c];
+            }
+            __syncwarp();
+            if (lane == 0) {
+                sbar_arrive(s_u32(&xready[buf]));
+                sbar_arrive(s_u32(&dempty[buf]));
+            }
+        }
+    } else {
+        // warps 0-7: row tid % 128 of each tile, columns [16 h, 16 h + 16), h = tid / 128
+        const int row = tid & (STR_ROWS - 1), h = tid >> 7;
+        uint32_t g = 0;
+        for (int jj = 0; jj < nb && !*abort_flag; ++jj) {
+            const int j = lower ? jj : nb - 1 - jj, buf = jj & 1;
+            if (!sbar_wait(s_u32(&xready[buf]), (jj >> 1) & 1)) {
+                fail(15);
+                break;
+            }
+            const cf *xj = xb + buf * TB * NC;
+            int lo, hi;
+            range(j, lo, hi);
+            const int nt = (hi - lo + STR_ROWS - 1) / STR_ROWS;
+            bool ok = true;
+            for (int t = 0; t < nt; ++t, ++g) {
+                const int q = g % S;
+                if (!sbar_wait(s_u32(&full[q]), (g / S) & 1)) {
+                    fail(16);
+                    ok = false;
+                    break;
+                }
+                const float *tr = ring + (size_t)q * (STR_TILE_BYTES / 4), *ti = tr + TB * STR_ROWS;
+                cf acc[NC];
+#pragma unroll
+                for (int c = 0; c < NC; ++c) acc[c] = fmk(0.f, 0.f);
+#pragma unroll
+                for (int kk = 0; kk < TB / 2; ++kk) {
+                    const int k = 16 * h + kk;
+                    const float ar = tr[k * STR_ROWS + row], ai = ti[k * STR_ROWS + row];
+                    cf x[NC];
+                    if (NC % 2 == 0) {
+#pragma unroll
+                        for (int c = 0; c < NC; c += 2) {
+                            const float4 v = *reinterpret_cast<const float4 *>(xj + k * NC + c);
+                            x[c] = fmk(v.x, v.y);
+                            x[c + 1] = fmk(v.z, v.w);
+                        }
+                    } else {
+#pragma unroll
+                        for (int c = 0; c < NC; ++c) x[c] = xj[k * NC + c];
+                    }
+#pragma unroll
+                    for (int c = 0; c < NC; ++c) {
+                        acc[c].x = fmaf(ar, x[c].x, acc[c].x);
+                        acc[c].x = fmaf(-ai, x[c].y, acc[c].x);
+                        acc[c].y = fmaf(ar, x[c].y, acc[c].y);
+                        acc[c].y = fmaf(ai, x[c].x, acc[c].y);
+                    }
+                }
+                sbar_arrive(s_u32(&empty[q]));   // this thread's reads of the tile are done
+                // second half -> first half through a double buffer (bounded waits)
+                const int rbuf = g & 1;
+                cf *rb = red + rbuf * STR_ROWS * NC;
+                if (h == 1) {
+                    if (g >= 2 && !sbar_wait(s_u32(&red_empty[rbuf]), ((g >> 1) - 1) & 1)) {
+                        fail(17);
+                        ok = false;
+                        break;
+                    }
+#pragma unroll
+                    for (int c = 0; c < NC; ++c) rb[row * NC + c] = acc[c];
+                    sbar_arrive(s_u32(&red_full[rbuf]));
+                } else {
+                    if (!sbar_wait(s_u32(&red_full[rbuf]), (g >> 1) & 1)) {
+                        fail(18);
+                        ok = false;
+                        break;
+                    }
+                    const int i = tile_row(lo, hi, t) + row;
+                    cf o[NC];
+#pragma unroll
+                    for (int c = 0; c < NC; ++c) o[c] = rb[row * NC + c];
+                    sbar_arrive(s_u32(&red_empty[rbuf]));
+                    if (i >= lo && i < hi) {
+#pragma unroll
+                        for (int c = 0; c < NC; ++c) {
+                            cf &u = r[i * NC + c];
+                            u.x -= acc[c].x + o[c].x;
+                            u.y -= acc[c].y + o[c].y;
+                        }
+                    }
+                    if (t == 0 && jj < nb - 1) sbar_arrive(s_u32(rows_ready));
+                }
+            }
+            if (!ok) break;
+        }
+    }
+}
+
 __global__ void set_identity_kernel(float *W, int64_t ldw, int64_t plane, int64_t sW, int n) {
     const int64_t b = blockIdx.z;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1273,8 +1594,57 @@ static int trsv_rl(Ctx &c, bool lower, int n, int m, CMatF T, const float *inv, 
     return MNPB_OK;
 }
 
+// Shared memory of trsv_stream_kernel<NC> with S ring stages (0 if too large).
+static int stream_smem(int n, int nc, int S) {
+    const int64_t b = 1024 + (int64_t)S * STR_TILE_BYTES + 2 * 2 * TB * TB * 4 +
+                      2 * TB * nc * (int64_t)sizeof(cf) + 2 * STR_ROWS * nc * (int64_t)sizeof(cf) +
+                      (int64_t)n * nc * sizeof(cf) + (2 * S + 11) * 8 + 16;
+    return b <= 220 * 1024 ? (int)b : 0;
+}
+
+template <int NC>
+static int trsv_stream(Ctx &c, bool lower, int n, int m, CMatF T, const float *inv, CMatF X,
+                       int S) {
+    const int nb = ceil_div(n, TB);
+    const int smem = stream_smem(n, NC, S);
+    static int attr_bytes = 0;
+    if (smem > attr_bytes) {
+        if (cudaFuncSetAttribute(trsv_stream_kernel<NC>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, smem) !=
+            cudaSuccess) {
+            set_error("trsv_stream_kernel: cannot reserve %d bytes of shared memory", smem);
+            return MNPB_ECUDA;
+        }
+        attr_bytes = smem;
+    }
+    CUtensorMap mr, mi;
+    const uint64_t dims[3] = {(uint64_t)n, (uint64_t)n, (uint64_t)c.batch};
+    const uint64_t strides[2] = {(uint64_t)T.ld * 4, (uint64_t)T.stride * 4};
+    const uint32_t box[3] = {STR_ROWS, TB, 1};
+    MNPB_TRY(tc::encode_map_f32(&mr, T.p, dims, strides, box, 0));
+    MNPB_TRY(tc::encode_map_f32(&mi, T.p + T.plane, dims, strides, box, 0));
+    ProfScope ps(c.s, PC_TRSV, 4.0 * (double)n * n * c.batch);   // bytes of the triangle
+    prof_tag("n=%d m=%d B=%d %s stream", n, m, c.batch, lower ? "L" : "U");
+    trsv_stream_kernel<NC><<<c.batch, STR_THREADS, smem, c.s>>>(
+        mr, mi, n, m, lower ? 1 : 0, inv, X.p, X.ld, X.plane, X.stride, nb, S);
+    MNPB_LAUNCH_CHECK("trsv_stream_kernel");
+    return MNPB_OK;
+}
+
 static int trsv(Ctx &c, bool lower, int n, int m, CMatF T, const float *inv, CMatF X,
                 int *state) {
+    // triangle streamed by TMA when it is 16-byte aligned and the ring fits
+    // beside the right-hand sides in shared memory
+    const bool a16 = ((uintptr_t)T.p & 15) == 0 && T.ld % 4 == 0 && T.plane % 4 == 0 &&
+                     T.stride % 4 == 0 && ((uintptr_t)inv & 15) == 0;
+    if (a16 && m <= 4) {
+        const int nc = m <= 1 ? 1 : 4;
+        int S = 6;
+        while (S >= 2 && stream_smem(n, nc, S) == 0) --S;
+        if (S >= 2)
+            return nc == 1 ? trsv_stream<1>(c, lower, n, m, T, inv, X, S)
+                           : trsv_stream<4>(c, lower, n, m, T, inv, X, S);
+    }
     // one CTA per matrix when the right-hand sides fit in shared memory and
     // the triangle allows 8-byte row-pair loads
     const bool even = ((uintptr_t)T.p & 7) == 0 && T.ld % 2 == 0 && T.plane % 2 == 0 &&

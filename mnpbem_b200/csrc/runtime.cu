@@ -135,7 +135,9 @@ extern "C" int mnpb_prof_end(int ncls, double *ms, double *work, int64_t *count)
     return MNPB_OK;
 }
 
-// Write the launches of the last profiled interval as CSV (class, ms, work, tag).
+// Write the launches of the last profiled interval as CSV (class, ms, work,
+// gap_ms = device time from the previous record's end to this record's start,
+// i.e. idle time plus work launched outside the library, tag).
 extern "C" int mnpb_prof_dump(const char *path) {
     clear_error();
     FILE *f = fopen(path, "w");
@@ -143,11 +145,13 @@ extern "C" int mnpb_prof_dump(const char *path) {
         set_error("prof_dump: cannot open %s", path);
         return MNPB_EINVAL;
     }
-    fprintf(f, "class,ms,work,tag\n");
-    for (auto &r : g_last) {
-        float t = 0.f;
+    fprintf(f, "class,ms,work,gap_ms,tag\n");
+    for (size_t i = 0; i < g_last.size(); ++i) {
+        const Rec &r = g_last[i];
+        float t = 0.f, g = 0.f;
         cudaEventElapsedTime(&t, r.a, r.b);
-        fprintf(f, "%d,%.6f,%.6g,%s\n", r.cls, t, r.work, r.tag);
+        if (i > 0) cudaEventElapsedTime(&g, g_last[i - 1].b, r.a);
+        fprintf(f, "%d,%.6f,%.6g,%.6f,%s\n", r.cls, t, r.work, g, r.tag);
     }
     fclose(f);
     return MNPB_OK;

@@ -716,6 +716,31 @@ static int make_map(CUtensorMap *map, const float *base, uint64_t d0, uint64_t d
     return MNPB_OK;
 }
 
+int encode_map_f32(void *map, const float *base, const uint64_t dims[3],
+                   const uint64_t stride_bytes[2], const uint32_t box[3], int swizzle) {
+    EncodeFn enc = get_encode();
+    if (!enc) {
+        set_error("tma: cuTensorMapEncodeTiled unavailable");
+        return MNPB_ECUDA;
+    }
+    if (((uintptr_t)base & 15) || (stride_bytes[0] & 15) || (stride_bytes[1] & 15)) {
+        set_error("tma: operand not 16-byte aligned (base %p)", base);
+        return MNPB_EINVAL;
+    }
+    cuuint64_t d[3] = {dims[0], dims[1], dims[2]};
+    cuuint64_t st[2] = {stride_bytes[0], stride_bytes[1]};
+    cuuint32_t bx[3] = {box[0], box[1], box[2]};
+    cuuint32_t es[3] = {1, 1, 1};
+    CUresult r = enc((CUtensorMap *)map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, (void *)base, d, st,
+                     bx, es, CU_TENSOR_MAP_INTERLEAVE_NONE, (CUtensorMapSwizzle)swizzle,
+                     CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) {
+        set_error("tma: cuTensorMapEncodeTiled failed (%d)", (int)r);
+        return MNPB_ECUDA;
+    }
+    return MNPB_OK;
+}
+
 static int num_sms() {
     static int n = 0;
     if (n == 0) {

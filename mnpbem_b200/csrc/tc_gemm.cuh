@@ -28,5 +28,11 @@ int cgemm_tf32(cudaStream_t s, int M, int N, int K, int batch, float alpha, CMat
                bool a_tf32 = false);
 int tc_error_read_and_clear(cudaStream_t s, int *code);
 
+// 3-D FP32 TMA descriptor (written into the 128-byte CUtensorMap storage at
+// map): dims[0] contiguous, byte strides of dims 1 and 2, box, swizzle as
+// CUtensorMapSwizzle.  Checks the 16-byte rules of base and strides.
+int encode_map_f32(void *map, const float *base, const uint64_t dims[3],
+                   const uint64_t stride_bytes[2], const uint32_t box[3], int swizzle);
+
 }  // namespace tc
 }  // namespace mnpb
