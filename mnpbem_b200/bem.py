@@ -93,6 +93,8 @@ class _MixedBatch(object):
         self.dinv = torch.empty(int(_lib.lib().mnpb_bemret_dinv_floats(n, B)), **f32)
         wb = int(_lib.lib().mnpb_bemret_workspace_mixed(n, B))
         self.work = torch.empty(wb, dtype=torch.uint8, device=dev)
+        self.eps = torch.empty((B, 4), dtype=torch.float64, device=dev)
+        self.kvac = torch.empty(B, dtype=torch.float64, device=dev)
         self.iters = None
         self.relres = None
 
@@ -138,7 +140,7 @@ class BEMRet(object):
             kvac[b] = 2 * np.pi / enei
         return eps, kvac
 
-    def _factor(self, eneis, stream=None):
+    def _factor(self, eneis, stream=None, reuse=True):
         t = self.tables
         n, B = t.n, len(eneis)
         kblk, sblk = t.k_tables(eneis)
@@ -153,7 +155,7 @@ class BEMRet(object):
                  ptr(bt.H2), ptr(bt.D), n, n * n, ptr(bt.eps), ptr(bt.kvac), ptr(t.nvec),
                  ptr(bt.piv), ptr(bt.info), ptr(bt.work), bt.work.numel())
             return bt
-        bt = _MixedBatch(t, eneis)
+        bt = self._mixed_batch(eneis, stream) if reuse else _MixedBatch(t, eneis)
         ld = bt.ld
         d_k = torch.from_numpy(np.ascontiguousarray(kblk)).to(t.device)
         d_s = torch.from_numpy(np.ascontiguousarray(sblk)).to(t.device)
@@ -162,18 +164,36 @@ class BEMRet(object):
              ptr(poff), ptr(d_k), ptr(d_s), t.nref, ptr(t.rows), ptr(t.cols), ptr(t.g),
              ptr(t.fn), ptr(bt.G1), ptr(bt.H1), ptr(bt.G2), ptr(bt.H2), ld, ld * n,
              ptr(bt.G1p), ptr(bt.H1p), ptr(bt.G2p), ptr(bt.H2p), ld, 2 * ld * n, ld * n)
-        bt.eps = torch.from_numpy(eps).to(t.device)
-        bt.kvac = torch.from_numpy(kvac).to(t.device)
+        bt.eps.copy_(torch.from_numpy(np.ascontiguousarray(eps)).view(B, 4))
+        bt.kvac.copy_(torch.from_numpy(np.ascontiguousarray(kvac)).view(B))
         call('mnpb_bemret_init_mixed', sh, n, B, ptr(bt.G1p), ptr(bt.G2p), ptr(bt.H1p),
              ptr(bt.H2p), ptr(bt.Dp), ld, ptr(bt.eps), ptr(bt.kvac), ptr(t.nvec), ptr(bt.piv),
              ptr(bt.info), ptr(bt.dinv), ptr(bt.work), bt.work.numel())
+        return bt
+
+    def _mixed_batch(self, eneis, stream):
+        """Device buffers for a mixed batch.  The latest batch's buffers are
+        kept and handed out again to the next batch of the same size on the
+        same stream (stream order makes the reuse safe), so that the
+        factorisation's launch sequence sees the same addresses and the
+        library replays it as a CUDA graph."""
+        key = (len(eneis), _lib.stream_handle(stream).value)
+        cached = getattr(self, '_mixed_cache', None)
+        if cached is not None and cached[0] == key:
+            bt = cached[1]
+            bt.eneis = list(eneis)
+            bt.iters, bt.relres = None, None
+            return bt
+        self._mixed_cache = None       # release the old buffers before allocating
+        bt = _MixedBatch(self.tables, eneis)
+        self._mixed_cache = (key, bt)
         return bt
 
     def init(self, enei):
         """Matrices for wavelength ``enei``; no-op if already there (bem_ret.py:293-311)."""
         if self.enei is not None and np.isclose(self.enei, enei):
             return self
-        self._batch = self._factor([enei])
+        self._batch = self._factor([enei], reuse=False)   # kept across solve() calls
         info = self._batch.info.cpu().numpy()
         if info.any():
             raise _lib.MNPBError('BEMRet.init', 3, "zero pivot at column {}".format(int(info.max())))
