@@ -349,7 +349,13 @@ class BEMRet(object):
             bt = self._factor(chunk, stream=st)
             pots, K = self._spectrum_pots(exc, chunk, st)
             xout = self._solve_batch(bt, pots, K, stream=st)
-            return xout.cpu().numpy(), K
+            # device -> pinned host copy (page-locked: full PCIe rate), then a
+            # numpy view of it
+            host = torch.empty(xout.shape, dtype=xout.dtype, pin_memory=True)
+            with torch.cuda.stream(st):
+                host.copy_(xout, non_blocking=True)
+            st.synchronize()
+            return host.numpy(), K
 
         if streams > 1:
             res = self.pipeline(chunks, work, streams)
