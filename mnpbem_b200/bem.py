@@ -364,8 +364,17 @@ class BEMRet(object):
             res = [work(c, cur) for c in chunks]
         out = []
         for chunk, (x, K) in zip(chunks, res):
+            # one reordering copy per field for the whole chunk; each
+            # wavelength's fields are contiguous views of it
+            sig1 = np.ascontiguousarray(x[:, 0].transpose(0, 2, 1))        # (B, n, K)
+            sig2 = np.ascontiguousarray(x[:, 4].transpose(0, 2, 1))
+            h1 = np.ascontiguousarray(x[:, 1:4].transpose(0, 3, 1, 2))    # (B, n, 3, K)
+            h2 = np.ascontiguousarray(x[:, 5:8].transpose(0, 3, 1, 2))
+            if K == 1:
+                sig1, sig2, h1, h2 = sig1[..., 0], sig2[..., 0], h1[..., 0], h2[..., 0]
             for b, enei in enumerate(chunk):
-                out.append(self._to_compstruct(x[b], K, enei))
+                out.append(CompStruct(self.p, enei, sig1=sig1[b], sig2=sig2[b], h1=h1[b],
+                                      h2=h2[b]))
         return out
 
     def _spectrum_pots(self, exc, eneis, stream=None):

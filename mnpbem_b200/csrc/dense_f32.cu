@@ -170,11 +170,32 @@ __global__ void __launch_bounds__(SLAB_THREADS) panel_slab_kernel(int n, int k0,
     float *sre = slab_sm, *sim = slab_sm + (int64_t)SW * mmax;
     for (int cs = k0; cs < k0 + kb; cs += SW) {
         const int ms = n - cs;                         // slab rows cs .. n-1
-        for (int e = tid; e < SW * ms; e += SLAB_THREADS) {
-            const int j = e / ms, i = e - j * ms;
-            const int64_t o = (int64_t)(cs + j) * lda + cs + i;
-            sre[j * mmax + i] = A[o];
-            sim[j * mmax + i] = A[o + plane];
+        // every load of a thread's rows issued before its shared-memory stores
+        // (SW columns x 2 rows x 2 planes in flight per thread)
+        {
+            const float *src = A + (int64_t)cs * lda + cs;
+            for (int i0 = tid; i0 < ms; i0 += 2 * SLAB_THREADS) {
+                float vr[SW][2], vi[SW][2];
+#pragma unroll
+                for (int j = 0; j < SW; ++j)
+#pragma unroll
+                    for (int u = 0; u < 2; ++u) {
+                        const int i = i0 + u * SLAB_THREADS;
+                        const int64_t o = (int64_t)j * lda + i;
+                        vr[j][u] = i < ms ? __ldcg(src + o) : 0.f;
+                        vi[j][u] = i < ms ? __ldcg(src + o + plane) : 0.f;
+                    }
+#pragma unroll
+                for (int j = 0; j < SW; ++j)
+#pragma unroll
+                    for (int u = 0; u < 2; ++u) {
+                        const int i = i0 + u * SLAB_THREADS;
+                        if (i < ms) {
+                            sre[j * mmax + i] = vr[j][u];
+                            sim[j * mmax + i] = vi[j][u];
+                        }
+                    }
+            }
         }
         __syncthreads();
         for (int jj = 0; jj < SW; ++jj) {
@@ -252,11 +273,14 @@ __global__ void __launch_bounds__(SLAB_THREADS) panel_slab_kernel(int n, int k0,
             }
             __syncthreads();
         }
-        for (int e = tid; e < SW * ms; e += SLAB_THREADS) {
-            const int j = e / ms, i = e - j * ms;
-            const int64_t o = (int64_t)(cs + j) * lda + cs + i;
-            A[o] = sre[j * mmax + i];
-            A[o + plane] = sim[j * mmax + i];
+        {
+            float *dst = A + (int64_t)cs * lda + cs;
+            for (int i = tid; i < ms; i += SLAB_THREADS)
+#pragma unroll
+                for (int j = 0; j < SW; ++j) {
+                    dst[(int64_t)j * lda + i] = sre[j * mmax + i];
+                    dst[(int64_t)j * lda + i + plane] = sim[j * mmax + i];
+                }
         }
         // the slab's SW row interchanges, applied to the panel's other columns
         // in one gather / permute / scatter (at most 2 SW distinct rows)
