@@ -210,8 +210,13 @@ int64_t mnpb_bemret_workspace_mixed(int64_t n, int64_t batch);
 /* The algebra of mnpb_bemret_init_f64 on planar FP32 matrices (leading
  * dimension ld, a multiple of 4; plane = ld*n; batch stride 2*ld*n) with
  * every LU, triangular solve and GEMM on TF32 tensor cores: G1 -> LU(G1),
- * G2 -> LU(G2), H1 -> Sigma1, H2 -> LU(Sigma), D -> Delta^-1.  Replaces
- * mnpbem/bem/bem_ret.py:437-523 in the mixed-precision solver. */
+ * G2 -> LU(G2), H1 -> Sigma1, H2 -> LU(Sigma), D -> Delta^-1.  Factor
+ * values are stored rounded to nearest TF32.  From the second call with the
+ * same sizes, buffers and device on, the launch sequence is captured once as
+ * a CUDA graph (on a stream of the library's own) and replayed on `stream`;
+ * calls made while `stream` is being captured by the caller issue the plain
+ * launches.  Replaces mnpbem/bem/bem_ret.py:437-523 in the mixed-precision
+ * solver. */
 int mnpb_bemret_init_mixed(void *stream, int64_t n, int64_t batch, float *G1, float *G2,
                            float *H1, float *H2, float *D, int64_t ld, const double *eps,
                            const double *kvac, const double *nvec, int32_t *piv, int32_t *info,

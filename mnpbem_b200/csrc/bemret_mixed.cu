@@ -393,8 +393,10 @@ static int init_mixed_body(cudaStream_t s, int64_t n, int64_t batch, float *G1, 
 // The factorisation is ~2,000 launches whose arguments depend only on the
 // sizes and the buffer addresses, so it is replayed as a CUDA graph: the
 // first call with a given (sizes, addresses, device) runs normally, the
-// second is captured (thread-local capture mode), instantiated and launched,
-// later ones launch the instantiated graph.  Up to kGraphs such graphs are
+// second is captured (thread-local capture mode, on a stream of the
+// library's own), instantiated and launched on the caller's stream, later
+// ones launch the instantiated graph.  Calls made while the caller's stream
+// is itself being captured take the plain launch sequence.  Up to kGraphs such graphs are
 // kept (least recently used replaced).  Not used while the event profiler
 // records (its per-launch records come from the host-side launch sequence).
 namespace {
@@ -416,6 +418,16 @@ struct InitGraph {
     uint64_t used;
 };
 constexpr int kGraphs = 4;
+constexpr int kMaxDev = 64;
+// one non-blocking stream per device for the captures (created once)
+cudaStream_t capture_stream(int dev) {
+    static cudaStream_t st[kMaxDev] = {};
+    if (!st[dev] && cudaStreamCreateWithFlags(&st[dev], cudaStreamNonBlocking) != cudaSuccess) {
+        cudaGetLastError();
+        st[dev] = nullptr;
+    }
+    return st[dev];
+}
 std::mutex g_graph_mu;
 std::vector<InitGraph> g_graphs;
 uint64_t g_graph_clock = 0;
@@ -434,14 +446,23 @@ extern "C" int mnpb_bemret_init_mixed(void *stream, int64_t n, int64_t batch, fl
     MNPB_REQUIRE(work_bytes >= mnpb_bemret_workspace_mixed(n, batch),
                  "bemret_init_mixed: workspace too small");
     cudaStream_t s = as_stream(stream);
-    auto body = [&]() {
-        return init_mixed_body(s, n, batch, G1, G2, H1, H2, D, ld, eps, kvac, nvec, piv, info,
+    auto body = [&](cudaStream_t st) {
+        return init_mixed_body(st, n, batch, G1, G2, H1, H2, D, ld, eps, kvac, nvec, piv, info,
                                dinv, work, work_bytes);
     };
-    if (prof_on()) return body();
+    if (prof_on()) return body(s);
+    // a caller that is capturing its own graph gets the plain launch sequence
+    cudaStreamCaptureStatus cst = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(s, &cst) != cudaSuccess || cst != cudaStreamCaptureStatusNone) {
+        cudaGetLastError();
+        return body(s);
+    }
     InitKey key{{G1, G2, H1, H2, D, eps, kvac, nvec, piv, info, dinv, work},
                 n, batch, ld, work_bytes, 0};
-    if (cudaGetDevice(&key.dev) != cudaSuccess) return body();
+    if (cudaGetDevice(&key.dev) != cudaSuccess || key.dev < 0 || key.dev >= kMaxDev) {
+        cudaGetLastError();
+        return body(s);
+    }
     std::lock_guard<std::mutex> lk(g_graph_mu);
     InitGraph *hit = nullptr;
     for (auto &g : g_graphs)
@@ -456,31 +477,35 @@ extern "C" int mnpb_bemret_init_mixed(void *stream, int64_t n, int64_t batch, fl
             g_graphs.erase(lru);
         }
         g_graphs.push_back(InitGraph{key, nullptr, 0, ++g_graph_clock});
-        return body();
+        return body(s);
     }
     hit->used = ++g_graph_clock;
     if (!hit->exec) {
-        if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+        // captured on a stream of the library's own (the caller's may be the
+        // legacy default stream, which cannot be captured); capturing runs
+        // nothing, the instantiated graph is then launched on the caller's
+        const cudaStream_t cs = capture_stream(key.dev);
+        if (!cs || cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
             cudaGetLastError();
-            return body();
+            return body(s);
         }
         const int64_t l0 = g_launches.load();
-        const int rc = body();
+        const int rc = body(cs);
         cudaGraph_t graph = nullptr;
-        const cudaError_t ec = cudaStreamEndCapture(s, &graph);
+        const cudaError_t ec = cudaStreamEndCapture(cs, &graph);
         hit->launches = g_launches.load() - l0;
         g_launches.fetch_sub(hit->launches);   // counted again when the graph runs
         if (rc != MNPB_OK || ec != cudaSuccess || !graph) {
             if (graph) cudaGraphDestroy(graph);
             cudaGetLastError();
-            return rc != MNPB_OK ? rc : body();
+            return rc != MNPB_OK ? rc : body(s);
         }
         cudaGraphExec_t exec = nullptr;
         const cudaError_t ei = cudaGraphInstantiate(&exec, graph, 0);
         cudaGraphDestroy(graph);
         if (ei != cudaSuccess) {
             cudaGetLastError();
-            return body();
+            return body(s);
         }
         hit->exec = exec;
     }
