@@ -43,6 +43,21 @@ def _scalar_eps(p, enei):
     return complex(e1[0]), complex(e2[0])
 
 
+def _fields_by_wavelength(x, K):
+    """sig1, sig2 (B, n[, K]) and h1, h2 (B, n, 3[, K]) from a batch of
+    solution vectors x (B, 8, K, n) (sig1, h1x..z, sig2, h2x..z): one
+    reordering copy per field for the whole batch, so that each wavelength's
+    fields are contiguous views; the trailing K axis is dropped for K = 1
+    (the layout ``BEMRet._to_compstruct`` gives one wavelength)."""
+    sig1 = np.ascontiguousarray(x[:, 0].transpose(0, 2, 1))
+    sig2 = np.ascontiguousarray(x[:, 4].transpose(0, 2, 1))
+    h1 = np.ascontiguousarray(x[:, 1:4].transpose(0, 3, 1, 2))
+    h2 = np.ascontiguousarray(x[:, 5:8].transpose(0, 3, 1, 2))
+    if K == 1:
+        sig1, sig2, h1, h2 = sig1[..., 0], sig2[..., 0], h1[..., 0], h2[..., 0]
+    return sig1, sig2, h1, h2
+
+
 class _RetBatch(object):
     """Device buffers of one factorised batch of wavelengths (FP64)."""
 
@@ -364,14 +379,7 @@ class BEMRet(object):
             res = [work(c, cur) for c in chunks]
         out = []
         for chunk, (x, K) in zip(chunks, res):
-            # one reordering copy per field for the whole chunk; each
-            # wavelength's fields are contiguous views of it
-            sig1 = np.ascontiguousarray(x[:, 0].transpose(0, 2, 1))        # (B, n, K)
-            sig2 = np.ascontiguousarray(x[:, 4].transpose(0, 2, 1))
-            h1 = np.ascontiguousarray(x[:, 1:4].transpose(0, 3, 1, 2))    # (B, n, 3, K)
-            h2 = np.ascontiguousarray(x[:, 5:8].transpose(0, 3, 1, 2))
-            if K == 1:
-                sig1, sig2, h1, h2 = sig1[..., 0], sig2[..., 0], h1[..., 0], h2[..., 0]
+            sig1, sig2, h1, h2 = _fields_by_wavelength(x, K)
             for b, enei in enumerate(chunk):
                 out.append(CompStruct(self.p, enei, sig1=sig1[b], sig2=sig2[b], h1=h1[b],
                                       h2=h2[b]))
