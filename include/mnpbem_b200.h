@@ -298,6 +298,23 @@ int mnpb_cgemm_tf32(void *stream, int64_t m, int64_t n, int64_t k, int64_t batch
                     int64_t ldb, int64_t planeB, int64_t sB, float beta, float *C, int64_t ldc,
                     int64_t planeC, int64_t sC, void *work, int64_t work_bytes);
 
+/* mnpb_cgemm_tf32 with options (`flags`, an OR of the bits below):
+ *   MNPB_GEMM_A_TF32  A already holds TF32 values (the low 13 mantissa bits
+ *                     zero): the tensor cores read A in place from the
+ *                     column-major matrix (MN-major operand, no pack, `work`
+ *                     may be NULL).  A, lda, planeA and sA must be multiples
+ *                     of 16 bytes.  This is how the mixed factorisation
+ *                     applies its stored (TF32-rounded) factors.
+ *   MNPB_GEMM_ROUND_C store C rounded to nearest TF32.
+ * Replaces the same cuBLAS zgemm calls as mnpb_cgemm_tf32. */
+#define MNPB_GEMM_A_TF32 1
+#define MNPB_GEMM_ROUND_C 2
+int mnpb_cgemm_tf32_ex(void *stream, int64_t m, int64_t n, int64_t k, int64_t batch, float alpha,
+                       const float *A, int64_t lda, int64_t planeA, int64_t sA, const float *B,
+                       int64_t ldb, int64_t planeB, int64_t sB, float beta, float *C,
+                       int64_t ldc, int64_t planeC, int64_t sC, void *work, int64_t work_bytes,
+                       int32_t flags);
+
 /* Same GEMM as mnpb_cgemm_tf32, but it allocates nothing and takes no
  * workspace: the packed TF32 copy of A goes into a fixed 64 MiB array of the
  * library's static device memory (one per device, reserved when the module
@@ -308,7 +325,10 @@ int mnpb_cgemm_tf32(void *stream, int64_t m, int64_t n, int64_t k, int64_t batch
  *   - Limit: mnpb_cgemm_tf32_workspace(m, k, batch) <= 67108864 bytes, else
  *     MNPB_ENOMEM with the sizes in mnpb_last_error() and nothing launched.
  *   - The first call on each device does the setup (address lookup of the
- *     array, kernel attributes); make it before any stream capture.
+ *     array; the first launch of each kernel on a device also raises its
+ *     shared-memory limit there); make it before any stream capture.
+ *   - `stream` must belong to the current device (the array used is the
+ *     current device's); a stream of another device gives MNPB_EINVAL.
  *   - Nothing has to be zeroed beforehand: every scratch element is written
  *     before it is read.
  *   - Calls that overlap in time on one device (other streams, other host
@@ -321,6 +341,17 @@ int mnpb_cgemm_tf32_noalloc(void *stream, int64_t m, int64_t n, int64_t k, int64
 /* First bounded-wait timeout recorded by a tensor-core kernel since the last
  * call (0 = none); reading clears it. */
 int mnpb_tc_error(void *stream, int32_t *code);
+
+/* Failure-path check of the bounded device waits (no reference counterpart:
+ * the reference's GPU path catches exceptions and falls back to the CPU,
+ * mnpbem/bem/bem_ret.py:321-355).  Launches one thread that waits, with the
+ * helper the kernels use, on something nothing completes -- kind 0: an
+ * mbarrier (tensor-core GEMM), kind 1: a flag spin (`flag`, one device int,
+ * triangular solve), kind 2: an mbarrier (streamed triangular solve) -- for
+ * at most limit_ns (<= 2e9).  The wait gives up, records its error word like
+ * a kernel would, and returns; the probe then reads and clears the word and
+ * returns MNPB_ETIMEOUT with a message.  The device context stays usable. */
+int mnpb_wait_probe(void *stream, int32_t kind, int64_t limit_ns, int32_t *flag);
 
 /* Quasistatic matrix for a batch of wavelengths: M_b = -(diag(lambda_b) + F)
  * with lambda = 2 pi (eps1+eps2)/(eps1-eps2) per face (eps12: device,

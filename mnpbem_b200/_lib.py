@@ -57,9 +57,13 @@ SIGNATURES = {
     'mnpb_cgemm_tf32_workspace': [_I64, _I64, _I64],
     'mnpb_cgemm_tf32': [_P, _I64, _I64, _I64, _I64, C.c_float, _P, _I64, _I64, _I64, _P, _I64,
                         _I64, _I64, C.c_float, _P, _I64, _I64, _I64, _P, _I64],
+    'mnpb_cgemm_tf32_ex': [_P, _I64, _I64, _I64, _I64, C.c_float, _P, _I64, _I64, _I64, _P,
+                           _I64, _I64, _I64, C.c_float, _P, _I64, _I64, _I64, _P, _I64,
+                           C.c_int32],
     'mnpb_cgemm_tf32_noalloc': [_P, _I64, _I64, _I64, _I64, C.c_float, _P, _I64, _I64, _I64,
                                 _P, _I64, _I64, _I64, C.c_float, _P, _I64, _I64, _I64],
     'mnpb_tc_error': [_P, _P],
+    'mnpb_wait_probe': [_P, C.c_int32, _I64, _P],
     'mnpb_hmat_aca': [_P, _I64, _P, _I64, _P, _I64, _P, _P, _P, _I64, _I64, _D, _P, _P],
     'mnpb_hmat_gather_dense': [_P, _P, _I64, _P, _I64, _P, _P, _P],
     'mnpb_hmat_compact': [_P, _I64, _P, _P, _P, _P, _P, _P, _P, _P, _P],

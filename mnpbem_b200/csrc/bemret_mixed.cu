@@ -669,10 +669,12 @@ extern "C" int mnpb_bemret_solve_refine(
     }
     // relres holds each entry's relative residual before its last correction
     // (no extra pass over the FP64 operator just to report the final one)
-    int terr = 0;
+    int terr = 0, gerr = 0;
     MNPB_TRY(f32::trsv_error_read_and_clear(s, &terr));
-    if (terr) {
-        set_error("bemret_solve_refine: a triangular-solve wait timed out");
+    MNPB_TRY(tc::tc_error_read_and_clear(s, &gerr));
+    if (terr || gerr) {
+        set_error("bemret_solve_refine: a bounded device wait timed out (%s)",
+                  terr ? "triangular solve" : "tensor-core GEMM of the factorisation");
         return MNPB_ETIMEOUT;
     }
     for (int b = 0; b < B; ++b)

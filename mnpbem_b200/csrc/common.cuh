@@ -47,6 +47,21 @@ int check_launch(const char *what);
 
 inline cudaStream_t as_stream(void *s) { return reinterpret_cast<cudaStream_t>(s); }
 
+// Current device ordinal (-1 if cudaGetDevice fails).
+int current_device();
+// Raise `fn`'s dynamic shared-memory limit to `bytes` on the current device
+// (once per kernel and device; thread-safe).  MNPB_ECUDA with a message
+// naming `what` on failure.
+int smem_opt_in(const void *fn, int bytes, const char *what);
+template <typename F> inline int smem_opt_in(F *fn, int bytes, const char *what) {
+    return smem_opt_in((const void *)fn, bytes, what);
+}
+// Number of SMs of the current device (cached per device; 148 if unknown).
+int device_sms();
+// MNPB_EINVAL unless stream `s` belongs to the current device (the legacy
+// and per-thread default streams always do).
+int check_stream_device(cudaStream_t s, const char *what);
+
 // ---------------------------------------------------------------------------
 // optional per-kernel-class timing with CUDA events (mnpb_prof_begin/end)
 // ---------------------------------------------------------------------------

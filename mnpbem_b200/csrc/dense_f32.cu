@@ -690,6 +690,14 @@ __device__ __forceinline__ int ld_acquire(const int *p) {
     asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
     return v;
 }
+// Spins (acquire loads) until *p == want, for at most `limit` ns of wall
+// time; false if it gave up.
+__device__ __forceinline__ bool wait_flag(const int *p, int want, uint64_t limit) {
+    const uint64_t t0 = gtimer();
+    while (ld_acquire(p) != want)
+        if (gtimer() - t0 > limit) return false;
+    return true;
+}
 
 // Inverse of each 32 x 32 diagonal block of the unit-lower (lower = 1) or
 // upper (lower = 0) factor; out[b][blk][2][32][32] (planar, column-major).
@@ -793,15 +801,7 @@ __global__ void __launch_bounds__(256) trsv_kernel(int n, int m, int lower, cons
         }
         if (ii > known) {
             // lane 0 of each warp waits (acquire); __syncwarp orders the lanes' reads
-            if (r == 0) {
-                const uint64_t t0 = gtimer();
-                while (ld_acquire(fl + i) != epoch) {
-                    if (gtimer() - t0 > TRSV_WAIT_NS) {
-                        atomicCAS(&g_trsv_error, 0, 1);
-                        break;
-                    }
-                }
-            }
+            if (r == 0 && !wait_flag(fl + i, epoch, TRSV_WAIT_NS)) atomicCAS(&g_trsv_error, 0, 1);
             __syncwarp();
             known = ii;
         }
@@ -1025,7 +1025,8 @@ __device__ __forceinline__ void sbar_expect(uint32_t bar, uint32_t bytes) {
 __device__ __forceinline__ void sbar_arrive(uint32_t bar) {
     asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
 }
-__device__ __forceinline__ bool sbar_wait(uint32_t bar, uint32_t parity) {
+__device__ __forceinline__ bool sbar_wait(uint32_t bar, uint32_t parity,
+                                          uint64_t limit = STR_WAIT_NS) {
     const uint64_t t0 = gtimer();
     while (true) {
         uint32_t ok;
@@ -1037,7 +1038,7 @@ __device__ __forceinline__ bool sbar_wait(uint32_t bar, uint32_t parity) {
             : "r"(bar), "r"(parity)
             : "memory");
         if (ok) return true;
-        if (gtimer() - t0 > STR_WAIT_NS) return false;
+        if (gtimer() - t0 > limit) return false;
     }
 }
 __device__ __forceinline__ void s_tma3(uint32_t dst, const CUtensorMap *map, uint32_t bar, int c0,
@@ -1368,17 +1369,7 @@ static int trsm_small(Ctx &c, int mode, int kb, CMatF T, CMatF B, int nvec) {
     return MNPB_OK;
 }
 
-static int dev_sms() {
-    static int n = 0;
-    if (n == 0) {
-        int dev = 0, v = 0;
-        n = (cudaGetDevice(&dev) == cudaSuccess &&
-             cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess && v > 0)
-                ? v
-                : 148;
-    }
-    return n;
-}
+static int dev_sms() { return device_sms(); }
 
 static int split_point(int n) {
     int h = n / 2;
@@ -1466,15 +1457,7 @@ static int trsm(Ctx &c, int mode, int n, int m, CMatF T, CMatF B) {
     const int64_t keep = (c.work_bytes - inv_bytes) / 256 * 256;
     if (n <= TS || m < TL || keep < trsm_pack_bytes(mode, n, m, c.batch))
         return trsm_rec(c, mode, n, m, T, B, nullptr, 0);
-    static bool attr = false;
-    if (!attr) {
-        if (cudaFuncSetAttribute(tri_inv_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 TL * TL * (int)sizeof(cf)) != cudaSuccess) {
-            set_error("tri_inv_kernel: cannot reserve shared memory");
-            return MNPB_ECUDA;
-        }
-        attr = true;
-    }
+    MNPB_TRY(smem_opt_in(tri_inv_kernel, TL * TL * (int)sizeof(cf), "tri_inv_kernel"));
     float *inv = (float *)((char *)c.work + keep);
     {
         dim3 grid(nb, c.batch);
@@ -1512,19 +1495,8 @@ static int rgetrf(Ctx &c, int n, int off, int w, CMatF A, int32_t *ipiv, int64_t
     if (w <= TS) {
         ProfScope ps(c.s, PC_PANEL, 8.0 * w * w * (double)(n - off) * c.batch / 2);
         prof_tag("off=%d w=%d B=%d", off, w, c.batch);
-        static bool attr = false;
-        if (!attr) {
-            if (cudaFuncSetAttribute(panel_slab_kernel<8>,
-                                     cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     200 * 1024) != cudaSuccess ||
-                cudaFuncSetAttribute(panel_slab_kernel<4>,
-                                     cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     200 * 1024) != cudaSuccess) {
-                set_error("panel_slab_kernel: cannot reserve shared memory");
-                return MNPB_ECUDA;
-            }
-            attr = true;
-        }
+        MNPB_TRY(smem_opt_in(panel_slab_kernel<8>, 200 * 1024, "panel_slab_kernel<8>"));
+        MNPB_TRY(smem_opt_in(panel_slab_kernel<4>, 200 * 1024, "panel_slab_kernel<4>"));
         // more matrices than SMs: 4-column slabs, half the shared memory, so
         // that two CTAs share an SM and the batch runs in one wave
         const int64_t slab8 = (int64_t)8 * (n - off) * 8, slab4 = slab8 / 2;
@@ -1600,15 +1572,7 @@ template <int NC>
 static int trsv_rl(Ctx &c, bool lower, int n, int m, CMatF T, const float *inv, CMatF X) {
     const int nb = ceil_div(n, TB);
     const int dyn = n * NC * (int)sizeof(cf);
-    static int attr_bytes = 0;
-    if (dyn > 48 * 1024 && dyn > attr_bytes) {
-        if (cudaFuncSetAttribute(trsv_rl_kernel<NC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 dyn) != cudaSuccess) {
-            set_error("trsv_rl_kernel: cannot reserve %d bytes of shared memory", dyn);
-            return MNPB_ECUDA;
-        }
-        attr_bytes = dyn;
-    }
+    if (dyn > 48 * 1024) MNPB_TRY(smem_opt_in(trsv_rl_kernel<NC>, dyn, "trsv_rl_kernel"));
     ProfScope ps(c.s, PC_TRSV, 4.0 * (double)n * n * c.batch);   // bytes of the triangle
     prof_tag("n=%d m=%d B=%d %s", n, m, c.batch, lower ? "L" : "U");
     trsv_rl_kernel<NC><<<c.batch, RL_THREADS, dyn, c.s>>>(n, m, lower ? 1 : 0, T.p, T.ld, T.plane,
@@ -1631,16 +1595,7 @@ static int trsv_stream(Ctx &c, bool lower, int n, int m, CMatF T, const float *i
                        int S) {
     const int nb = ceil_div(n, TB);
     const int smem = stream_smem(n, NC, S);
-    static int attr_bytes = 0;
-    if (smem > attr_bytes) {
-        if (cudaFuncSetAttribute(trsv_stream_kernel<NC>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, smem) !=
-            cudaSuccess) {
-            set_error("trsv_stream_kernel: cannot reserve %d bytes of shared memory", smem);
-            return MNPB_ECUDA;
-        }
-        attr_bytes = smem;
-    }
+    MNPB_TRY(smem_opt_in(trsv_stream_kernel<NC>, smem, "trsv_stream_kernel"));
     CUtensorMap mr, mi;
     const uint64_t dims[3] = {(uint64_t)n, (uint64_t)n, (uint64_t)c.batch};
     const uint64_t strides[2] = {(uint64_t)T.ld * 4, (uint64_t)T.stride * 4};
@@ -1711,6 +1666,35 @@ int getrs_few(Ctx &c, int n, int m, CMatF LU, const int32_t *ipiv, int64_t sP,
     return trsv(c, false, n, m, LU, invU, B, state);
 }
 
+// Failure-path probe of the triangular solves' two wait helpers: kind 1
+// spins with wait_flag on a zeroed flag for the value 1 (which nothing
+// writes), kind 2 waits with sbar_wait on an mbarrier that expects one
+// arrival and never gets it.  Each gives up after `limit_ns`, records code 9
+// in the error word as a solve would, and returns.
+__global__ void trsv_wait_probe_kernel(int kind, const int *flag, uint64_t limit_ns) {
+    __shared__ __align__(8) uint64_t bar;
+    bool ok;
+    if (kind == 1) {
+        ok = wait_flag(flag, 1, limit_ns);
+    } else {
+        const uint32_t b = s_u32(&bar);
+        sbar_init(b, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        ok = sbar_wait(b, 0, limit_ns);
+    }
+    if (!ok) atomicCAS(&g_trsv_error, 0, 9);
+}
+
+int trsv_wait_probe(cudaStream_t s, int kind, int *flag, uint64_t limit_ns) {
+    if (cudaMemsetAsync(flag, 0, sizeof(int), s) != cudaSuccess) {
+        set_error("trsv_wait_probe: cannot clear the flag");
+        return MNPB_ECUDA;
+    }
+    trsv_wait_probe_kernel<<<1, 1, 0, s>>>(kind, flag, limit_ns);
+    MNPB_LAUNCH_CHECK("trsv_wait_probe_kernel");
+    return MNPB_OK;
+}
+
 int trsv_error_read_and_clear(cudaStream_t s, int *code) {
     int v = 0, z = 0;
     if (cudaMemcpyFromSymbolAsync(&v, g_trsv_error, sizeof(int), 0, cudaMemcpyDeviceToHost, s) !=
@@ -1770,4 +1754,34 @@ extern "C" int mnpb_getrs_c32p(void *stream, int64_t n, int64_t batch, int64_t n
     f32::Ctx c(as_stream(stream), (int)batch, (float *)work, work_bytes);
     return f32::getrs(c, (int)n, (int)nrhs, tc::CMatF{(float *)LU, ld, plane, stride}, piv,
                       pstride, tc::CMatF{B, ldb, planeB, bstride});
+}
+
+// ---------------------------------------------------------------------------
+// Failure-path probe of the bounded device waits (see the header).
+// ---------------------------------------------------------------------------
+#include "tc_gemm.cuh"
+
+extern "C" int mnpb_wait_probe(void *stream, int32_t kind, int64_t limit_ns, int32_t *flag) {
+    using namespace mnpb;
+    clear_error();
+    MNPB_REQUIRE(kind >= 0 && kind <= 2, "wait_probe: kind must be 0, 1 or 2");
+    MNPB_REQUIRE(limit_ns > 0 && limit_ns <= 2000000000ll, "wait_probe: limit_ns in (0, 2e9]");
+    MNPB_REQUIRE(kind != 1 || flag, "wait_probe: kind 1 needs a device int");
+    cudaStream_t s = as_stream(stream);
+    int code = 0;
+    if (kind == 0) {
+        MNPB_TRY(tc::wait_probe(s, (uint64_t)limit_ns));
+        MNPB_TRY(tc::tc_error_read_and_clear(s, &code));
+    } else {
+        MNPB_TRY(f32::trsv_wait_probe(s, kind, (int *)flag, (uint64_t)limit_ns));
+        MNPB_TRY(f32::trsv_error_read_and_clear(s, &code));
+    }
+    if (code) {
+        set_error("wait_probe: the %s wait gave up after %lld ns (error word %d)",
+                  kind == 0 ? "tensor-core mbarrier" : kind == 1 ? "triangular-solve flag"
+                                                                 : "triangular-solve mbarrier",
+                  (long long)limit_ns, code);
+        return MNPB_ETIMEOUT;
+    }
+    return MNPB_OK;
 }

@@ -38,6 +38,9 @@ int64_t trsv_state_bytes(int n, int batch);
 int getrs_few(Ctx &c, int n, int m, tc::CMatF LU, const int32_t *ipiv, int64_t sP,
               const float *invL, const float *invU, tc::CMatF B, int *state);
 int trsv_error_read_and_clear(cudaStream_t s, int *code);
+// One-thread kernel whose wait (kind 1: flag spin, kind 2: mbarrier) of the
+// triangular solves can only time out after limit_ns; records code 9.
+int trsv_wait_probe(cudaStream_t s, int kind, int *flag, uint64_t limit_ns);
 
 }  // namespace f32
 }  // namespace mnpb

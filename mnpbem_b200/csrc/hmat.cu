@@ -480,12 +480,7 @@ extern "C" int mnpb_hmat_aca(void *stream, int64_t n, const double *A, int64_t l
                  (long long)max_mn);
     cudaStream_t s = as_stream(stream);
     const int smem = (int)max_mn;
-    if (smem > 48 * 1024 &&
-        cudaFuncSetAttribute(hm::aca_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) !=
-            cudaSuccess) {
-        set_error("hmat_aca: cannot reserve %d bytes of shared memory", smem);
-        return MNPB_ECUDA;
-    }
+    if (smem > 48 * 1024) MNPB_TRY(smem_opt_in(hm::aca_kernel, smem, "hmat_aca"));
     ProfScope ps(s, PC_ACA, 0.0);
     hm::aca_kernel<<<(unsigned)nblk, hm::ACA_T, smem, s>>>(
         (const cd *)A, lda, c2p, (const int4 *)blocks, offU, offV, (int)kmax, htol, (cd *)UV, rank);

@@ -30,6 +30,83 @@ int check_launch(const char *what) {
     return MNPB_OK;
 }
 
+// ---- per-device kernel attributes ------------------------------------------
+// cudaFuncSetAttribute acts on the current device only, so the raised
+// dynamic shared-memory limit is remembered per (kernel, device) pair; the
+// table is guarded by one lock (callers on several host threads are safe).
+namespace {
+struct SmemKey {
+    const void *fn;
+    int dev;
+    int bytes;
+};
+std::mutex g_attr_mu;
+std::vector<SmemKey> g_attr;
+std::mutex g_sms_mu;
+int g_sms[64] = {};
+}  // namespace
+
+int current_device() {
+    int dev = -1;
+    if (cudaGetDevice(&dev) != cudaSuccess) return -1;
+    return dev;
+}
+
+int smem_opt_in(const void *fn, int bytes, const char *what) {
+    const int dev = current_device();
+    if (dev < 0) {
+        set_error("%s: cudaGetDevice failed", what);
+        return MNPB_ECUDA;
+    }
+    std::lock_guard<std::mutex> lk(g_attr_mu);
+    for (auto &k : g_attr)
+        if (k.fn == fn && k.dev == dev && k.bytes >= bytes) return MNPB_OK;
+    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e != cudaSuccess) {
+        set_error("%s: cannot reserve %d bytes of shared memory on device %d: %s", what, bytes,
+                  dev, cudaGetErrorString(e));
+        return MNPB_ECUDA;
+    }
+    for (auto &k : g_attr)
+        if (k.fn == fn && k.dev == dev) {
+            k.bytes = bytes;
+            return MNPB_OK;
+        }
+    g_attr.push_back({fn, dev, bytes});
+    return MNPB_OK;
+}
+
+int device_sms() {
+    const int dev = current_device();
+    if (dev < 0 || dev >= 64) return 148;
+    std::lock_guard<std::mutex> lk(g_sms_mu);
+    if (g_sms[dev] == 0) {
+        int v = 0;
+        g_sms[dev] = (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) ==
+                          cudaSuccess &&
+                      v > 0)
+                         ? v
+                         : 148;
+    }
+    return g_sms[dev];
+}
+
+int check_stream_device(cudaStream_t s, const char *what) {
+    if (s == nullptr || s == cudaStreamLegacy || s == cudaStreamPerThread) return MNPB_OK;
+    int sd = -1;
+    const int dev = current_device();
+    cudaError_t e = cudaStreamGetDevice(s, &sd);
+    if (e != cudaSuccess) {
+        set_error("%s: cudaStreamGetDevice failed: %s", what, cudaGetErrorString(e));
+        return MNPB_ECUDA;
+    }
+    if (sd != dev) {
+        set_error("%s: the stream belongs to device %d but device %d is current", what, sd, dev);
+        return MNPB_EINVAL;
+    }
+    return MNPB_OK;
+}
+
 // ---- event profiler ---------------------------------------------------------
 // Events come from a pool; records are appended to a shared list under one
 // lock; each host thread keeps its own open record (launches nest only

@@ -59,8 +59,9 @@ __device__ __forceinline__ uint64_t global_ns() {
     asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
     return t;
 }
-// Bounded parity wait (WAIT_NS of wall time); returns false on timeout.
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+// Bounded parity wait (`limit` ns of wall time); returns false on timeout.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity,
+                                          uint64_t limit = WAIT_NS) {
     const uint64_t t0 = global_ns();
     while (true) {
         uint32_t ok;
@@ -72,7 +73,7 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
             : "r"(bar), "r"(parity)
             : "memory");
         if (ok) return true;
-        if (global_ns() - t0 > WAIT_NS) return false;
+        if (global_ns() - t0 > limit) return false;
     }
 }
 __device__ __forceinline__ void tma_load_3d(uint32_t dst, const CUtensorMap *map, uint32_t bar,
@@ -665,6 +666,25 @@ __global__ void __launch_bounds__(256) pack_a_tf32_vec_kernel(const float *__res
     }
 }
 
+// Failure-path probe: one thread initialises an mbarrier that expects one
+// arrival, never arrives, and waits on it with mbar_wait -- the helper every
+// wait of the tensor-core kernels uses -- for at most `limit_ns`.  The wait
+// gives up, the error word gets code 9 as a kernel's would, and the kernel
+// returns; nothing else is touched.
+__global__ void wait_probe_kernel(uint64_t limit_ns) {
+    __shared__ __align__(8) uint64_t bar;
+    const uint32_t b = smem_u32(&bar);
+    mbar_init(b, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    if (!mbar_wait(b, 0, limit_ns)) atomicCAS(&g_tc_error, 0, 9);
+}
+
+int wait_probe(cudaStream_t s, uint64_t limit_ns) {
+    wait_probe_kernel<<<1, 1, 0, s>>>(limit_ns);
+    MNPB_LAUNCH_CHECK("wait_probe_kernel");
+    return MNPB_OK;
+}
+
 // ---------------------------------------------------------------------------
 // host side
 // ---------------------------------------------------------------------------
@@ -741,18 +761,7 @@ int encode_map_f32(void *map, const float *base, const uint64_t dims[3],
     return MNPB_OK;
 }
 
-static int num_sms() {
-    static int n = 0;
-    if (n == 0) {
-        int dev = 0, v = 0;
-        if (cudaGetDevice(&dev) == cudaSuccess &&
-            cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess && v > 0)
-            n = v;
-        else
-            n = 148;
-    }
-    return n;
-}
+static int num_sms() { return device_sms(); }
 
 int64_t cgemm_tf32_workspace(int M, int K, int batch) {
     const int64_t Mp = (M + BM - 1) / BM * BM, Kp = (K + BK - 1) / BK * BK;
@@ -763,16 +772,8 @@ template <int BN, bool AMN>
 static int launch_tf32(cudaStream_t s, const CUtensorMap &mA, const CUtensorMap &mAi,
                        const CMatF &B, int M, int N, int K, int Kp, int Mp, int batch, Epi ep) {
     using TL = Tile<BN>;
-    static bool attr_set = false;
-    if (!attr_set) {
-        if (cudaFuncSetAttribute(cgemm_tf32_kernel<BN, AMN>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 TL::smem_bytes(TL::MAX_ST)) != cudaSuccess) {
-            set_error("tc_gemm: cannot set shared memory size");
-            return MNPB_ECUDA;
-        }
-        attr_set = true;
-    }
+    MNPB_TRY(smem_opt_in(cgemm_tf32_kernel<BN, AMN>, TL::smem_bytes(TL::MAX_ST),
+                         "cgemm_tf32_kernel"));
     CUtensorMap mBr, mBi;
     MNPB_TRY(make_map(&mBr, B.p, K, N, batch, B.ld, B.stride, BN));
     MNPB_TRY(make_map(&mBi, B.p + B.plane, K, N, batch, B.ld, B.stride, BN));
@@ -790,16 +791,8 @@ static int launch_tf32(cudaStream_t s, const CUtensorMap &mA, const CUtensorMap 
     // (narrower tiles already overlap epilogues across several CTAs per SM)
     if (BN == 128 && ntiles >= 2 * num_sms()) {
         // persistent: one CTA per SM, double-buffered accumulators
-        static bool pattr = false;
-        if (!pattr) {
-            if (cudaFuncSetAttribute(cgemm_tf32_persistent<BN, AMN>,
-                                     cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     TL::smem_bytes(TL::MAX_ST)) != cudaSuccess) {
-                set_error("tc_gemm: cannot set shared memory size (persistent)");
-                return MNPB_ECUDA;
-            }
-            pattr = true;
-        }
+        MNPB_TRY(smem_opt_in(cgemm_tf32_persistent<BN, AMN>, TL::smem_bytes(TL::MAX_ST),
+                             "cgemm_tf32_persistent"));
         const int pst = TL::MAX_ST;
         const int grid = (int)(ntiles < num_sms() ? ntiles : num_sms());
         cgemm_tf32_persistent<BN, AMN><<<grid, 192, TL::smem_bytes(pst), s>>>(
@@ -907,6 +900,27 @@ extern "C" int mnpb_cgemm_tf32(void *stream, int64_t m, int64_t n, int64_t k, in
                           beta, c, (float *)work, work_bytes);
 }
 
+extern "C" int mnpb_cgemm_tf32_ex(void *stream, int64_t m, int64_t n, int64_t k, int64_t batch,
+                                  float alpha, const float *A, int64_t lda, int64_t planeA,
+                                  int64_t sA, const float *B, int64_t ldb, int64_t planeB,
+                                  int64_t sB, float beta, float *C, int64_t ldc, int64_t planeC,
+                                  int64_t sC, void *work, int64_t work_bytes, int32_t flags) {
+    clear_error();
+    MNPB_REQUIRE(m >= 0 && n >= 0 && k > 0 && batch > 0 && batch < 65536,
+                 "cgemm_tf32_ex: bad sizes");
+    MNPB_REQUIRE((flags & ~3) == 0, "cgemm_tf32_ex: unknown flag bits 0x%x", (unsigned)flags);
+    const bool a_tf32 = (flags & MNPB_GEMM_A_TF32) != 0;
+    MNPB_REQUIRE(A && B && C && (work || a_tf32), "cgemm_tf32_ex: null pointer");
+    tc::CMatF a{(float *)A, lda, planeA, sA}, b{(float *)B, ldb, planeB, sB}, c{C, ldc, planeC, sC};
+    if (a_tf32)
+        MNPB_REQUIRE(((uintptr_t)A & 15) == 0 && lda % 4 == 0 && planeA % 4 == 0 && sA % 4 == 0,
+                     "cgemm_tf32_ex: MNPB_GEMM_A_TF32 needs A, lda, planeA and sA aligned to "
+                     "16 bytes");
+    return tc::cgemm_tf32(as_stream(stream), (int)m, (int)n, (int)k, (int)batch, alpha, a, b,
+                          beta, c, (float *)work, work_bytes, (flags & MNPB_GEMM_ROUND_C) != 0,
+                          a_tf32);
+}
+
 extern "C" int mnpb_tc_error(void *stream, int32_t *code) {
     clear_error();
     MNPB_REQUIRE(code, "tc_error: null pointer");
@@ -946,40 +960,27 @@ static __device__ __align__(256) float g_static_pack[kStaticPackBytes / 4];
 
 constexpr int kMaxDevices = 64;
 
-template <int BN> static cudaError_t opt_in_smem() {
-    using TL = Tile<BN>;
-    return cudaFuncSetAttribute(cgemm_tf32_kernel<BN, false>,
-                                cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                TL::smem_bytes(TL::MAX_ST));
-}
-
 // Device address of g_static_pack on the current device, looked up once per
-// device (under a lock) together with the kernels' shared-memory opt-in.
+// device under a lock.  (The kernels' shared-memory opt-in is made per device
+// by the launch path itself, for every tile width and the persistent kernel.)
 static int static_pack_scratch(float **out) {
     static std::mutex mu;
     static float *addr[kMaxDevices] = {};
-    int dev = -1;
-    cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess) {
-        set_error("cgemm_tf32_noalloc: cudaGetDevice failed: %s", cudaGetErrorString(e));
+    const int dev = current_device();
+    if (dev < 0) {
+        set_error("cgemm_tf32_noalloc: cudaGetDevice failed");
         return MNPB_ECUDA;
     }
-    if (dev < 0 || dev >= kMaxDevices) {
+    if (dev >= kMaxDevices) {
         set_error("cgemm_tf32_noalloc: device ordinal %d out of range", dev);
         return MNPB_EINVAL;
     }
     std::lock_guard<std::mutex> lk(mu);
     if (!addr[dev]) {
         void *p = nullptr;
-        e = cudaGetSymbolAddress(&p, g_static_pack);
+        cudaError_t e = cudaGetSymbolAddress(&p, g_static_pack);
         if (e != cudaSuccess || !p) {
             set_error("cgemm_tf32_noalloc: cudaGetSymbolAddress failed on device %d: %s", dev,
-                      cudaGetErrorString(e));
-            return MNPB_ECUDA;
-        }
-        if ((e = opt_in_smem<32>()) != cudaSuccess || (e = opt_in_smem<64>()) != cudaSuccess ||
-            (e = opt_in_smem<128>()) != cudaSuccess) {
-            set_error("cgemm_tf32_noalloc: cannot set shared memory size on device %d: %s", dev,
                       cudaGetErrorString(e));
             return MNPB_ECUDA;
         }
@@ -1013,6 +1014,8 @@ extern "C" int mnpb_cgemm_tf32_noalloc(void *stream, int64_t m, int64_t n, int64
                   (long long)tc::kStaticPackBytes);
         return MNPB_ENOMEM;
     }
+    // the scratch array used is the current device's: the stream must be one of its streams
+    MNPB_TRY(check_stream_device(as_stream(stream), "cgemm_tf32_noalloc"));
     float *scratch = nullptr;
     MNPB_TRY(tc::static_pack_scratch(&scratch));
     tc::CMatF a{(float *)A, lda, planeA, sA}, b{(float *)B, ldb, planeB, sB}, c{C, ldc, planeC, sC};

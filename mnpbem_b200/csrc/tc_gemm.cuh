@@ -27,6 +27,9 @@ int cgemm_tf32(cudaStream_t s, int M, int N, int K, int batch, float alpha, CMat
                float beta, CMatF C, float *work, int64_t work_bytes, bool round_out = false,
                bool a_tf32 = false);
 int tc_error_read_and_clear(cudaStream_t s, int *code);
+// Launches a one-thread kernel whose mbarrier wait (the tensor-core kernels'
+// bounded wait, limit `limit_ns`) can only time out; it records code 9.
+int wait_probe(cudaStream_t s, uint64_t limit_ns);
 
 // 3-D FP32 TMA descriptor (written into the 128-byte CUtensorMap storage at
 // map): dims[0] contiguous, byte strides of dims 1 and 2, box, swizzle as

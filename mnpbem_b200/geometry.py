@@ -623,7 +623,7 @@ def load_mesh(name):
 
     The packaged meshes are the reference's own mesh-generator outputs
     (curved meshes are stored with their midpoint vertices), written by
-    ``mnpbem_b200/data/make_meshes.py``.
+    ``tests/golden/make_meshes.py``.
     """
     import os
     if not _MESH_CACHE:

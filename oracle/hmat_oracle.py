@@ -13,11 +13,25 @@ import numpy as np
 import scipy.sparse.linalg as spla
 
 
-def aca_block(fun_row, fun_col, m, n, htol, kmax):
+def _margin(a):
+    """Relative gap between the largest and second-largest entry of a (the
+    closeness of an argmax decision; 1 if there is no runner-up)."""
+    if a.size < 2:
+        return 1.0
+    top = np.partition(a, -2)[-2:]
+    return float((top[1] - top[0]) / top[1]) if top[1] > 0 else 1.0
+
+
+def aca_block(fun_row, fun_col, m, n, htol, kmax, diag=None):
     """Partially-pivoted ACA of one m x n block (hmatrix.py:195-336).
 
     fun_row(i) -> row i (n,), fun_col(j) -> column j (m,) of the block.
-    Returns U (m, r), V (n, r) with block ~ U V^T, and the pivots.
+    Returns U (m, r), V (n, r) with block ~ U V^T, and the pivots.  If
+    ``diag`` is a list, one dict per step is appended to it: the stop-test
+    ratio sqrt(new) / (htol sqrt(fro)) (the block stops once it is < 1) and
+    the relative margins of the column and row pivot choices -- how close
+    each decision was, for explaining a rank that differs under other
+    rounding.
     """
     max_rank = min(m, n, kmax)
     U = np.empty((m, max_rank), dtype=complex)
@@ -33,6 +47,9 @@ def aca_block(fun_row, fun_col, m, n, htol, kmax):
         a = np.abs(row)
         a[used_c] = 0.0
         pcol = int(np.argmax(a))
+        step = {'col_margin': _margin(a)}
+        if diag is not None:
+            diag.append(step)
         piv = row[pcol]
         if np.abs(piv) < 1e-15:
             break
@@ -51,11 +68,13 @@ def aca_block(fun_row, fun_col, m, n, htol, kmax):
         for j in range(rank - 1):
             cross += 2.0 * (np.vdot(U[:, j], u) * np.vdot(V[:, j], row)).real
         fro += new + cross
+        step['stop_ratio'] = (np.sqrt(new) / (htol * np.sqrt(abs(fro)))) if fro > 0 else np.inf
         if fro > 0 and np.sqrt(new) < htol * np.sqrt(abs(fro)):
             break
         a = np.abs(u)
         a[used_r] = 0.0
         prow = int(np.argmax(a))
+        step['row_margin'] = _margin(a)
     if rank == 0:
         return np.zeros((m, 1), complex), np.zeros((n, 1), complex), pivots
     return U[:, :rank].copy(), V[:, :rank].copy(), pivots
@@ -71,14 +90,33 @@ class HMatrixOracle(object):
         self.dense = []
         for r0, m, c0, k in part.dense:
             self.dense.append(A[np.ix_(c2p[r0:r0 + m], c2p[c0:c0 + k])])
-        self.U, self.V, self.pivots = [], [], []
+        self.U, self.V, self.pivots, self.diag = [], [], [], []
         for r0, m, c0, k in part.lowrank:
             rows, cols = c2p[r0:r0 + m], c2p[c0:c0 + k]
+            dg = []
             U, V, piv = aca_block(lambda i: A[rows[i], cols], lambda j: A[rows, cols[j]],
-                                  m, k, htol, kmax)
+                                  m, k, htol, kmax, diag=dg)
             self.U.append(U)
             self.V.append(V)
             self.pivots.append(piv)
+            self.diag.append(dg)
+
+    def near_tie(self, i, rank_other, tol=1e-9):
+        """Why block i could end at rank_other under other rounding: a stop
+        test within tol of its threshold, or a pivot choice whose top two
+        candidates are within tol, at or before the step where the two
+        ranks part.  Returns a description, or None if nothing explains it."""
+        dg = self.diag[i]
+        upto = min(len(dg), max(rank_other, self.U[i].shape[1]))
+        for s, st in enumerate(dg[:upto]):
+            r = st.get('stop_ratio')
+            if r is not None and np.isfinite(r) and abs(r - 1.0) < tol:
+                return 'stop test at step %d within %.1e of its threshold' % (s + 1, abs(r - 1))
+            for key in ('col_margin', 'row_margin'):
+                if st.get(key, 1.0) < tol:
+                    return '%s pivot at step %d: top two candidates %.1e apart' % (
+                        key.split('_')[0], s + 1, st[key])
+        return None
 
     def ranks(self):
         return np.array([u.shape[1] for u in self.U], dtype=np.int64)

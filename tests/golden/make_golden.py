@@ -1,6 +1,7 @@
 """Generate the golden fixtures by running the reference (PyMNPBEM) on CPU.
 
-    python tests/golden/make_golden.py [/path/to/reference]
+    python tests/golden/make_golden.py /path/to/reference
+    MNPBEM_REFERENCE=/path/to/reference python tests/golden/make_golden.py
 
 Needs the reference project importable (pure Python + NumPy/SciPy/Numba);
 ``tests/golden/mplstub`` stands in for ``matplotlib.path``, which the
@@ -188,5 +189,13 @@ def main(ref_root):
     print('rod done')
 
 
+def reference_root():
+    root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get('MNPBEM_REFERENCE')
+    if not root:
+        raise SystemExit("give the reference checkout as the first argument or in "
+                         "MNPBEM_REFERENCE")
+    return root
+
+
 if __name__ == '__main__':
-    main(sys.argv[1] if len(sys.argv) > 1 else '/root/reference')
+    main(reference_root())

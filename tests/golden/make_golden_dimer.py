@@ -1,6 +1,7 @@
 """Generate the dimer golden fixture by running the reference (PyMNPBEM) on CPU.
 
-    python tests/golden/make_golden_dimer.py [/path/to/reference]
+    python tests/golden/make_golden_dimer.py /path/to/reference
+    MNPBEM_REFERENCE=/path/to/reference python tests/golden/make_golden_dimer.py
 
 Two gold Drude spheres trisphere(144, 10 nm) 2 nm apart on the x axis (centres
 at x = -6 and +6 nm), inout [[2, 1], [2, 1]], in a host medium of eps = 1.77,
@@ -60,5 +61,13 @@ def main(ref_root):
     print('wrote golden_dimer.npz')
 
 
+def reference_root():
+    root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get('MNPBEM_REFERENCE')
+    if not root:
+        raise SystemExit("give the reference checkout as the first argument or in "
+                         "MNPBEM_REFERENCE")
+    return root
+
+
 if __name__ == '__main__':
-    main(sys.argv[1] if len(sys.argv) > 1 else '/root/reference')
+    main(reference_root())

@@ -1,7 +1,8 @@
 """Generate the H-matrix / iterative-solver golden fixtures by running the
 reference (PyMNPBEM) on CPU.
 
-    python tests/golden/make_golden_hmat.py [/path/to/reference]
+    python tests/golden/make_golden_hmat.py /path/to/reference
+    MNPBEM_REFERENCE=/path/to/reference python tests/golden/make_golden_hmat.py
 
 Output ``golden_hmat.npz`` holds, per case:
 
@@ -167,5 +168,13 @@ def main(ref_root):
     print('wrote golden_hmat.npz')
 
 
+def reference_root():
+    root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get('MNPBEM_REFERENCE')
+    if not root:
+        raise SystemExit("give the reference checkout as the first argument or in "
+                         "MNPBEM_REFERENCE")
+    return root
+
+
 if __name__ == '__main__':
-    main(sys.argv[1] if len(sys.argv) > 1 else '/root/reference')
+    main(reference_root())

@@ -2,7 +2,8 @@
 
 Run in a checkout that has the reference project (PyMNPBEM) available:
 
-    python mnpbem_b200/data/make_meshes.py /path/to/reference
+    python tests/golden/make_meshes.py /path/to/reference
+    MNPBEM_REFERENCE=/path/to/reference python tests/golden/make_meshes.py
 
 The meshes are the reference's own mesh-generator outputs (the BEM path takes
 a ready surface mesh as input; mesh generation is not part of it):
@@ -25,6 +26,7 @@ import sys
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
+DATA = os.path.join(HERE, '..', '..', 'mnpbem_b200', 'data')
 
 SPHERES = [(32, 10.0), (60, 10.0), (144, 10.0), (144, 20.0), (256, 20.0), (1444, 40.0)]
 RODS = [(20.0, 80.0, (31, 21, 41)), (20.0, 80.0, (61, 31, 101)), (20.0, 80.0, (97, 47, 171))]
@@ -32,7 +34,7 @@ RODS = [(20.0, 80.0, (31, 21, 41)), (20.0, 80.0, (61, 31, 101)), (20.0, 80.0, (9
 
 def main(ref_root):
     sys.path.insert(0, ref_root)
-    sys.path.insert(0, os.path.join(HERE, '..', '..', 'tests', 'golden', 'mplstub'))
+    sys.path.insert(0, os.path.join(HERE, 'mplstub'))
     from mnpbem.geometry.mesh_generators import trisphere, trirod
     from mnpbem.spectrum.spectrum_ret import _load_pinfty_default
 
@@ -50,9 +52,17 @@ def main(ref_root):
     pin = _load_pinfty_default()
     out['pinfty256_nvec'] = np.asarray(pin.nvec, dtype=np.float64)
     out['pinfty256_area'] = np.asarray(pin.area, dtype=np.float64)
-    np.savez_compressed(os.path.join(HERE, 'meshes.npz'), **out)
+    np.savez_compressed(os.path.join(DATA, 'meshes.npz'), **out)
     print('wrote', sorted(out))
 
 
+def reference_root():
+    root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get('MNPBEM_REFERENCE')
+    if not root:
+        raise SystemExit("give the reference checkout as the first argument or in "
+                         "MNPBEM_REFERENCE")
+    return root
+
+
 if __name__ == '__main__':
-    main(sys.argv[1] if len(sys.argv) > 1 else '/root/reference')
+    main(reference_root())

@@ -131,3 +131,49 @@ def test_c1_2884_faces(gpu_ok):
 def test_native_library_was_used(gpu_ok):
     from mnpbem_b200 import _lib
     assert _lib.launch_count() > 0
+
+
+def test_c0_refined_coefficient_subset(gpu_ok):
+    """trisphere(144, 20) (284 curved faces): every 23rd refined pair of the
+    reference (g and the closure-corrected f, greenret_refined.py:122-516,
+    compgreen_ret.py:376-400), matched pair by pair (row, col)."""
+    cp, s = _cp('trisphere_144_20')
+    z = golden('golden_c0')
+    b = bem.BEMRet(cp)
+    t = b.tables
+    key = {(int(r), int(c)): i for i, (r, c) in enumerate(zip(t.h_rows, t.h_cols))}
+    idx = np.array([key[(int(r), int(c))] for r, c in zip(z['ref_rows'], z['ref_cols'])])
+    assert len(idx) == len(z['ref_sub']) > 400
+    g = t.g.cpu().numpy()[idx]
+    f = t.f.cpu().numpy()[idx]
+    assert rel(g, z['ref_g'].real) < 1e-13
+    assert rel(f, z['ref_f'].real) < 1e-11
+    # self pairs (polar quadrature) and near pairs (face quadrature) both present
+    kinds = t.h_kinds[idx]
+    assert (kinds == 2).sum() > 10 and (kinds == 1).sum() > 100
+
+
+@pytest.fixture(scope='module')
+def c1sig():
+    cp, s = _cp('trisphere_1444_40')
+    return cp, golden('golden_c1_sig')
+
+
+def test_c1_fp64_sigma_five_wavelengths(gpu_ok, c1sig):
+    """trisphere(1444, 40) (2884 faces): the plain FP64 GPU path against the
+    reference BEMRet at 400, 470 (resonance), 520, 600, 800 nm -- sigma within
+    1e-10 (max-norm relative), h within 1e-9, extinction and scattering within
+    1e-10."""
+    cp, z = c1sig
+    b = bem.BEMRet(cp)
+    exc = excitation.PlaneWaveRet(pol=[[1, 0, 0]], dir=[[0, 0, 1]])
+    sols = b.solve_spectrum(exc, list(z['lams']), batch=5)
+    for i, sg in enumerate(sols):
+        assert rel(sg.sig1, z['sig1_%d' % i]) < 1e-10, i
+        assert rel(sg.sig2, z['sig2_%d' % i]) < 1e-10, i
+        assert rel(sg.h1, z['h1_%d' % i]) < 1e-9, i
+        assert rel(sg.h2, z['h2_%d' % i]) < 1e-9, i
+    ext = np.array([exc.extinction(sg) for sg in sols]).ravel()
+    sca = np.array([exc.scattering(sg)[0] for sg in sols]).ravel()
+    assert np.max(np.abs(ext - z['ext']) / np.abs(z['ext'])) < 1e-10
+    assert np.max(np.abs(sca - z['sca']) / np.abs(z['sca'])) < 1e-10

@@ -46,3 +46,68 @@ def test_cgemm_tf32(gpu_ok, m, n, k, batch, alpha, beta):
     out = _cplx(C, m, n)
     err = (out - ref).abs().pow(2).sum().sqrt() / ref.abs().pow(2).sum().sqrt()
     assert err.item() < 2e-3, err.item()
+
+
+def _round_tf32(x):
+    """Round FP32 values to nearest TF32 (10 mantissa bits), ties away from
+    zero -- the rounding of cvt.rna.tf32.f32."""
+    u = x.contiguous().view(torch.int32)
+    u = (u + 0x1000) & ~0x1FFF
+    return u.view(torch.float32)
+
+
+@pytest.mark.parametrize('m,n,k,batch,alpha,beta', [
+    (128, 32, 32, 1, 1.0, 0.0),          # BN = 32 tiles
+    (200, 60, 50, 3, -1.0, 1.0),         # BN = 64, ragged M, N, K
+    (300, 130, 100, 2, 1.0, 1.0),        # BN = 128, grid kernel, ragged
+    (1000, 400, 300, 16, -1.0, 1.0),     # 512 tiles >= 2 per SM: persistent kernel
+    (2884, 1440, 1444, 2, -1.0, 1.0)])   # the largest trailing update of the 2884-face LU
+def test_cgemm_tf32_a_in_place(gpu_ok, m, n, k, batch, alpha, beta):
+    """A read in place (MN-major TMA tiles, 128B swizzle on 32-byte atoms):
+    the path the mixed factorisation takes for its stored TF32 factors,
+    compared with a complex128 product of the same (TF32-valued) A."""
+    lda, ldb, ldc = (m + 3) // 4 * 4, (k + 3) // 4 * 4, (m + 3) // 4 * 4
+    A = _round_tf32(_planar(batch, m, k, lda, 11))
+    B = _planar(batch, k, n, ldb, 12)
+    C = _planar(batch, m, n, ldc, 13)
+    ref = alpha * (_cplx(A, m, k) @ _cplx(B, k, n)) + beta * _cplx(C, m, n)
+    call('mnpb_cgemm_tf32_ex', _lib.stream_handle(), m, n, k, batch, alpha, ptr(A), lda, k * lda,
+         2 * k * lda, ptr(B), ldb, n * ldb, 2 * n * ldb, beta, ptr(C), ldc, n * ldc, 2 * n * ldc,
+         None, 0, 1)
+    torch.cuda.synchronize()
+    code = np.zeros(1, dtype=np.int32)
+    call('mnpb_tc_error', _lib.stream_handle(), ptr(code))
+    assert code[0] == 0
+    out = _cplx(C, m, n)
+    err = (out - ref).abs().pow(2).sum().sqrt() / ref.abs().pow(2).sum().sqrt()
+    assert err.item() < 2e-3, err.item()
+
+
+def test_cgemm_tf32_round_output(gpu_ok):
+    """MNPB_GEMM_ROUND_C: every stored element of C is a TF32 value."""
+    m, n, k, batch = 256, 100, 64, 2
+    lda, ldb, ldc = m, k, m
+    A = _round_tf32(_planar(batch, m, k, lda, 21))
+    B = _planar(batch, k, n, ldb, 22)
+    C = torch.zeros((batch, 2, n, ldc), dtype=torch.float32, device='cuda')
+    ref = _cplx(A, m, k) @ _cplx(B, k, n)
+    call('mnpb_cgemm_tf32_ex', _lib.stream_handle(), m, n, k, batch, 1.0, ptr(A), lda, k * lda,
+         2 * k * lda, ptr(B), ldb, n * ldb, 2 * n * ldb, 0.0, ptr(C), ldc, n * ldc, 2 * n * ldc,
+         None, 0, 3)
+    torch.cuda.synchronize()
+    assert int((C.view(torch.int32) & 0x1FFF).abs().sum().item()) == 0
+    out = _cplx(C, m, n)
+    err = (out - ref).abs().pow(2).sum().sqrt() / ref.abs().pow(2).sum().sqrt()
+    assert err.item() < 2e-3, err.item()
+
+
+def test_cgemm_tf32_ex_rejects_unaligned_in_place_a(gpu_ok):
+    """An in-place A must be 16-byte aligned (TMA); refused on the host."""
+    m = n = k = 64
+    A = torch.zeros((2, k, 66), dtype=torch.float32, device='cuda')
+    B = torch.zeros((2, n, k), dtype=torch.float32, device='cuda')
+    C = torch.zeros((2, n, m), dtype=torch.float32, device='cuda')
+    rc = _lib.lib().mnpb_cgemm_tf32_ex(_lib.stream_handle(), m, n, k, 1, 1.0, ptr(A), 66,
+                                       k * 66, 2 * k * 66, ptr(B), k, n * k, 2 * n * k, 0.0,
+                                       ptr(C), m, n * m, 2 * n * m, None, 0, 1)
+    assert rc == 1     # MNPB_EINVAL: lda = 66 floats is not a multiple of 16 bytes

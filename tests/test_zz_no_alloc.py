@@ -1,11 +1,13 @@
 """Allocation-free tensor-core GEMM (mnpb_cgemm_tf32_noalloc) against the
 workspace-taking entry point (mnpb_cgemm_tf32) on the same inputs.
 
-Two calls of the allocation-free entry run back to back with different shapes,
-so the second reuses the static scratch the first wrote.  Each result must
-agree with mnpb_cgemm_tf32's within the TF32 GEMM tolerance (relative
-Frobenius error below 2e-3, as for mnpb_cgemm_tf32 against complex128).
-The file name sorts last so that it also runs after every other test."""
+Calls of the allocation-free entry run back to back with different shapes,
+so each reuses the static scratch the one before it wrote.  The last shape has
+enough 128 x 128 tiles (384, at least two per SM) to run the persistent
+kernel.  Each result must agree with mnpb_cgemm_tf32's and with a complex128
+product of the same inputs within the TF32 GEMM tolerance (relative Frobenius
+error below 2e-3).  The file name sorts last so that it also runs after every
+other test."""
 import ctypes
 
 import numpy as np
@@ -42,7 +44,8 @@ def _tc_error():
 
 
 def test_noalloc_matches_workspace_gemm_twice(gpu_ok):
-    cases = [(200, 100, 50, 3, -1.0, 1.0, 11), (384, 64, 1000, 2, 1.0, 1.0, 21)]
+    cases = [(200, 100, 50, 3, -1.0, 1.0, 11), (384, 64, 1000, 2, 1.0, 1.0, 21),
+             (2048, 1024, 1024, 3, -1.0, 1.0, 31)]
     outs = []
     for m, n, k, batch, alpha, beta, seed in cases:
         lda, ldb, ldc = (m + 3) // 4 * 4, (k + 3) // 4 * 4, (m + 3) // 4 * 4
@@ -50,6 +53,7 @@ def test_noalloc_matches_workspace_gemm_twice(gpu_ok):
         B = _planar(batch, n, ldb, seed + 1)
         C0 = _planar(batch, n, ldc, seed + 2)
         C_ws, C_na = C0.clone(), C0.clone()
+        ref = alpha * (_cplx(A, m) @ _cplx(B, k)) + beta * _cplx(C0, m)
         wb = int(_lib.lib().mnpb_cgemm_tf32_workspace(m, k, batch))
         assert wb <= STATIC_BYTES
         work = torch.empty(wb, dtype=torch.uint8, device='cuda')
@@ -57,12 +61,14 @@ def test_noalloc_matches_workspace_gemm_twice(gpu_ok):
              *_args(m, n, k, batch, alpha, beta, A, B, C_ws), ptr(work), wb)
         call('mnpb_cgemm_tf32_noalloc', _lib.stream_handle(),
              *_args(m, n, k, batch, alpha, beta, A, B, C_na))
-        outs.append((m, C_ws, C_na))
+        outs.append((m, C_ws, C_na, ref))
     torch.cuda.synchronize()
     assert _tc_error() == 0
-    for m, C_ws, C_na in outs:
+    for m, C_ws, C_na, ref in outs:
         ws, na = _cplx(C_ws, m), _cplx(C_na, m)
         err = ((na - ws).abs().pow(2).sum().sqrt() / ws.abs().pow(2).sum().sqrt()).item()
+        assert err < 2e-3, err
+        err = ((na - ref).abs().pow(2).sum().sqrt() / ref.abs().pow(2).sum().sqrt()).item()
         assert err < 2e-3, err
 
 
