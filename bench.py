@@ -64,10 +64,20 @@ def parse():
     ap.add_argument('--no-iterative', action='store_true',
                     help='skip the H-matrix / GMRES measurement on the 25k-face rod')
     ap.add_argument('--iter-nlam', type=int, default=6)
-    ap.add_argument('--probe', default=None, choices=['tc_gemm', 'hmat', 'lu'],
+    ap.add_argument('--probe', default=None,
+                    choices=['tc_gemm', 'tc_gemm_packed', 'assemble', 'solve', 'hmat', 'lu'],
                     help='run one representative kernel on a small case (profiling target) '
                          'and print its timing instead of the benchmark')
+    ap.add_argument('--fp64-steps', type=int, default=None,
+                    help='timed sweeps of the plain FP64 GPU path (default: --steps)')
     return ap.parse_args()
+
+
+def _sphere2884():
+    import mnpbem_b200 as M
+    v, f = M.load_mesh('trisphere_1444_40')
+    s = M.Particle(v, f, interp='curv')
+    return M.ComParticle([M.EpsConst(1.0), M.EpsDrude(*DRUDE)], [s], [[2, 1]])
 
 
 def run_probe(args):
@@ -75,7 +85,13 @@ def run_probe(args):
     device at most, a handful of launches):
 
     * tc_gemm: C = C - A B, planar complex FP32, M = 2884, N = 1440,
-      K = 1444, batch 4 (the largest trailing update of the 2884-face LU);
+      K = 1444, batch 4 (the largest trailing update of the 2884-face LU), A
+      TF32-valued and read in place (MN-major) as the factorisation does;
+    * tc_gemm_packed: the same with A packed K-major first;
+    * assemble: the mixed-path assembly (c128 + planar FP32 copies of G1, H1,
+      G2, H2) of the 2884-face sphere for 4 wavelengths;
+    * solve: mixed factorisation + FP64-refined solve of the 2884-face sphere
+      for 4 wavelengths (the streamed few-RHS triangular solves run here);
     * hmat: the four-matrix H-matrix product of trirod(20, 80, [61, 31, 101])
       (9600 faces) at 600 nm, ACA cleaf 64 htol 1e-6, 4 right-hand sides;
     * lu: mixed-precision LU (recursive, tensor-core updates, shared-memory
@@ -86,20 +102,55 @@ def run_probe(args):
     torch.manual_seed(0)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     out = {"probe": args.probe}
-    if args.probe == 'tc_gemm':
+    flops = None
+    if args.probe in ('tc_gemm', 'tc_gemm_packed'):
         M, N, K, B = 2884, 1440, 1444, 4
         ld, ldb = 2884, 1444
         A = torch.randn((B, 2, K, ld), device='cuda')
+        if args.probe == 'tc_gemm':
+            A = ((A.view(torch.int32) + 0x1000) & ~0x1FFF).view(torch.float32)
         Bm = torch.randn((B, 2, N, ldb), device='cuda')
         C = torch.randn((B, 2, N, ld), device='cuda')
         wb = int(_lib.lib().mnpb_cgemm_tf32_workspace(M, K, B))
         W = torch.empty(wb, dtype=torch.uint8, device='cuda')
+        flag = 1 if args.probe == 'tc_gemm' else 0
 
         def f():
-            call('mnpb_cgemm_tf32', _lib.stream_handle(), M, N, K, B, -1.0, ptr(A), ld, K * ld,
-                 2 * K * ld, ptr(Bm), ldb, N * ldb, 2 * N * ldb, 1.0, ptr(C), ld, N * ld,
-                 2 * N * ld, ptr(W), wb)
+            call('mnpb_cgemm_tf32_ex', _lib.stream_handle(), M, N, K, B, -1.0, ptr(A), ld,
+                 K * ld, 2 * K * ld, ptr(Bm), ldb, N * ldb, 2 * N * ldb, 1.0, ptr(C), ld, N * ld,
+                 2 * N * ld, ptr(W), wb, flag)
         flops = 8.0 * M * N * K * B
+        out["algorithmic_bytes"] = 4.0 * B * (2 * K * M + 2 * N * K + 2 * 2 * N * M)
+    elif args.probe in ('assemble', 'solve'):
+        from mnpbem_b200 import bem, excitation
+        cp = _sphere2884()
+        solver = bem.BEMRet(cp, precision='mixed', refine_tol=1e-8)
+        t = solver.tables
+        eneis = [450.0, 500.0, 550.0, 600.0]
+        exc = excitation.PlaneWaveRet(pol=[[1.0, 0, 0]], dir=[[0, 0, 1.0]])
+        if args.probe == 'assemble':
+            from mnpbem_b200.bem import _MixedBatch
+            bt = _MixedBatch(t, eneis)
+            kblk, sblk = t.k_tables(eneis)
+            d_k = torch.from_numpy(np.ascontiguousarray(kblk)).cuda()
+            d_s = torch.from_numpy(np.ascontiguousarray(sblk)).cuda()
+            poff = np.ascontiguousarray(t.part_off, dtype=np.int64)
+            n, ld, Bn = t.n, bt.ld, len(eneis)
+
+            def f():
+                call('mnpb_assemble_ret2', _lib.stream_handle(), n, Bn, ptr(t.pos),
+                     ptr(t.nvec), ptr(t.area), t.nparts, ptr(poff), ptr(d_k), ptr(d_s), t.nref,
+                     ptr(t.rows), ptr(t.cols), ptr(t.g), ptr(t.fn), ptr(bt.G1), ptr(bt.H1),
+                     ptr(bt.G2), ptr(bt.H2), ld, ld * n, ptr(bt.G1p), ptr(bt.H1p), ptr(bt.G2p),
+                     ptr(bt.H2p), ld, 2 * ld * n, ld * n)
+            # per wavelength: G1, H1, G2, H2 written as c128 + planar FP32 (24 B an
+            # entry), refined pairs read once (g[6], fn[6] doubles + row, col)
+            out["algorithmic_bytes"] = Bn * (4.0 * n * n * (16 + 8) + t.nref * 104)
+        else:
+            def f():
+                bt = solver._factor(eneis)
+                pots, K = exc.potential_device(cp, t, eneis)
+                solver._solve_batch(bt, pots, K)
     elif args.probe == 'hmat':
         import mnpbem_b200 as Mb
         from mnpbem_b200.bem_iter import BEMRetIter
@@ -118,7 +169,6 @@ def run_probe(args):
         def f():
             hmat_matvec(hms, xs, ys, 4)
         out["bytes"] = sum(h.stored_bytes() for h in hms)
-        flops = None
     else:
         n, B = 2884, 8
         ld = 2884
@@ -147,6 +197,8 @@ def run_probe(args):
         out["tflops"] = flops / ms / 1e9
     if "bytes" in out:
         out["GBs"] = out["bytes"] / ms / 1e6
+    if "algorithmic_bytes" in out:
+        out["GBs_algorithmic"] = out["algorithmic_bytes"] / ms / 1e6
     print(json.dumps(out))
 
 
@@ -266,6 +318,32 @@ def measured_peaks():
         with open(path) as f:
             return json.load(f), 'measured'
     return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}, 'fallback'
+
+
+def profile_traffic():
+    """DRAM bytes per launch of the dominant kernels, from the committed ncu
+    summaries (profiles/roofline_traffic.json: kernel class -> dram_bytes,
+    the captured launch, its algorithmic bytes and the summary file)."""
+    path = os.path.join(ROOT, 'profiles', 'roofline_traffic.json')
+    if not os.path.exists(path):
+        return {}
+    with open(path) as f:
+        return json.load(f)
+
+
+def solution_errors(xa, xb, ext_a, ext_b, sca_a, sca_b):
+    """Largest relative errors over the wavelengths of a sweep: sigma and h
+    per wavelength as max |a - b| / max |b| (tests/test_bem_iter.py:100-103
+    of the reference), extinction and scattering as |a - b| / |b|."""
+    def per_lam(a, b):
+        return float(np.max(np.abs(a - b).reshape(len(a), -1).max(axis=1) /
+                            np.abs(b).reshape(len(b), -1).max(axis=1)))
+    return {"sigma1_max_rel_err": per_lam(xa[:, 0], xb[:, 0]),
+            "sigma2_max_rel_err": per_lam(xa[:, 4], xb[:, 4]),
+            "h1_max_rel_err": per_lam(xa[:, 1:4], xb[:, 1:4]),
+            "h2_max_rel_err": per_lam(xa[:, 5:8], xb[:, 5:8]),
+            "ext_max_rel_err": float(np.max(np.abs(ext_a - ext_b) / np.abs(ext_b))),
+            "sca_max_rel_err": float(np.max(np.abs(sca_a - sca_b) / np.abs(sca_b)))}
 
 
 # ---------------------------------------------------------------------------
@@ -389,6 +467,30 @@ def main():
         e = torch.cat(exts).cpu().numpy()          # (NLAM, K=1, ndir=1, 3)
         return np.real(4 * np.pi / kk * np.imag(np.sum(np.conj(exc.pol[0]) * e[:, 0, 0], axis=1)))
 
+    def full_solutions(slv):
+        """Solutions (NLAM, 8, K, n), extinction and scattering (NLAM,) of one
+        sweep: the forward far field for extinction (planewave_ret.py:437) and
+        the 256-direction far-field sphere for scattering (spectrum_ret.py:395)."""
+        from mnpbem_b200.excitation import pinfty
+        nvec_s, area_s = pinfty()
+        xs, es, ss = [], [], []
+        for s0 in range(0, NLAM, B):
+            chunk = eneis[s0:s0 + B]
+            bt = slv._factor(chunk)
+            pots, K = exc.potential_device(cp, slv.tables, chunk)
+            xout = slv._solve_batch(bt, pots, K)
+            if getattr(bt, 'iters', None) is not None:
+                refine_iters.extend(int(v) for v in bt.iters)
+            del bt
+            e, _ = exc.farfield_device(cp, slv.tables, xout, chunk, exc.dir)
+            es.append(e)
+            ef, hf = exc.farfield_device(cp, slv.tables, xout, chunk, nvec_s)
+            ef, hf = ef[:, 0].cpu().numpy(), hf[:, 0].cpu().numpy()
+            dsca = 0.5 * np.real(np.einsum('dc,bdc->bd', nvec_s, np.cross(ef, np.conj(hf))))
+            ss.append(dsca @ area_s / 0.5)          # vacuum: 0.5 Re sqrt(eps) = 0.5
+            xs.append(xout.cpu().numpy())
+        return np.concatenate(xs), ext_of(es), np.concatenate(ss)
+
     torch.cuda.synchronize()
     for _ in range(args.warmup):
         device_step()
@@ -447,59 +549,89 @@ def main():
     d2h = NLAM * 8 * K * n * 16                        # sig1, h1, sig2, h2 per wavelength
 
     peaks, peak_kind = measured_peaks()
+    traffic = profile_traffic()
     # dominant kernel by device time
     dom = max(prof.items(), key=lambda kv: kv[1][0]) if prof else None
     roof = None
     if dom is not None:
         name, (dms, work, cnt) = dom
         tot_ms = sum(v[0] for v in prof.values())
+        tr = traffic.get(name) or {}
         if name in ('zgemm_f64',):
             achieved = work / (dms / 1000.0) / 1e12
             peak = 37.0
             roof = {"kernel": name, "bound": "fp64", "achieved": achieved, "peak": peak,
-                    "unit": "TFLOP/s", "frac": achieved / peak, "traffic": None,
+                    "unit": "TFLOP/s", "frac": achieved / peak,
                     "peak_source": "nominal B200 FP64 (no measured FP64 peak in "
-                                   "MEASURED_PEAKS.json)",
-                    "launches": cnt, "share": dms / tot_ms}
+                                   "MEASURED_PEAKS.json)"}
         elif name in ('tc_gemm',):
             achieved = work / (dms / 1000.0) / 1e12
             peak = peaks['bf16_tflops_sustained']
-            # DRAM bytes of one representative launch from an ncu capture
-            # (ncu --set full -k regex:cgemm_tf32_persistent ... bench.py --probe tc_gemm)
             roof = {"kernel": name, "bound": "tensor", "achieved": achieved, "peak": peak,
-                    "unit": "TFLOP/s", "frac": achieved / peak, "traffic": 551.5e6,
-                    "traffic_launch": "cgemm_tf32_persistent<128>, M=2884 N=1440 K=1444 "
-                                      "batch 4 (algorithmic 466e6 B)",
-                    "peak_source": peak_kind + " bf16 sustained",
-                    "frac_of_tf32_ceiling": achieved / (peak / 2.0),
-                    "launches": cnt, "share": dms / tot_ms}
+                    "unit": "TFLOP/s", "frac": achieved / peak,
+                    "peak_source": peak_kind + " bf16 sustained (the TF32 tensor rate is half "
+                                               "of it)",
+                    "frac_of_tf32_ceiling": achieved / (peak / 2.0)}
         else:
             achieved = work / (dms / 1000.0) / 1e9
             peak = peaks['hbm_gbs']
             roof = {"kernel": name, "bound": "hbm", "achieved": achieved, "peak": peak,
-                    "unit": "GB/s", "frac": achieved / peak, "traffic": None,
-                    "peak_source": peak_kind, "launches": cnt, "share": dms / tot_ms}
+                    "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind}
+        # DRAM bytes of one representative launch from a committed ncu capture
+        roof["traffic"] = tr.get("dram_bytes")
+        if tr:
+            roof["traffic_launch"] = tr.get("launch")
+            roof["traffic_algorithmic_bytes"] = tr.get("algorithmic_bytes")
+            roof["traffic_source"] = tr.get("source")
+        roof["launches"] = cnt
+        roof["share"] = dms / tot_ms
         roof["by_class_ms"] = {k: round(v[0] / args.steps, 3) for k, v in prof.items()}
+        if 'assemble' in prof:
+            ams, awork, acnt = prof['assemble']
+            roof["assembly"] = {"achieved_GBs": awork / (ams / 1000.0) / 1e9,
+                                "peak_GBs": peaks['hbm_gbs'],
+                                "frac": awork / (ams / 1000.0) / 1e9 / peaks['hbm_gbs'],
+                                "traffic": (traffic.get('assemble') or {}).get("dram_bytes")}
 
     accuracy = None
+    fp64 = None
     if rank == 0 and not args.no_accuracy:
-        # extinction of this path against the plain FP64 GPU path on the same sweep
+        # every result of this path against the plain FP64 GPU path on the same
+        # 81-wavelength sweep: sigma, h, extinction, scattering
         refine_iters.clear()
-        ext_p = ext_of(device_step())
+        xm, ext_m, sca_m = full_solutions(solver)
         iters = list(refine_iters)
+        solver._mixed_cache = None
+        torch.cuda.empty_cache()
         ref_solver = solver if args.path == 'fp64' else bem.BEMRet(cp, precision='fp64')
-        torch.cuda.synchronize()
-        t0 = time.time()
-        ext_64 = ext_of(device_step(ref_solver))
-        torch.cuda.synchronize()
-        t64 = time.time() - t0
-        accuracy = {"ext_max_rel_err_vs_fp64": float(np.max(np.abs(ext_p - ext_64) / np.abs(ext_64))),
-                    "fp64_path_lambda_solves_per_s": NLAM / t64,
-                    "fp64_path_sample": "one sweep, wall clock"}
+        x64, ext_64, sca_64 = full_solutions(ref_solver)
+        accuracy = {"vs": "plain FP64 GPU path (itself within 1e-10 of the reference on sigma, "
+                          "tests/test_gpu_parity.py)", "wavelengths": NLAM}
+        accuracy.update(solution_errors(xm, x64, ext_m, ext_64, sca_m, sca_64))
         if iters:
             accuracy["refine_corrections_mean"] = float(np.mean(iters))
             accuracy["refine_corrections_max"] = int(np.max(iters))
+        # the FP64 path timed exactly like the headline: same warm-up and steps,
+        # CUDA events around the timed sweeps
+        fsteps = args.fp64_steps if args.fp64_steps is not None else args.steps
+        for _ in range(args.warmup):
+            device_step(ref_solver)
+        torch.cuda.synchronize()
+        f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        f0.record()
+        for _ in range(fsteps):
+            device_step(ref_solver)
+        f1.record()
+        torch.cuda.synchronize()
+        fms = f0.elapsed_time(f1)
+        fp64 = {"value": NLAM * fsteps / (fms / 1000.0), "unit": UNIT,
+                "ms_per_step": fms / fsteps, "steps": fsteps, "warmup": args.warmup,
+                "timing": "CUDA events over the timed sweeps after the warm-up sweeps, as the "
+                          "headline"}
+        fp64["speedup_value"] = value / fp64["value"]
+        fp64["speedup_e2e"] = e2e_value / fp64["value"]
         del ref_solver
+        torch.cuda.empty_cache()
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -522,7 +654,7 @@ def main():
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f64" if args.path == 'fp64' else "tf32/bf16x3+f64-refine",
+            "dtype": "f64" if args.path == 'fp64' else "tf32+f64-refine",
             "data": "synthetic",
             "config": {"workload": WORKLOAD, "path": args.path, "batch_wavelengths": B,
                        "refine_tol": solver.refine_tol if args.path == 'mixed' else None,
@@ -537,6 +669,7 @@ def main():
                     "d2h_bytes_per_step": d2h},
             "gpu_launches": launches,
             "accuracy": accuracy,
+            "fp64_path": fp64,
             "roofline": roof,
             "cpu_baseline": cpu,
             "clocks": ck,

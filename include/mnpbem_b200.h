@@ -360,6 +360,53 @@ int mnpb_stat_matrix(void *stream, int64_t n, int64_t batch, const double *F, in
                      const double *eps12, double *M, int64_t ld, int64_t stride);
 
 /* ---------------------------------------------------------------------------
+ * Green functions of one region pair, entry by entry, and their products
+ * ------------------------------------------------------------------------- */
+
+/* Keys of mnpb_green_eval / mnpb_green_apply (compgreen_ret.py:507-553). */
+#define MNPB_KEY_G 0
+#define MNPB_KEY_F 1
+#define MNPB_KEY_H1 2
+#define MNPB_KEY_H2 3
+#define MNPB_KEY_GP 4   /* Cartesian derivative, 3 components */
+#define MNPB_KEY_H1P 5
+#define MNPB_KEY_H2P 6
+
+/* Entries of the region-pair Green function for `key` at one wavelength.
+ * Replaces mnpbem/greenfun/compgreen_ret.py:507-738 (eval, eval_block, and
+ * eval with `ind`, _eval2 / eval_ind at 859-908, 1770-1857) with the entries
+ * of greenret_refined.py:654-867; with kblk = 0 the quasistatic entries of
+ * mnpbem/greenfun/compgreen_stat.py:678-990 (CompGreenStat.eval).
+ * Tables (device): face data, particle offsets poff (host, nparts+1), kblk
+ * (nparts x nparts complex, re/im) and sblk (nparts x nparts; 0 = block not
+ * connected) of the region pair, the refined pairs as CSR (rptr n+1, cols
+ * ascending within a row) with g (nref x 6), fn (nref x 6), f (nref x 3 x 6).
+ * ind == NULL: columns [col_start, col_start + ncol), out row-major complex
+ * (n x ncol), or (n x 3 x ncol) for vector keys.  Otherwise the nind entries
+ * at row-major linear indices ind (device int64, i * n + j): out (nind) or
+ * (nind x 3). */
+int mnpb_green_eval(void *stream, int64_t n, const double *pos, const double *nvec,
+                    const double *area, int nparts, const int64_t *poff, const double *kblk,
+                    const double *sblk, const int64_t *rptr, const int32_t *cols,
+                    const double *g, const double *fn, const double *f, int key,
+                    int64_t col_start, int64_t ncol, const int64_t *ind, int64_t nind,
+                    double *out);
+
+/* Products with the region-pair Green function, entries computed on the fly
+ * (no n x n storage), for potentials and fields at the faces.  Replaces the
+ * matmul / cross of mnpbem/greenfun/compgreen_ret.py:912-1136 (field,
+ * potential).  x, y device, row-major complex:
+ *   mode 0, scalar key: y (n x m)     = M x, x (n x m), m <= 12
+ *   mode 1, vector key: y (n x 3 x m) = Gp x, x (n x m), m <= 4
+ *   mode 2, vector key: y (n x 3 x m) = sum_j Gp_ij cross x_j, x (n x 3 x m),
+ *                       m <= 4. */
+int mnpb_green_apply(void *stream, int64_t n, const double *pos, const double *nvec,
+                     const double *area, int nparts, const int64_t *poff, const double *kblk,
+                     const double *sblk, const int64_t *rptr, const int32_t *cols,
+                     const double *g, const double *fn, const double *f, int key, int mode,
+                     int64_t m, const double *x, double *y);
+
+/* ---------------------------------------------------------------------------
  * Plane-wave excitation and cross sections (batched over wavelengths)
  * ------------------------------------------------------------------------- */
 

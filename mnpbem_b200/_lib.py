@@ -83,6 +83,10 @@ SIGNATURES = {
     'mnpb_mlp_adam': [_P, _I64, _P, _P, _P, _P, _P, _D, _D, _D, _D, _I64],
     'mnpb_mlp_to_bf16': [_P, _I64, _P, _P],
     'mnpb_stat_matrix': [_P, _I64, _I64, _P, _I64, _P, _P, _I64, _I64],
+    'mnpb_green_eval': [_P, _I64, _P, _P, _P, _I, _P, _P, _P, _P, _P, _P, _P, _P, _I, _I64, _I64,
+                        _P, _I64, _P],
+    'mnpb_green_apply': [_P, _I64, _P, _P, _P, _I, _P, _P, _P, _P, _P, _P, _P, _P, _I, _I, _I64,
+                         _P, _P],
     'mnpb_planewave_potential': [_P, _I64, _I64, _I64, _P, _P, _P, _P, _P, _P, _P, _P, _P],
     'mnpb_farfield': [_P, _I64, _I64, _I64, _I64, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P],
 }

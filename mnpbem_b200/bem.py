@@ -311,6 +311,21 @@ class BEMRet(object):
     def __truediv__(self, exc):
         return self.solve(exc)
 
+    def potential(self, sig, inout=2):
+        """Potentials and surface derivatives inside (1) or outside (2) of the
+        particle for a solution (bem_ret.py:1833-1858, delegating to
+        CompGreenRet.potential); the Green-function entries are evaluated on
+        the fly on the GPU.  Unlike the reference this does not factorise the
+        BEM matrices of ``sig.enei`` first: potentials need only G and H."""
+        return self.g.potential(sig, inout)
+
+    def field(self, sig, inout=2):
+        """Electric and magnetic fields inside (1) or outside (2) of the
+        particle for a solution (bem_ret.py:1860-1895, delegating to
+        CompGreenRet.field: e = i k (G1 h1 + G2 h2) - H1p sig1 - H2p sig2,
+        h = H1p x h1 + H2p x h2); no factorisation needed, as for potential."""
+        return self.g.field(sig, inout)
+
     # ------------------------------------------------------- spectrum sweeps
     @staticmethod
     def pipeline(chunks, work, streams):

@@ -426,9 +426,296 @@ __global__ void assemble_refined_kernel(int64_t nref, int64_t batch, PartTable p
     st.put(b, i, j, out[0], out[1], out[2], out[3]);
 }
 
+// ---------------------------------------------------------------------------
+// Region-pair Green functions entry by entry and their products with surface
+// charges and currents.
+//
+// CompGreenRet.eval / eval_block / eval(ind) (mnpbem/greenfun/compgreen_ret.py:
+// 507-738, 859-908) assemble, for region pair (i, j), every particle block
+// whose connectivity is non-zero at that block's wavenumber; the entries are
+// those of GreenRetRefined.eval (greenret_refined.py:654-867): the far formula
+// with the phase, the refined Taylor sum on near/self pairs, H1/H2 = F +- 2 pi
+// and H1p/H2p = Gp +- 2 pi nvec on the diagonal.  Gp is the Cartesian
+// derivative (faux r a e^{ikd}, refined sum_n f[:, c, n] (ik)^n).  With k = 0
+// the same entries are the quasistatic ones of CompGreenStat (compgreen_stat.py:
+// 219-464, 859-990): e^0 = 1 and (ik)^n = 0 for n > 0 leave the order-0
+// coefficients, which equal the static refined values.
+// ---------------------------------------------------------------------------
+enum GreenKey { GK_G = 0, GK_F = 1, GK_H1 = 2, GK_H2 = 3, GK_GP = 4, GK_H1P = 5, GK_H2P = 6 };
+
+struct EvalTables {
+    int64_t n;
+    PartTable parts;
+    const double *pos, *nvec, *area;
+    const double *kblk;    // nparts x nparts complex wavenumbers (re, im)
+    const double *sblk;    // nparts x nparts factors (0: block not connected)
+    const int64_t *rptr;   // refined pairs, CSR by row, columns ascending
+    const int32_t *cols;
+    const double *g, *fn, *f;   // (nref, 6), (nref, 6), (nref, 3, 6)
+};
+
+__device__ __forceinline__ int64_t find_refined(const EvalTables &t, int64_t i, int64_t j) {
+    int64_t lo = t.rptr[i], hi = t.rptr[i + 1];
+    while (lo < hi) {
+        const int64_t mid = (lo + hi) >> 1;
+        const int64_t c = t.cols[mid];
+        if (c < j)
+            lo = mid + 1;
+        else if (c > j)
+            hi = mid;
+        else
+            return mid;
+    }
+    return -1;
+}
+
+// Entry (i, j) for `key`: v[0] for scalar keys, v[0..2] for Gp/H1p/H2p.
+__device__ void green_entry(const EvalTables &t, int key, int64_t i, int64_t j, cd v[3]) {
+    v[0] = v[1] = v[2] = cmk(0.0, 0.0);
+    const int np = t.parts.nparts;
+    const int64_t blk = (int64_t)part_of(t.parts, i) * np + part_of(t.parts, j);
+    const double sg = t.sblk[blk];
+    if (sg == 0.0) return;
+    const cd k = cmk(t.kblk[2 * blk], t.kblk[2 * blk + 1]);
+    const double x = t.pos[3 * i] - t.pos[3 * j];
+    const double y = t.pos[3 * i + 1] - t.pos[3 * j + 1];
+    const double z = t.pos[3 * i + 2] - t.pos[3 * j + 2];
+    double d = sqrt(x * x + y * y + z * z);
+    if (d < kEps || i == j) d = kEps;
+    const bool vec = key >= GK_GP;
+    const cd ph = cexpi(k, d);
+    const int64_t p = find_refined(t, i, j);
+    if (p >= 0) {
+        const cd ik = cmk(-k.y, k.x);
+        cd pw = cmk(1.0, 0.0), s0 = cmk(0.0, 0.0), s1 = s0, s2 = s0;
+        for (int m = 0; m <= kOrder; ++m) {
+            if (!vec) {
+                s0 = cadd(s0, cscale(pw, key == GK_G ? t.g[6 * p + m] : t.fn[6 * p + m]));
+            } else {
+                s0 = cadd(s0, cscale(pw, t.f[18 * p + m]));
+                s1 = cadd(s1, cscale(pw, t.f[18 * p + 6 + m]));
+                s2 = cadd(s2, cscale(pw, t.f[18 * p + 12 + m]));
+            }
+            pw = cmul(pw, ik);
+        }
+        v[0] = cmul(s0, ph);
+        if (vec) {
+            v[1] = cmul(s1, ph);
+            v[2] = cmul(s2, ph);
+        }
+    } else {
+        const double a = t.area[j];
+        const double inv_d = 1.0 / d;
+        if (key == GK_G) {
+            v[0] = cscale(ph, a * inv_d);
+        } else {
+            const double inv_d2 = inv_d * inv_d;
+            const cd faux = cmk((-k.y - inv_d) * inv_d2, k.x * inv_d2);
+            if (!vec) {
+                const double nx = t.nvec[3 * i], ny = t.nvec[3 * i + 1], nz = t.nvec[3 * i + 2];
+                const cd tt = cadd(cadd(cscale(faux, nx * x), cscale(faux, ny * y)),
+                                   cscale(faux, nz * z));
+                v[0] = cmul(cscale(tt, a), ph);
+            } else {
+                v[0] = cmul(cscale(cscale(faux, x), a), ph);
+                v[1] = cmul(cscale(cscale(faux, y), a), ph);
+                v[2] = cmul(cscale(cscale(faux, z), a), ph);
+            }
+        }
+    }
+    if (sg != 1.0)
+        for (int c = 0; c < 3; ++c) v[c] = cscale(v[c], sg);
+    if (i == j) {
+        const double two_pi = 6.283185307179586;
+        if (key == GK_H1) v[0].x += two_pi;
+        if (key == GK_H2) v[0].x -= two_pi;
+        if (key == GK_H1P || key == GK_H2P) {
+            const double sgn = key == GK_H1P ? two_pi : -two_pi;
+            for (int c = 0; c < 3; ++c) v[c].x += sgn * t.nvec[3 * i + c];
+        }
+    }
+}
+
+// Dense column range [c0, c0 + ncol) (ind == NULL; out row-major (n, ncol) or
+// (n, 3, ncol)), or the entries at row-major linear indices ind[0..nind)
+// (out (nind) or (nind, 3)).
+__global__ void __launch_bounds__(256) green_eval_kernel(EvalTables t, int key, int64_t c0,
+                                                         int64_t ncol, const int64_t *ind,
+                                                         int64_t nind, cd *out) {
+    const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const bool vec = key >= GK_GP;
+    cd v[3];
+    if (ind) {
+        if (tid >= nind) return;
+        const int64_t l = ind[tid];
+        green_entry(t, key, l / t.n, l % t.n, v);
+        if (vec)
+            for (int c = 0; c < 3; ++c) out[3 * tid + c] = v[c];
+        else
+            out[tid] = v[0];
+        return;
+    }
+    if (tid >= t.n * ncol) return;
+    const int64_t i = tid / ncol, jj = tid - i * ncol;
+    green_entry(t, key, i, c0 + jj, v);
+    if (vec)
+        for (int c = 0; c < 3; ++c) out[(i * 3 + c) * ncol + jj] = v[c];
+    else
+        out[tid] = v[0];
+}
+
+// Products with the region-pair matrix, one CTA per row i, entries computed
+// on the fly (no n x n storage):
+//   mode 0 (scalar key): y(i, c)    = sum_j M_ij x(j, c),             c < m
+//   mode 1 (vector key): y(i, q, c) = sum_j Gp_ij[q] x(j, c),         c < m
+//   mode 2 (vector key): y(i, :, c) = sum_j Gp_ij x x(j, :, c)  (cross product)
+// x, y row-major complex; m <= APPLY_MAXM columns (m <= APPLY_MAXM / 3 for
+// modes 1 and 2).
+constexpr int APPLY_MAXM = 12;
+constexpr int APPLY_T = 128;
+
+__global__ void __launch_bounds__(APPLY_T) green_apply_kernel(EvalTables t, int key, int mode,
+                                                              int m, const cd *__restrict__ x,
+                                                              cd *__restrict__ y) {
+    const int64_t i = blockIdx.x;
+    const int nout = mode == 0 ? m : 3 * m;
+    double acc[2 * APPLY_MAXM];
+#pragma unroll
+    for (int q = 0; q < 2 * APPLY_MAXM; ++q) acc[q] = 0.0;
+    for (int64_t j = threadIdx.x; j < t.n; j += APPLY_T) {
+        cd v[3];
+        green_entry(t, key, i, j, v);
+        if (mode == 0) {
+#pragma unroll
+            for (int c = 0; c < APPLY_MAXM; ++c)
+                if (c < m) {
+                    const cd r = cmul(v[0], x[j * m + c]);
+                    acc[2 * c] += r.x;
+                    acc[2 * c + 1] += r.y;
+                }
+        } else if (mode == 1) {
+#pragma unroll
+            for (int c = 0; c < APPLY_MAXM / 3; ++c)
+                if (c < m) {
+                    const cd xv = x[j * m + c];
+#pragma unroll
+                    for (int q = 0; q < 3; ++q) {
+                        const cd r = cmul(v[q], xv);
+                        acc[2 * (q * m + c)] += r.x;
+                        acc[2 * (q * m + c) + 1] += r.y;
+                    }
+                }
+        } else {
+#pragma unroll
+            for (int c = 0; c < APPLY_MAXM / 3; ++c)
+                if (c < m) {
+                    const cd hx = x[(j * 3 + 0) * m + c], hy = x[(j * 3 + 1) * m + c],
+                             hz = x[(j * 3 + 2) * m + c];
+                    const cd r0 = csub(cmul(v[1], hz), cmul(v[2], hy));
+                    const cd r1 = csub(cmul(v[2], hx), cmul(v[0], hz));
+                    const cd r2 = csub(cmul(v[0], hy), cmul(v[1], hx));
+                    acc[2 * (0 * m + c)] += r0.x;
+                    acc[2 * (0 * m + c) + 1] += r0.y;
+                    acc[2 * (1 * m + c)] += r1.x;
+                    acc[2 * (1 * m + c) + 1] += r1.y;
+                    acc[2 * (2 * m + c)] += r2.x;
+                    acc[2 * (2 * m + c) + 1] += r2.y;
+                }
+        }
+    }
+    __shared__ double red[APPLY_T / 32][2 * APPLY_MAXM];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+#pragma unroll
+    for (int q = 0; q < 2 * APPLY_MAXM; ++q) {
+        const double w = warp_sum(acc[q]);
+        if (lane == 0) red[warp][q] = w;
+    }
+    __syncthreads();
+    if (threadIdx.x < 2 * nout) {
+        double sum = 0.0;
+        for (int w = 0; w < APPLY_T / 32; ++w) sum += red[w][threadIdx.x];
+        reinterpret_cast<double *>(y + i * nout)[threadIdx.x] = sum;
+    }
+}
+
 }  // namespace mnpb
 
 using namespace mnpb;
+
+static int eval_tables(EvalTables &t, int64_t n, const double *pos, const double *nvec,
+                       const double *area, int nparts, const int64_t *poff, const double *kblk,
+                       const double *sblk, const int64_t *rptr, const int32_t *cols,
+                       const double *g, const double *fn, const double *f, const char *what) {
+    MNPB_REQUIRE(n > 0 && n < (int64_t(1) << 31), "%s: bad n", what);
+    MNPB_REQUIRE(nparts >= 1 && nparts <= kMaxParts, "%s: nparts must be 1..%d", what,
+                 kMaxParts);
+    MNPB_REQUIRE(pos && nvec && area && poff && kblk && sblk && rptr && cols && g && fn && f,
+                 "%s: null pointer", what);
+    t.n = n;
+    t.parts.nparts = nparts;
+    for (int p = 0; p <= nparts; ++p) t.parts.off[p] = poff[p];
+    MNPB_REQUIRE(t.parts.off[0] == 0 && t.parts.off[nparts] == n, "%s: bad offsets", what);
+    t.pos = pos;
+    t.nvec = nvec;
+    t.area = area;
+    t.kblk = kblk;
+    t.sblk = sblk;
+    t.rptr = rptr;
+    t.cols = cols;
+    t.g = g;
+    t.fn = fn;
+    t.f = f;
+    return MNPB_OK;
+}
+
+extern "C" int mnpb_green_eval(void *stream, int64_t n, const double *pos, const double *nvec,
+                               const double *area, int nparts, const int64_t *poff,
+                               const double *kblk, const double *sblk, const int64_t *rptr,
+                               const int32_t *cols, const double *g, const double *fn,
+                               const double *f, int key, int64_t col_start, int64_t ncol,
+                               const int64_t *ind, int64_t nind, double *out) {
+    clear_error();
+    EvalTables t;
+    MNPB_TRY(eval_tables(t, n, pos, nvec, area, nparts, poff, kblk, sblk, rptr, cols, g, fn, f,
+                         "green_eval"));
+    MNPB_REQUIRE(key >= GK_G && key <= GK_H2P, "green_eval: key must be 0..6");
+    MNPB_REQUIRE(out, "green_eval: null output");
+    const int64_t tot = ind ? nind : n * ncol;
+    if (!ind)
+        MNPB_REQUIRE(col_start >= 0 && ncol >= 0 && col_start + ncol <= n,
+                     "green_eval: column range [%lld, %lld) outside [0, %lld)",
+                     (long long)col_start, (long long)(col_start + ncol), (long long)n);
+    else
+        MNPB_REQUIRE(nind >= 0, "green_eval: nind < 0");
+    if (tot == 0) return MNPB_OK;
+    cudaStream_t s = as_stream(stream);
+    green_eval_kernel<<<ceil_div(tot, 256), 256, 0, s>>>(t, key, col_start, ncol, ind, nind,
+                                                        (cd *)out);
+    MNPB_LAUNCH_CHECK("green_eval_kernel");
+    return MNPB_OK;
+}
+
+extern "C" int mnpb_green_apply(void *stream, int64_t n, const double *pos, const double *nvec,
+                                const double *area, int nparts, const int64_t *poff,
+                                const double *kblk, const double *sblk, const int64_t *rptr,
+                                const int32_t *cols, const double *g, const double *fn,
+                                const double *f, int key, int mode, int64_t m, const double *x,
+                                double *y) {
+    clear_error();
+    EvalTables t;
+    MNPB_TRY(eval_tables(t, n, pos, nvec, area, nparts, poff, kblk, sblk, rptr, cols, g, fn, f,
+                         "green_apply"));
+    MNPB_REQUIRE(key >= GK_G && key <= GK_H2P, "green_apply: key must be 0..6");
+    MNPB_REQUIRE(mode >= 0 && mode <= 2 && (mode == 0) == (key < GK_GP),
+                 "green_apply: mode 0 takes a scalar key, modes 1 and 2 a vector key");
+    MNPB_REQUIRE(m >= 1 && m <= (mode == 0 ? APPLY_MAXM : APPLY_MAXM / 3),
+                 "green_apply: m = %lld columns out of range", (long long)m);
+    MNPB_REQUIRE(x && y, "green_apply: null pointer");
+    green_apply_kernel<<<(unsigned)n, APPLY_T, 0, as_stream(stream)>>>(t, key, mode, (int)m,
+                                                                       (const cd *)x, (cd *)y);
+    MNPB_LAUNCH_CHECK("green_apply_kernel");
+    return MNPB_OK;
+}
 
 extern "C" int mnpb_refine_coefficients(void *stream, int64_t n, const double *pos,
                                         const double *nvec, const double *tvec1,

@@ -22,6 +22,7 @@ import torch
 
 from . import _lib
 from ._lib import call, ptr
+from .compstruct import CompStruct
 from .materials import eps_k
 
 __all__ = ["SurfaceTables", "CompGreenRet", "CompGreenStat", "region_tables"]
@@ -138,6 +139,8 @@ class SurfaceTables(object):
         self.h_pos, self.h_nvec, self.h_area = pos, nvec, area
         rptr, cols, kinds = refinematrix_csr(pos, pos, rad, rad, abs_cutoff, rel_cutoff)
         rows = np.repeat(np.arange(n, dtype=np.int32), np.diff(rptr)).astype(np.int32)
+        if len(cols) > 1 and not np.all((np.diff(cols) > 0) | (np.diff(rows) != 0)):
+            raise RuntimeError("refinematrix: columns not ascending within a row")
         self.h_rptr, self.h_rows, self.h_cols, self.h_kinds = rptr, rows, cols, kinds
         self.nref = len(cols)
         qpos, qw, qoff = _points(p, 'quad')
@@ -236,6 +239,69 @@ class SurfaceTables(object):
         return d_k, d_s
 
 
+    # ---- entries and products of one region pair ---------------------------
+    def _eval_args(self, kb, sb):
+        dev = self.device
+        d_k = torch.from_numpy(np.ascontiguousarray(kb, dtype=np.float64)).to(dev)
+        d_s = torch.from_numpy(np.ascontiguousarray(sb, dtype=np.float64)).to(dev)
+        poff = np.ascontiguousarray(self.part_off, dtype=np.int64)
+        return (self.n, ptr(self.pos), ptr(self.nvec), ptr(self.area), self.nparts, ptr(poff),
+                ptr(d_k), ptr(d_s), ptr(self.rptr), ptr(self.cols), ptr(self.g), ptr(self.fn),
+                ptr(self.f)), (d_k, d_s)
+
+    def green_eval(self, kb, sb, key, col_start=0, ncol=None, ind=None, stream=None):
+        """Device entries of the region pair given by the block tables kb
+        (np, np, 2), sb (np, np): columns [col_start, col_start + ncol) as
+        (n, ncol) / (n, 3, ncol) complex, or the entries at row-major linear
+        indices ``ind`` as (len(ind),) / (len(ind), 3)."""
+        args, keep = self._eval_args(kb, sb)
+        vec = key >= KEYS['Gp']
+        c128 = dict(dtype=torch.complex128, device=self.device)
+        if ind is not None:
+            d_ind = torch.from_numpy(np.ascontiguousarray(ind, dtype=np.int64)).to(self.device)
+            nind = d_ind.numel()
+            out = torch.zeros((nind, 3) if vec else (nind,), **c128)
+            call('mnpb_green_eval', _lib.stream_handle(stream), *args, key, 0, 0, ptr(d_ind),
+                 nind, ptr(out))
+            return out
+        ncol = self.n - col_start if ncol is None else ncol
+        out = torch.zeros((self.n, 3, ncol) if vec else (self.n, ncol), **c128)
+        call('mnpb_green_eval', _lib.stream_handle(stream), *args, key, col_start, ncol, None,
+             0, ptr(out))
+        return out
+
+    def green_apply(self, kb, sb, key, x, stream=None):
+        """Product of the region-pair matrix with device vectors, entries on
+        the fly: scalar key, x (n, m) -> (n, m); vector key, x (n, m) ->
+        (n, 3, m); vector key, x (n, 3, m) -> cross products (n, 3, m)."""
+        args, keep = self._eval_args(kb, sb)
+        vec = key >= KEYS['Gp']
+        x = x.to(torch.complex128).contiguous()
+        n = self.n
+        if not vec:
+            outs = []
+            for c0 in range(0, x.shape[1], 12):
+                xx = x[:, c0:c0 + 12].contiguous()
+                y = torch.empty_like(xx)
+                call('mnpb_green_apply', _lib.stream_handle(stream), *args, key, 0,
+                     xx.shape[1], ptr(xx), ptr(y))
+                outs.append(y)
+            return torch.cat(outs, dim=1)
+        mode = 2 if x.dim() == 3 else 1
+        m = x.shape[-1]
+        outs = []
+        for c0 in range(0, m, 4):
+            xx = x[..., c0:c0 + 4].contiguous()
+            y = torch.empty((n, 3, xx.shape[-1]), dtype=torch.complex128, device=self.device)
+            call('mnpb_green_apply', _lib.stream_handle(stream), *args, key, mode,
+                 xx.shape[-1], ptr(xx), ptr(y))
+            outs.append(y)
+        return torch.cat(outs, dim=2)
+
+
+KEYS = {'G': 0, 'F': 1, 'H1': 2, 'H2': 3, 'Gp': 4, 'H1p': 5, 'H2p': 6}
+
+
 def region_tables(tables, i, j, enei):
     """k/sign tables selecting region pair (i, j) on side 1 (compgreen_ret.py:739-858)."""
     npart = tables.nparts
@@ -256,9 +322,13 @@ def region_tables(tables, i, j, enei):
 class CompGreenRet(object):
     """Retarded Green function of a particle with itself (refined, closed).
 
-    ``eval(i, j, key, enei)`` -> (n, n) complex host matrix for region pair
-    (i, j) (0 inside, 1 outside), key in G, F, H1, H2; 0 if no block
-    connects (compgreen_ret.py:507-553, 739-858).
+    ``eval(i, j, key, enei[, ind])`` -> the (n, n) complex host matrix of
+    region pair (i, j) (0 inside, 1 outside) for key G, F, H1, H2, or (n, 3, n)
+    for the Cartesian derivatives Gp, H1p, H2p; 0 if no block connects
+    (compgreen_ret.py:507-553, 739-858).  ``eval_block`` returns a column
+    range, ``potential`` / ``field`` the potentials and fields at the faces
+    of a solution (compgreen_ret.py:912-1036), computed with on-the-fly
+    entries (no n x n matrix is stored for them).
     """
 
     def __init__(self, p1, p2=None, **options):
@@ -276,34 +346,143 @@ class CompGreenRet(object):
         self.con = [[np.where(io[:, a][:, None] == io[:, b][None, :], io[:, a][:, None], 0)
                      for b in range(2)] for a in range(2)]
 
+    def _blocks(self, i, j, enei):
+        kblk, sblk = region_tables(self.tables, i, j, enei)
+        return kblk[0, 0], sblk[0, 0]
+
+    @staticmethod
+    def _key(key):
+        if key not in KEYS:
+            raise ValueError("Unknown key: {}".format(key))
+        return KEYS[key]
+
     def eval(self, i, j, key, enei, ind=None):
+        """Region-pair matrix (compgreen_ret.py:507-553).  With ``ind``
+        (row-major linear indices i * n + j, as the reference's _eval2) the
+        selected entries, (len(ind),) or (len(ind), 3); entries of blocks
+        that are not connected are 0."""
+        kk = self._key(key)
+        kb, sb = self._blocks(i, j, enei)
         if ind is not None:
-            raise NotImplementedError("CompGreenRet.eval: selected elements")
-        if key not in ('G', 'F', 'H1', 'H2'):
-            raise NotImplementedError("CompGreenRet.eval: key {}".format(key))
+            ind = np.asarray(ind, dtype=np.int64).ravel()
+            n = self.tables.n
+            if ind.size and (ind.min() < 0 or ind.max() >= n * n):
+                raise IndexError("CompGreenRet.eval: index out of range")
+            out = self.tables.green_eval(kb, sb, kk, ind=ind)
+            torch.cuda.synchronize()
+            return out.cpu().numpy()
         if not np.any(self.con[i][j]):
             return 0
-        t = self.tables
-        n = t.n
-        kblk, sblk = region_tables(t, i, j, enei)
-        bufs = [torch.empty((1, n, n), dtype=torch.complex128, device=t.device) for _ in range(4)]
-        t.assemble(kblk, sblk, bufs, mode=0)
-        torch.cuda.synchronize()
-        G1, H1, G2, H2 = [b[0].cpu().numpy().T for b in bufs]
-        if key == 'G':
-            return np.ascontiguousarray(G1)
-        if key == 'H1':
-            return np.ascontiguousarray(H1)
-        if key == 'H2':
-            return np.ascontiguousarray(H2)
-        F = H1.copy()
-        F[np.diag_indices(n)] -= TWO_PI
-        return F
+        out = self.tables.green_eval(kb, sb, kk).cpu().numpy()
+        if not np.any(out):
+            return 0
+        return out
+
+    def eval_block(self, i, j, key, enei, col_start, col_stop):
+        """Columns [col_start, col_stop) of ``eval(i, j, key, enei)``
+        (compgreen_ret.py:555-617): (n, ncol), or (n, 3, ncol) for Gp/H1p/H2p;
+        zeros if no block connects."""
+        kk = self._key(key)
+        col_start, col_stop = int(col_start), int(col_stop)
+        if not (0 <= col_start <= col_stop <= self.tables.n):
+            raise ValueError("eval_block col range ({}, {}) out of bounds for p2.n={}"
+                             .format(col_start, col_stop, self.tables.n))
+        kb, sb = self._blocks(i, j, enei)
+        out = self.tables.green_eval(kb, sb, kk, col_start=col_start,
+                                     ncol=col_stop - col_start)
+        return out.cpu().numpy()
+
+    # ---- potentials and fields at the faces --------------------------------
+    def _apply(self, region, col, key, x):
+        """M(region, col; key) applied to device x, or None if no block of
+        the region pair is connected (the reference's matmul with 0)."""
+        if not np.any(self.con[region][col]):
+            return None
+        kb, sb = self._blocks(region, col, self._enei)
+        return self.tables.green_apply(kb, sb, KEYS[key], x)
+
+    @staticmethod
+    def _as_cols(v, n, vec):
+        """(n[, 3][, K]) host array -> device (n, K) or (n, 3, K), and K."""
+        a = np.asarray(v, dtype=complex)
+        if vec:
+            a = a.reshape(n, 3, -1)
+        else:
+            a = a.reshape(n, -1)
+        return torch.from_numpy(np.ascontiguousarray(a)).cuda(), a.shape[-1]
+
+    def potential(self, sig, inout=1):
+        """Potentials and surface derivatives inside (inout=1) or outside
+        (inout=2) from sigma/h (compgreen_ret.py:980-1036): phi = G1 sig1 +
+        G2 sig2, phip with H1/H2, a and ap with the currents."""
+        n = self.tables.n
+        self._enei = sig.enei
+        r = min(inout - 1, 1)
+        hk = 'H1' if inout == 1 else 'H2'
+        s1, K = self._as_cols(sig.sig1, n, False)
+        s2, _ = self._as_cols(sig.sig2, n, False)
+        h1, _ = self._as_cols(sig.h1, n, True)
+        h2, _ = self._as_cols(sig.h2, n, True)
+        sh = s1.ndim
+
+        def comb(key, x1, x2, vec):
+            out = None
+            for col, x in ((0, x1), (1, x2)):
+                xx = x.reshape(n, -1) if vec else x
+                y = self._apply(r, col, key, xx)
+                if y is not None:
+                    out = y if out is None else out + y
+            if out is None:
+                return 0
+            out = out.cpu().numpy()
+            out = out.reshape(n, 3, -1) if vec else out
+            return out[..., 0] if K == 1 else out
+
+        phi, phip = comb('G', s1, s2, False), comb(hk, s1, s2, False)
+        a, ap = comb('G', h1, h2, True), comb(hk, h1, h2, True)
+        del sh
+        if inout == 1:
+            return CompStruct(self.p1, sig.enei, phi1=phi, phi1p=phip, a1=a, a1p=ap)
+        return CompStruct(self.p1, sig.enei, phi2=phi, phi2p=phip, a2=a, a2p=ap)
+
+    def field(self, sig, inout=1):
+        """Electric and magnetic fields inside (inout=1) or outside (inout=2)
+        (compgreen_ret.py:912-978): e = i k (G1 h1 + G2 h2) - Hp1 sig1 -
+        Hp2 sig2, h = Hp1 x h1 + Hp2 x h2 with Hp = H1p (inside) or H2p
+        (outside) of both column regions, k = 2 pi / enei."""
+        n = self.tables.n
+        self._enei = sig.enei
+        k = 2 * np.pi / sig.enei
+        r = min(inout - 1, 1)
+        pk = 'H1p' if inout == 1 else 'H2p'
+        s1, K = self._as_cols(sig.sig1, n, False)
+        s2, _ = self._as_cols(sig.sig2, n, False)
+        h1, _ = self._as_cols(sig.h1, n, True)
+        h2, _ = self._as_cols(sig.h2, n, True)
+        e = torch.zeros((n, 3, K), dtype=torch.complex128, device='cuda')
+        hh = torch.zeros_like(e)
+        for col, s, h in ((0, s1, h1), (1, s2, h2)):
+            g = self._apply(r, col, 'G', h.reshape(n, -1))
+            if g is not None:
+                e += 1j * k * g.reshape(n, 3, K)
+            p = self._apply(r, col, pk, s)
+            if p is not None:
+                e -= p
+            c = self._apply(r, col, pk, h)
+            if c is not None:
+                hh += c
+        e, hh = e.cpu().numpy(), hh.cpu().numpy()
+        if K == 1:
+            e, hh = e[..., 0], hh[..., 0]
+        return CompStruct(self.p1, sig.enei, e=e, h=hh)
 
 
 class CompGreenStat(object):
     """Quasistatic Green function of a particle with itself: ``F`` (refined,
-    closed-surface corrected), mnpbem/greenfun/compgreen_stat.py:219-294, 466-528."""
+    closed-surface corrected), ``G``, and ``eval(*keys, ind=...)`` for G, F,
+    H1, H2, Gp, H1p, H2p (mnpbem/greenfun/compgreen_stat.py:219-294, 466-528,
+    678-990).  Entries come from the retarded entry kernel at k = 0, where the
+    phase is 1 and only the order-0 refined coefficients remain."""
 
     def __init__(self, p1, p2=None, **options):
         if p2 is not None and p2 is not p1:
@@ -316,8 +495,53 @@ class CompGreenStat(object):
         self.F_dev = torch.empty((n, n), dtype=torch.float64, device=t.device)
         call('mnpb_static_matrix', _lib.stream_handle(), n, ptr(t.pos), ptr(t.nvec), ptr(t.area),
              ptr(t.rptr), ptr(t.cols), ptr(t.fstat), ptr(t.cdir), ptr(t.fsum), ptr(self.F_dev), n)
+        npart = t.nparts
+        self._kb = np.zeros((npart, npart, 2))
+        self._sb = np.ones((npart, npart))
 
     @property
     def F(self):
         torch.cuda.synchronize()
         return np.ascontiguousarray(self.F_dev.cpu().numpy().T)
+
+    @property
+    def G(self):
+        return self._eval_key('G', None)
+
+    def _eval_key(self, key, ind):
+        if key not in KEYS:
+            raise ValueError("Unknown key: {}".format(key))
+        if key == 'F' and ind is None:
+            return self.F
+        if ind is not None:
+            ind = np.asarray(ind, dtype=np.int64).ravel()
+        out = self.tables.green_eval(self._kb, self._sb, KEYS[key], ind=ind).cpu().numpy()
+        return out.real if key in ('G', 'F', 'H1', 'H2') else out.real.copy()
+
+    def eval(self, *args, **kwargs):
+        """``eval('G')``, ``eval('H1', 'H2')``, ``eval(ind, 'G')`` or
+        ``eval('G', ind=ind)`` (compgreen_stat.py:678-750): one array per key,
+        a tuple for several keys; ``ind`` are row-major linear indices."""
+        if len(args) == 0:
+            raise ValueError("At least one key must be provided")
+        ind = kwargs.get('ind', None)
+        if not isinstance(args[0], str):
+            ind, keys = args[0], args[1:]
+        else:
+            keys = args
+        res = [self._eval_key(k, ind) for k in keys]
+        return res[0] if len(res) == 1 else tuple(res)
+
+    def eval_block(self, key, enei, col_start, col_stop):
+        """Columns [col_start, col_stop) of ``eval(key)`` (compgreen_stat.py:
+        750-800; ``enei`` is accepted and unused, as in the reference)."""
+        if key not in KEYS:
+            raise ValueError("Unknown key: {}".format(key))
+        col_start, col_stop = int(col_start), int(col_stop)
+        if not (0 <= col_start <= col_stop <= self.tables.n):
+            raise ValueError("eval_block col range out of bounds")
+        if key == 'F':
+            return np.ascontiguousarray(self.F[:, col_start:col_stop])
+        out = self.tables.green_eval(self._kb, self._sb, KEYS[key], col_start=col_start,
+                                     ncol=col_stop - col_start).cpu().numpy()
+        return np.ascontiguousarray(out.real)

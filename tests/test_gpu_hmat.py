@@ -215,3 +215,49 @@ def test_bemretiter_dense_sphere(gpu_ok):
     for name in ('sig1', 'sig2', 'h1', 'h2'):
         assert _rel(getattr(sig, name), g['iter_d_' + name]) < 1e-8, name
     assert abs(exc.extinction(sig) - float(g['iter_d_ext'])) < 1e-8 * abs(float(g['iter_d_ext']))
+
+
+def test_bemretiter_hmatrix_rod9600(gpu_ok):
+    """trirod(20, 80, [61, 31, 101]) (9600 flat faces, the largest rod of the
+    iterative family the reference can hold in 62 GB of host memory) at 600 nm
+    against the reference's BEMRetIter (cleaf 64, htol 1e-6, unpreconditioned
+    GMRES tol 1e-6) and its dense BEMRet (golden_rod9600.npz).
+
+    * The two GMRES runs walk the same Krylov process: operator applications
+      within 10 % of the reference's, and sigma / h / extinction close to the
+      reference's iterative solution.
+    * GMRES tol 1e-6 is not an extinction tolerance on this operator: the
+      reference's own iterative extinction sits 21 % from its dense one.  With
+      tol 1e-10 the GPU solve reaches the dense extinction to the ACA accuracy."""
+    from mnpbem_b200.bem_iter import BEMRetIter
+    from mnpbem_b200.excitation import PlaneWaveRet
+    from mnpbem_b200.geometry import ComParticle, trirod
+    from mnpbem_b200.materials import EpsConst, EpsDrude
+    g = golden('golden_rod9600')
+    cp = ComParticle([EpsConst(1.0), EpsDrude(10.0, 9.065, 0.0708)],
+                     [trirod(20.0, 80.0, (61, 31, 101))], [[2, 1]], 1)
+    assert cp.n == int(g['n'])
+    exc = PlaneWaveRet([[1.0, 0.0, 0.0]], [[0.0, 0.0, 1.0]])
+    enei = float(g['enei'])
+    bem = BEMRetIter(cp, hmatrix=True, cleaf=64, htol=1e-6, preconditioner='none', tol=1e-6,
+                     maxit=200)
+    sig, _ = bem.solve(exc.potential(cp, enei))
+    flag, relres, it = bem.info()
+    nmv = bem.matvec_counts()[-1]
+    ext = exc.extinction(sig)
+    ref_it, ref_d = float(g['iter_ext']), float(g['dense_ext'])
+    errs = {name: _rel(getattr(sig, name), g['iter_' + name]) for name in ('sig1', 'sig2')}
+    print('rod 9600, tol 1e-6: matvecs %d (reference %d), ext %.10g (reference iterative '
+          '%.10g, dense %.10g), sigma vs reference iterative %s'
+          % (nmv, int(g['iter_matvecs']), ext, ref_it, ref_d, errs))
+    assert flag[-1] == 0 and relres[-1] <= 1e-6
+    assert abs(nmv - int(g['iter_matvecs'])) <= 0.1 * int(g['iter_matvecs'])
+    assert abs(ext - ref_it) / abs(ref_it) < 2e-2
+    assert max(errs.values()) < 5e-2
+    bem.tol = 1e-10
+    sig, _ = bem.solve(exc.potential(cp, enei))
+    ext10 = exc.extinction(sig)
+    print('rod 9600, tol 1e-10: matvecs %d, ext %.10g (reference dense %.10g, rel %.2e)'
+          % (bem.matvec_counts()[-1], ext10, ref_d, abs(ext10 - ref_d) / abs(ref_d)))
+    assert bem.info()[0][-1] == 0
+    assert abs(ext10 - ref_d) / abs(ref_d) < 1e-2
