@@ -156,7 +156,11 @@ int64_t mnpb_bemret_workspace_f64(int64_t n, int64_t batch);
  * H2 -> Sigma (combined, LU-factorised), D -> Delta^-1.
  * Replaces mnpbem/bem/bem_ret.py:437-523 (init).  eps (device, batch x 2
  * complex): inside / outside dielectric constants (scalar per wavelength);
- * kvac (device, batch) vacuum wavenumbers 2 pi / enei; nvec (device n x 3).
+ * kvac (device, batch) vacuum wavenumbers 2 pi / enei; nvec (device n x 3)
+ * face normals of batch entry b at nvec + b * nvec_stride (stride 0: one
+ * particle for every entry, a wavelength sweep; stride 3 n: a batch of
+ * different particles with the same face count -- this holds for
+ * mnpb_bemret_excitation, _solve_f64, _init_mixed and _solve_refine too).
  * piv (device int32, [3][batch][n]) receives the pivots of G1, G2, Sigma.
  * All matrices c128, leading dimension ld, batch stride `stride`.  When G2
  * follows G1 (G2 == G1 + batch*stride) and H2 follows H1 the two halves are
@@ -164,7 +168,7 @@ int64_t mnpb_bemret_workspace_f64(int64_t n, int64_t batch);
  * info (device int32, [2][batch]) receives the first zero pivot (1-based) or 0. */
 int mnpb_bemret_init_f64(void *stream, int64_t n, int64_t batch, double *G1, double *G2,
                          double *H1, double *H2, double *D, int64_t ld, int64_t stride,
-                         const double *eps, const double *kvac, const double *nvec,
+                         const double *eps, const double *kvac, const double *nvec, int64_t nvec_stride,
                          int32_t *piv, int32_t *info, void *work, int64_t work_bytes);
 
 /* Excitation variables phi, a, alpha, De (x_in layout of the solve) from
@@ -174,7 +178,7 @@ int mnpb_bemret_init_f64(void *stream, int64_t n, int64_t batch, double *G1, dou
  * a2 (x,y,z), a2p (x,y,z). */
 int mnpb_bemret_excitation(void *stream, int64_t n, int64_t batch, int64_t nrhs,
                            const double *pots, const double *eps, const double *kvac,
-                           const double *nvec, double *x_in);
+                           const double *nvec, int64_t nvec_stride, double *x_in);
 
 /* Surface charges/currents for nrhs excitations per wavelength.
  * Replaces mnpbem/bem/bem_ret.py:1690-1810 (solve, Eqs. 19-20 of Garcia de
@@ -186,7 +190,7 @@ int mnpb_bemret_solve_f64(void *stream, int64_t n, int64_t batch, int64_t nrhs,
                           const double *G1, const double *G2, const double *S1,
                           const double *S, const double *D, int64_t ld, int64_t stride,
                           const int32_t *piv, const double *eps, const double *kvac,
-                          const double *nvec, const double *x_in, double *x_out,
+                          const double *nvec, int64_t nvec_stride, const double *x_in, double *x_out,
                           void *work, int64_t work_bytes);
 
 /* As mnpb_assemble_ret, writing in one pass both the c128 matrices (ld,
@@ -219,7 +223,7 @@ int64_t mnpb_bemret_workspace_mixed(int64_t n, int64_t batch);
  * solver. */
 int mnpb_bemret_init_mixed(void *stream, int64_t n, int64_t batch, float *G1, float *G2,
                            float *H1, float *H2, float *D, int64_t ld, const double *eps,
-                           const double *kvac, const double *nvec, int32_t *piv, int32_t *info,
+                           const double *kvac, const double *nvec, int64_t nvec_stride, int32_t *piv, int32_t *info,
                            float *dinv, void *work, int64_t work_bytes);
 
 /* Floats of the dinv buffer (inverses of the 32 x 32 diagonal blocks of the
@@ -244,7 +248,7 @@ int mnpb_bemret_solve_refine(void *stream, int64_t n, int64_t batch, int64_t nrh
                              const float *Sp, const float *Dp, int64_t ld, const int32_t *piv,
                              const float *dinv, const double *G1, const double *G2, const double *H1,
                              const double *H2, const double *eps, const double *kvac,
-                             const double *nvec, const double *b, double *x, int max_iter,
+                             const double *nvec, int64_t nvec_stride, const double *b, double *x, int max_iter,
                              double tol, int32_t *iters, double *relres, void *work,
                              int64_t work_bytes);
 
@@ -314,6 +318,14 @@ int mnpb_cgemm_tf32_ex(void *stream, int64_t m, int64_t n, int64_t k, int64_t ba
                        int64_t ldb, int64_t planeB, int64_t sB, float beta, float *C,
                        int64_t ldc, int64_t planeC, int64_t sC, void *work, int64_t work_bytes,
                        int32_t flags);
+
+/* Launch configuration of the tensor-core GEMMs (process-wide, for the
+ * autotuner; no reference counterpart): bn_wide (64 or 128) the tile width for
+ * N > 64, persist_tiles_per_sm the tile count per SM from which the persistent
+ * kernel is used (0: never), stages the operand-ring depth (0: as many as fit,
+ * else 2..4, capped by shared memory).  Defaults 128, 2, 0.  Takes effect for
+ * launches issued afterwards; cached factorisation graphs are rebuilt. */
+int mnpb_gemm_config(int32_t bn_wide, int32_t persist_tiles_per_sm, int32_t stages);
 
 /* Same GEMM as mnpb_cgemm_tf32, but it allocates nothing and takes no
  * workspace: the packed TF32 copy of A goes into a fixed 64 MiB array of the

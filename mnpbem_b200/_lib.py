@@ -34,22 +34,18 @@ SIGNATURES = {
     'mnpb_assemble_ret2': [_P, _I64, _I64, _P, _P, _P, _I, _P, _P, _P, _I64, _P, _P, _P, _P,
                            _P, _P, _P, _P, _I64, _I64, _P, _P, _P, _P, _I64, _I64, _I64],
     'mnpb_bemret_workspace_mixed': [_I64, _I64],
-    'mnpb_bemret_init_mixed': [_P, _I64, _I64, _P, _P, _P, _P, _P, _I64, _P, _P, _P, _P, _P, _P,
-                               _P, _I64],
+    'mnpb_bemret_init_mixed': [_P, _I64, _I64, _P, _P, _P, _P, _P, _I64, _P, _P, _P, _I64, _P, _P, _P, _P, _I64],
     'mnpb_bemret_dinv_floats': [_I64, _I64],
     'mnpb_bemret_refine_workspace': [_I64, _I64, _I64],
-    'mnpb_bemret_solve_refine': [_P, _I64, _I64, _I64, _P, _P, _P, _P, _P, _I64, _P, _P, _P, _P,
-                                 _P, _P, _P, _P, _P, _P, _P, _I, _D, _P, _P, _P, _I64],
+    'mnpb_bemret_solve_refine': [_P, _I64, _I64, _I64, _P, _P, _P, _P, _P, _I64, _P, _P, _P, _P, _P, _P, _P, _P, _P, _I64, _P, _P, _I, _D, _P, _P, _P, _I64],
     'mnpb_f32_workspace': [_I64, _I64],
     'mnpb_getrf_c32p': [_P, _I64, _I64, _P, _I64, _I64, _I64, _P, _I64, _P, _P, _I64],
     'mnpb_getrs_c32p': [_P, _I64, _I64, _I64, _P, _I64, _I64, _I64, _P, _I64, _P, _I64, _I64,
                         _I64, _P, _I64],
     'mnpb_bemret_workspace_f64': [_I64, _I64],
-    'mnpb_bemret_init_f64': [_P, _I64, _I64, _P, _P, _P, _P, _P, _I64, _I64, _P, _P, _P, _P, _P,
-                             _P, _I64],
-    'mnpb_bemret_solve_f64': [_P, _I64, _I64, _I64, _P, _P, _P, _P, _P, _I64, _I64, _P, _P, _P,
-                              _P, _P, _P, _P, _I64],
-    'mnpb_bemret_excitation': [_P, _I64, _I64, _I64, _P, _P, _P, _P, _P],
+    'mnpb_bemret_init_f64': [_P, _I64, _I64, _P, _P, _P, _P, _P, _I64, _I64, _P, _P, _P, _I64, _P, _P, _P, _I64],
+    'mnpb_bemret_solve_f64': [_P, _I64, _I64, _I64, _P, _P, _P, _P, _P, _I64, _I64, _P, _P, _P, _P, _I64, _P, _P, _P, _I64],
+    'mnpb_bemret_excitation': [_P, _I64, _I64, _I64, _P, _P, _P, _P, _I64, _P],
     'mnpb_getrf_f64': [_P, _I64, _I64, _P, _I64, _I64, _P, _I64, _P],
     'mnpb_getrs_f64': [_P, _I64, _I64, _I64, _P, _I64, _I64, _P, _I64, _P, _I64, _I64],
     'mnpb_zgemm': [_P, _I64, _I64, _I64, _I64, _D, _D, _P, _I64, _I64, _P, _I64, _I64, _D, _D,
@@ -63,6 +59,7 @@ SIGNATURES = {
     'mnpb_cgemm_tf32_noalloc': [_P, _I64, _I64, _I64, _I64, C.c_float, _P, _I64, _I64, _I64,
                                 _P, _I64, _I64, _I64, C.c_float, _P, _I64, _I64, _I64],
     'mnpb_tc_error': [_P, _P],
+    'mnpb_gemm_config': [C.c_int32, C.c_int32, C.c_int32],
     'mnpb_wait_probe': [_P, C.c_int32, _I64, _P],
     'mnpb_hmat_aca': [_P, _I64, _P, _I64, _P, _I64, _P, _P, _P, _I64, _I64, _D, _P, _P],
     'mnpb_hmat_gather_dense': [_P, _P, _I64, _P, _I64, _P, _P, _P],

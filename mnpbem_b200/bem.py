@@ -167,7 +167,7 @@ class BEMRet(object):
             bt.eps = torch.from_numpy(eps).to(t.device)
             bt.kvac = torch.from_numpy(kvac).to(t.device)
             call('mnpb_bemret_init_f64', sh, n, B, ptr(bt.G1), ptr(bt.G2), ptr(bt.H1),
-                 ptr(bt.H2), ptr(bt.D), n, n * n, ptr(bt.eps), ptr(bt.kvac), ptr(t.nvec),
+                 ptr(bt.H2), ptr(bt.D), n, n * n, ptr(bt.eps), ptr(bt.kvac), ptr(t.nvec), 0,
                  ptr(bt.piv), ptr(bt.info), ptr(bt.work), bt.work.numel())
             return bt
         bt = self._mixed_batch(eneis, stream) if reuse else _MixedBatch(t, eneis)
@@ -182,7 +182,7 @@ class BEMRet(object):
         bt.eps.copy_(torch.from_numpy(np.ascontiguousarray(eps)).view(B, 4))
         bt.kvac.copy_(torch.from_numpy(np.ascontiguousarray(kvac)).view(B))
         call('mnpb_bemret_init_mixed', sh, n, B, ptr(bt.G1p), ptr(bt.G2p), ptr(bt.H1p),
-             ptr(bt.H2p), ptr(bt.Dp), ld, ptr(bt.eps), ptr(bt.kvac), ptr(t.nvec), ptr(bt.piv),
+             ptr(bt.H2p), ptr(bt.Dp), ld, ptr(bt.eps), ptr(bt.kvac), ptr(t.nvec), 0, ptr(bt.piv),
              ptr(bt.info), ptr(bt.dinv), ptr(bt.work), bt.work.numel())
         return bt
 
@@ -259,13 +259,13 @@ class BEMRet(object):
         xin = torch.empty((B, 8, K, n), dtype=torch.complex128, device=t.device)
         xout = torch.empty_like(xin)
         call('mnpb_bemret_excitation', sh, n, B, K, ptr(pots_dev), ptr(bt.eps), ptr(bt.kvac),
-             ptr(t.nvec), ptr(xin))
+             ptr(t.nvec), 0, ptr(xin))
         if not bt.mixed:
             wb = B * n * 15 * K * 16
             work = torch.empty(wb, dtype=torch.uint8, device=t.device)
             call('mnpb_bemret_solve_f64', sh, n, B, K, ptr(bt.G1), ptr(bt.G2), ptr(bt.H1),
                  ptr(bt.H2), ptr(bt.D), n, n * n, ptr(bt.piv), ptr(bt.eps), ptr(bt.kvac),
-                 ptr(t.nvec), ptr(xin), ptr(xout), ptr(work), wb)
+                 ptr(t.nvec), 0, ptr(xin), ptr(xout), ptr(work), wb)
             return xout
         out = []
         for k0 in range(0, K, 4):          # the refinement solves up to 4 excitations at once
@@ -278,7 +278,7 @@ class BEMRet(object):
             relres = np.zeros(B)
             call('mnpb_bemret_solve_refine', sh, n, B, kk, ptr(bt.G1p), ptr(bt.G2p),
                  ptr(bt.H1p), ptr(bt.H2p), ptr(bt.Dp), bt.ld, ptr(bt.piv), ptr(bt.dinv), ptr(bt.G1),
-                 ptr(bt.G2), ptr(bt.H1), ptr(bt.H2), ptr(bt.eps), ptr(bt.kvac), ptr(t.nvec),
+                 ptr(bt.G2), ptr(bt.H1), ptr(bt.H2), ptr(bt.eps), ptr(bt.kvac), ptr(t.nvec), 0,
                  ptr(b_in), ptr(x), int(self.refine_maxit), float(self.refine_tol), ptr(iters),
                  ptr(relres), ptr(work), wb)
             bt.iters, bt.relres = iters, relres

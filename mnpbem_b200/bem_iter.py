@@ -237,7 +237,7 @@ class BEMRetIter(object):
                                device=self.device)
         pre.kvac = torch.tensor([self.k], dtype=torch.float64, device=self.device)
         call('mnpb_bemret_init_f64', sh, n, 1, ptr(pre.GG[0]), ptr(pre.GG[1]), ptr(pre.HH[0]),
-             ptr(pre.HH[1]), ptr(pre.D), n, n * n, ptr(pre.eps), ptr(pre.kvac), ptr(t.nvec),
+             ptr(pre.HH[1]), ptr(pre.D), n, n * n, ptr(pre.eps), ptr(pre.kvac), ptr(t.nvec), 0,
              ptr(pre.piv), ptr(pre.info), ptr(pre.work), pre.work.numel())
         if pre.info.any():
             raise _lib.MNPBError('BEMRetIter precond', 3, 'zero pivot')
@@ -253,7 +253,7 @@ class BEMRetIter(object):
         pre = self._pre
         call('mnpb_bemret_solve_f64', _lib.stream_handle(), n, 1, K, ptr(pre.GG[0]),
              ptr(pre.GG[1]), ptr(pre.HH[0]), ptr(pre.HH[1]), ptr(pre.D), n, n * n, ptr(pre.piv),
-             ptr(pre.eps), ptr(pre.kvac), ptr(t.nvec), ptr(xin), ptr(xout), ptr(work), wb)
+             ptr(pre.eps), ptr(pre.kvac), ptr(t.nvec), 0, ptr(xin), ptr(xout), ptr(work), wb)
         return xout.reshape(-1)
 
     # -------------------------------------------------------------- operator
@@ -292,7 +292,7 @@ class BEMRetIter(object):
         kvac = torch.tensor([self.k], dtype=torch.float64, device=self.device)
         b = torch.empty((1, 8, K, n), dtype=torch.complex128, device=self.device)
         call('mnpb_bemret_excitation', _lib.stream_handle(), n, 1, K, ptr(d_pots), ptr(eps),
-             ptr(kvac), ptr(t.nvec), ptr(b))
+             ptr(kvac), ptr(t.nvec), 0, ptr(b))
         return b.reshape(-1), K
 
     def solve(self, exc, x0=None):

@@ -30,8 +30,8 @@ extern "C" int64_t mnpb_bemret_workspace_f64(int64_t n, int64_t batch) {
 extern "C" int mnpb_bemret_init_f64(void *stream, int64_t n, int64_t batch, double *G1,
                                     double *G2, double *H1, double *H2, double *D, int64_t ld,
                                     int64_t stride, const double *eps, const double *kvac,
-                                    const double *nvec, int32_t *piv, int32_t *info, void *work,
-                                    int64_t work_bytes) {
+                                    const double *nvec, int64_t nvec_stride, int32_t *piv,
+                                    int32_t *info, void *work, int64_t work_bytes) {
     clear_error();
     MNPB_REQUIRE(n > 0 && batch > 0 && batch < 65536 && n < 65536 && ld >= n &&
                      stride >= ld * n,
@@ -71,7 +71,8 @@ extern "C" int mnpb_bemret_init_f64(void *stream, int64_t n, int64_t batch, doub
     MNPB_TRY(getrf(s, N, B, d, ld, stride, pivD, n, info));
     MNPB_TRY(set_identity(s, N, B, W, n, sw));
     MNPB_TRY(getrs(s, N, N, B, d, ld, stride, pivD, n, W, n, sw));
-    form_sigma_kernel<<<grid, 128, 0, s>>>(N, h2, W, n, sw, d, ld, stride, eps, kvac, nvec);
+    form_sigma_kernel<<<grid, 128, 0, s>>>(N, h2, W, n, sw, d, ld, stride, eps, kvac,
+                                           NvecView{nvec, nvec_stride});
     MNPB_LAUNCH_CHECK("form_sigma_kernel");
     MNPB_TRY(getrf(s, N, B, h2, ld, stride, pivS, ps, info));
     return MNPB_OK;
@@ -81,8 +82,9 @@ extern "C" int mnpb_bemret_solve_f64(void *stream, int64_t n, int64_t batch, int
                                      const double *G1, const double *G2, const double *S1,
                                      const double *S, const double *D, int64_t ld,
                                      int64_t stride, const int32_t *piv, const double *eps,
-                                     const double *kvac, const double *nvec, const double *x_in,
-                                     double *x_out, void *work, int64_t work_bytes) {
+                                     const double *kvac, const double *nvec, int64_t nvec_stride,
+                                     const double *x_in, double *x_out, void *work,
+                                     int64_t work_bytes) {
     clear_error();
     const int64_t K = nrhs;
     MNPB_REQUIRE(n > 0 && batch > 0 && K > 0 && K <= 64 && ld >= n, "bemret_solve: bad sizes");
@@ -103,19 +105,20 @@ extern "C" int mnpb_bemret_solve_f64(void *stream, int64_t n, int64_t batch, int
     cd *xout = (cd *)x_out;
     const int64_t ps = n;
     const int32_t *piv1 = piv, *piv2 = piv + batch * n, *pivS = piv + 2 * batch * n;
+    const NvecView nv{nvec, nvec_stride};
     dim3 g(ceil_div(n, 128), B);
     solve_prep_kernel<<<g, 128, 0, s>>>(N, k, xin, sx, T, sT, eps, kvac);
     MNPB_LAUNCH_CHECK("solve_prep_kernel");
     MNPB_TRY(zgemm(s, N, 4 * k, N, B, cmk(1, 0), (const cd *)S1, ld, stride, T, n, sT, cmk(0, 0),
                    U, n, sT));
-    solve_alpha_kernel<<<g, 128, 0, s>>>(N, k, xin, sx, U, sT, AP, sAP, R, sR, eps, kvac, nvec);
+    solve_alpha_kernel<<<g, 128, 0, s>>>(N, k, xin, sx, U, sT, AP, sAP, R, sR, eps, kvac, nv);
     MNPB_LAUNCH_CHECK("solve_alpha_kernel");
     MNPB_TRY(zgemm(s, N, 3 * k, N, B, cmk(1, 0), (const cd *)D, ld, stride, AP, n, sAP,
                    cmk(0, 0), V, n, sAP));
-    solve_rhs_kernel<<<g, 128, 0, s>>>(N, k, V, sAP, R, sR, eps, kvac, nvec);
+    solve_rhs_kernel<<<g, 128, 0, s>>>(N, k, V, sAP, R, sR, eps, kvac, nv);
     MNPB_LAUNCH_CHECK("solve_rhs_kernel");
     MNPB_TRY(getrs(s, N, k, B, (const cd *)S, ld, stride, pivS, ps, R, n, sR));
-    solve_h2pre_kernel<<<g, 128, 0, s>>>(N, k, AP, sAP, R, sR, eps, kvac, nvec);
+    solve_h2pre_kernel<<<g, 128, 0, s>>>(N, k, AP, sAP, R, sR, eps, kvac, nv);
     MNPB_LAUNCH_CHECK("solve_h2pre_kernel");
     MNPB_TRY(zgemm(s, N, 3 * k, N, B, cmk(1, 0), (const cd *)D, ld, stride, AP, n, sAP,
                    cmk(0, 0), V, n, sAP));
@@ -129,13 +132,14 @@ extern "C" int mnpb_bemret_solve_f64(void *stream, int64_t n, int64_t batch, int
 
 extern "C" int mnpb_bemret_excitation(void *stream, int64_t n, int64_t batch, int64_t nrhs,
                                       const double *pots, const double *eps, const double *kvac,
-                                      const double *nvec, double *x_in) {
+                                      const double *nvec, int64_t nvec_stride, double *x_in) {
     clear_error();
     MNPB_REQUIRE(n > 0 && batch > 0 && nrhs > 0 && batch < 65536, "bemret_excitation: bad sizes");
     MNPB_REQUIRE(pots && eps && kvac && nvec && x_in, "bemret_excitation: null pointer");
     dim3 g(ceil_div(n, 128), (unsigned)batch);
     excitation_kernel<<<g, 128, 0, as_stream(stream)>>>((int)n, (int)nrhs, (const cd *)pots,
-                                                        (cd *)x_in, eps, kvac, nvec);
+                                                        (cd *)x_in, eps, kvac,
+                                                        NvecView{nvec, nvec_stride});
     MNPB_LAUNCH_CHECK("excitation_kernel");
     return MNPB_OK;
 }

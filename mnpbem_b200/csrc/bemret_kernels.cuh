@@ -37,8 +37,9 @@ static __global__ void form_delta_kernel(int n, const cd *S1, cd *S2, cd *D, int
 // S <- S + k^2 (eps1-eps2)^2 (W o n n^T) ; D <- W
 static __global__ void form_sigma_kernel(int n, cd *S, const cd *W, int64_t ldw, int64_t sw, cd *D,
                                   int64_t ld, int64_t st, const double *eps, const double *kvac,
-                                  const double *nvec) {
+                                  NvecView nvv) {
     const int64_t b = blockIdx.z;
+    const double *nvec = nvv.at(b);
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y;
     if (i >= n) return;
@@ -70,8 +71,9 @@ static __global__ void solve_prep_kernel(int n, int K, const cd *xin, int64_t sx
 // U = Sigma1 T.  AP = alpha' (n x 3K), R = De' (n x K)
 static __global__ void solve_alpha_kernel(int n, int K, const cd *xin, int64_t sx, const cd *U,
                                    int64_t sU, cd *AP, int64_t sAP, cd *R, int64_t sR,
-                                   const double *eps, const double *kvac, const double *nvec) {
+                                   const double *eps, const double *kvac, NvecView nvv) {
     const int64_t b = blockIdx.y;
+    const double *nvec = nvv.at(b);
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const EpsK ek = load_epsk(eps, kvac, b);
@@ -99,8 +101,9 @@ static __global__ void solve_alpha_kernel(int n, int K, const cd *xin, int64_t s
 
 // R += ik n.((eps1-eps2) V)   with V = Delta^-1 alpha' (n x 3K)
 static __global__ void solve_rhs_kernel(int n, int K, const cd *V, int64_t sV, cd *R, int64_t sR,
-                                 const double *eps, const double *kvac, const double *nvec) {
+                                 const double *eps, const double *kvac, NvecView nvv) {
     const int64_t b = blockIdx.y;
+    const double *nvec = nvv.at(b);
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const EpsK ek = load_epsk(eps, kvac, b);
@@ -117,8 +120,9 @@ static __global__ void solve_rhs_kernel(int n, int K, const cd *V, int64_t sV, c
 
 // AP <- ik n (eps1-eps2) sig2 + AP     (sig2 in R)
 static __global__ void solve_h2pre_kernel(int n, int K, cd *AP, int64_t sAP, const cd *R, int64_t sR,
-                                   const double *eps, const double *kvac, const double *nvec) {
+                                   const double *eps, const double *kvac, NvecView nvv) {
     const int64_t b = blockIdx.y;
+    const double *nvec = nvv.at(b);
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const EpsK ek = load_epsk(eps, kvac, b);
@@ -164,8 +168,9 @@ static __global__ void solve_out_kernel(int n, int K, const cd *xin, int64_t sx,
 // pots columns (component-major, K each): phi1, phi1', a1 (3), a1' (3),
 // phi2, phi2', a2 (3), a2' (3).
 static __global__ void excitation_kernel(int n, int K, const cd *pots, cd *xin, const double *eps,
-                                  const double *kvac, const double *nvec) {
+                                  const double *kvac, NvecView nvv) {
     const int64_t b = blockIdx.y;
+    const double *nvec = nvv.at(b);
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const EpsK ek = load_epsk(eps, kvac, b);

@@ -48,8 +48,9 @@ __global__ void form_delta_p(int n, const float *S1, float *S2, float *D, int64_
 // S <- S + k^2 (eps1-eps2)^2 (W o n n^T) ; D <- W   (planar FP32)
 __global__ void form_sigma_p(int n, float *S, const float *W, float *D, int64_t ld, int64_t plane,
                              int64_t st, const double *eps, const double *kvac,
-                             const double *nvec) {
+                             NvecView nvv) {
     const int64_t b = blockIdx.z;
+    const double *nvec = nvv.at(b);
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y;
     if (i >= n) return;
@@ -144,8 +145,9 @@ __global__ void __launch_bounds__(256) zskinny_kernel(int n, int m, const cd *__
 // b and r use the excitation layout [phi | a (3) | De | alpha (3)].
 __global__ void residual_kernel(int n, int K, const cd *P1, const cd *P2, const cd *Q1,
                                 const cd *Q2, int64_t sP, const cd *bvec, cd *r, int64_t sx,
-                                const double *eps, const double *kvac, const double *nvec) {
+                                const double *eps, const double *kvac, NvecView nvv) {
     const int64_t b = blockIdx.y;
+    const double *nvec = nvv.at(b);
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const EpsK ek = load_epsk(eps, kvac, b);
@@ -294,7 +296,7 @@ static int mgetrs(f32::Ctx &c, int n, int m, const float *LU, const Factors &F,
 // Mixed BEMRet solve x_out = M^-1 x_in (same steps as mnpb_bemret_solve_f64).
 // Scratch: per batch entry 15 K n complex double + 2 x 8 K n planar float.
 static int msolve(f32::Ctx &c, int n, int K, const Factors &F, const double *eps,
-                  const double *kvac, const double *nvec, const cd *xin, cd *xout, cd *scr,
+                  const double *kvac, NvecView nvec, const cd *xin, cd *xout, cd *scr,
                   float *fscr) {
     cudaStream_t s = c.s;
     const int B = c.batch;
@@ -346,7 +348,7 @@ extern "C" int64_t mnpb_bemret_dinv_floats(int64_t n, int64_t batch) {
 
 static int init_mixed_body(cudaStream_t s, int64_t n, int64_t batch, float *G1, float *G2,
                            float *H1, float *H2, float *D, int64_t ld, const double *eps,
-                           const double *kvac, const double *nvec, int32_t *piv, int32_t *info,
+                           const double *kvac, NvecView nvec, int32_t *piv, int32_t *info,
                            float *dinv, void *work, int64_t work_bytes) {
     const int N = (int)n, B = (int)batch;
     const int64_t plane = ld * n, stride = 2 * plane;
@@ -402,13 +404,13 @@ static int init_mixed_body(cudaStream_t s, int64_t n, int64_t batch, float *G1, 
 namespace {
 struct InitKey {
     const void *p[12];
-    int64_t n, batch, ld, work_bytes;
+    int64_t n, batch, ld, work_bytes, nvec_stride, cfg_epoch;
     int dev;
     bool operator==(const InitKey &o) const {
         for (int i = 0; i < 12; ++i)
             if (p[i] != o.p[i]) return false;
         return n == o.n && batch == o.batch && ld == o.ld && work_bytes == o.work_bytes &&
-               dev == o.dev;
+               nvec_stride == o.nvec_stride && cfg_epoch == o.cfg_epoch && dev == o.dev;
     }
 };
 struct InitGraph {
@@ -436,8 +438,8 @@ uint64_t g_graph_clock = 0;
 extern "C" int mnpb_bemret_init_mixed(void *stream, int64_t n, int64_t batch, float *G1,
                                       float *G2, float *H1, float *H2, float *D, int64_t ld,
                                       const double *eps, const double *kvac, const double *nvec,
-                                      int32_t *piv, int32_t *info, float *dinv, void *work,
-                                      int64_t work_bytes) {
+                                      int64_t nvec_stride, int32_t *piv, int32_t *info,
+                                      float *dinv, void *work, int64_t work_bytes) {
     clear_error();
     MNPB_REQUIRE(n > 0 && batch > 0 && batch < 65536 && n < 65536 && ld >= n && ld % 4 == 0,
                  "bemret_init_mixed: bad sizes");
@@ -447,7 +449,8 @@ extern "C" int mnpb_bemret_init_mixed(void *stream, int64_t n, int64_t batch, fl
                  "bemret_init_mixed: workspace too small");
     cudaStream_t s = as_stream(stream);
     auto body = [&](cudaStream_t st) {
-        return init_mixed_body(st, n, batch, G1, G2, H1, H2, D, ld, eps, kvac, nvec, piv, info,
+        return init_mixed_body(st, n, batch, G1, G2, H1, H2, D, ld, eps, kvac,
+                               NvecView{nvec, nvec_stride}, piv, info,
                                dinv, work, work_bytes);
     };
     if (prof_on()) return body(s);
@@ -458,7 +461,7 @@ extern "C" int mnpb_bemret_init_mixed(void *stream, int64_t n, int64_t batch, fl
         return body(s);
     }
     InitKey key{{G1, G2, H1, H2, D, eps, kvac, nvec, piv, info, dinv, work},
-                n, batch, ld, work_bytes, 0};
+                n, batch, ld, work_bytes, nvec_stride, tc::gemm_config_epoch(), 0};
     if (cudaGetDevice(&key.dev) != cudaSuccess || key.dev < 0 || key.dev >= kMaxDev) {
         cudaGetLastError();
         return body(s);
@@ -536,7 +539,8 @@ extern "C" int mnpb_bemret_solve_refine(
     const float *S1p, const float *Sp, const float *Dp, int64_t ld, const int32_t *piv,
     const float *dinv, const double *G1, const double *G2, const double *H1, const double *H2,
     const double *eps,
-    const double *kvac, const double *nvec, const double *bvec, double *x, int max_iter,
+    const double *kvac, const double *nvec, int64_t nvec_stride, const double *bvec, double *x,
+    int max_iter,
     double tol, int32_t *iters, double *relres, void *work, int64_t work_bytes) {
     clear_error();
     const int64_t K = nrhs;
@@ -577,7 +581,8 @@ extern "C" int mnpb_bemret_solve_refine(
     const cd *bb = (const cd *)bvec;
     cd *xx = (cd *)x;
 
-    MNPB_TRY(msolve(c, N, k, F, eps, kvac, nvec, bb, xx, scr, fscr));
+    const NvecView nv{nvec, nvec_stride};
+    MNPB_TRY(msolve(c, N, k, F, eps, kvac, nv, bb, xx, scr, fscr));
     std::vector<double> hn(4 * batch);
     std::vector<int> done(batch, 0);
     for (int b = 0; b < B; ++b) {
@@ -613,7 +618,7 @@ extern "C" int mnpb_bemret_solve_refine(
         MNPB_LAUNCH_CHECK("zskinny_kernel");
         residual_kernel<<<gz, 128, 0, s>>>(N, k, P1, P2, Q1, Q2, sP4, bb + (int64_t)e0 * sx,
                                            r + (int64_t)e0 * sx, sx, eps + 4 * (int64_t)e0,
-                                           kvac + e0, nvec);
+                                           kvac + e0, nv.shifted(e0));
         MNPB_LAUNCH_CHECK("residual_kernel");
         return MNPB_OK;
     };
@@ -646,7 +651,7 @@ extern "C" int mnpb_bemret_solve_refine(
         const int Bp = B - b0;
         MNPB_TRY(residual(b0));
         f32::Ctx ca(s, Bp, (float *)wp, tcw);
-        MNPB_TRY(msolve(ca, N, k, F.at(b0), eps + 4 * (int64_t)b0, kvac + b0, nvec,
+        MNPB_TRY(msolve(ca, N, k, F.at(b0), eps + 4 * (int64_t)b0, kvac + b0, nv.shifted(b0),
                         r + (int64_t)b0 * sx, dx + (int64_t)b0 * sx, scr, fscr));
         axpy_kernel<<<ceil_div((int64_t)Bp * sx, 256), 256, 0, s>>>((int64_t)Bp * sx,
                                                                     dx + (int64_t)b0 * sx,

@@ -105,6 +105,17 @@ struct ProfScope {
 
 inline int ceil_div(int64_t a, int64_t b) { return (int)((a + b - 1) / b); }
 
+// Face normals of a batch of BEM systems: entry b's n x 3 table starts at
+// p + b * stride (stride 0: one table shared by every entry, a wavelength
+// sweep of one particle; stride n * 3: a batch of different particles with
+// the same face count).
+struct NvecView {
+    const double *p;
+    int64_t stride;
+    __host__ __device__ NvecView shifted(int64_t b0) const { return NvecView{p + b0 * stride, stride}; }
+    __host__ __device__ const double *at(int64_t b) const { return p + b * stride; }
+};
+
 // ---------------------------------------------------------------------------
 // complex double helpers (interleaved re, im)
 // ---------------------------------------------------------------------------

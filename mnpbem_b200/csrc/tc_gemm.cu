@@ -763,6 +763,16 @@ int encode_map_f32(void *map, const float *base, const uint64_t dims[3],
 
 static int num_sms() { return device_sms(); }
 
+// Launch configuration chosen by the autotuner (process-wide; the defaults
+// are the hand-picked ones): the tile width used for N > 64 (64 or 128), the
+// persistent kernel's threshold in tiles per SM (0: never persistent) and the
+// stage count of the operand ring (0: as many as fit).  Every change bumps
+// an epoch that cached launch sequences (CUDA graphs) are keyed on.
+static std::atomic<int> g_cfg_bn{128}, g_cfg_persist{2}, g_cfg_stages{0};
+static std::atomic<int64_t> g_cfg_epoch{0};
+
+int64_t gemm_config_epoch() { return g_cfg_epoch.load(); }
+
 int64_t cgemm_tf32_workspace(int M, int K, int batch) {
     const int64_t Mp = (M + BM - 1) / BM * BM, Kp = (K + BK - 1) / BK * BK;
     return (int64_t)batch * 2 * Mp * Kp * 4;
@@ -781,7 +791,9 @@ static int launch_tf32(cudaStream_t s, const CUtensorMap &mA, const CUtensorMap 
     // least large enough that no more CTAs share an SM than fit their
     // accumulators in its 512 TMEM columns
     const int KT = Kp / BK;
-    const int nst = KT < TL::MAX_ST ? KT : TL::MAX_ST;
+    const int cst = g_cfg_stages.load(std::memory_order_relaxed);
+    const int maxst = (cst >= 2 && cst < TL::MAX_ST) ? cst : TL::MAX_ST;
+    const int nst = KT < maxst ? KT : maxst;
     const int max_ctas_tmem = 512 / TL::TMEM_COLS;
     int dyn = TL::smem_bytes(nst);
     const int floor_bytes = (228 * 1024) / (max_ctas_tmem + 1) + 1024;
@@ -789,11 +801,12 @@ static int launch_tf32(cudaStream_t s, const CUtensorMap &mA, const CUtensorMap 
     const int MT = Mp / BM, NT = (N + BN - 1) / BN;
     const int64_t ntiles = (int64_t)MT * NT * batch;
     // (narrower tiles already overlap epilogues across several CTAs per SM)
-    if (BN == 128 && ntiles >= 2 * num_sms()) {
+    const int persist = g_cfg_persist.load(std::memory_order_relaxed);
+    if (BN == 128 && persist > 0 && ntiles >= (int64_t)persist * num_sms()) {
         // persistent: one CTA per SM, double-buffered accumulators
         MNPB_TRY(smem_opt_in(cgemm_tf32_persistent<BN, AMN>, TL::smem_bytes(TL::MAX_ST),
                              "cgemm_tf32_persistent"));
-        const int pst = TL::MAX_ST;
+        const int pst = maxst;
         const int grid = (int)(ntiles < num_sms() ? ntiles : num_sms());
         cgemm_tf32_persistent<BN, AMN><<<grid, 192, TL::smem_bytes(pst), s>>>(
             mA, mAi, mBr, mBi, ep, pst, MT, NT, (int)ntiles);
@@ -810,7 +823,8 @@ template <bool AMN>
 static int launch_any(cudaStream_t s, const CUtensorMap &mA, const CUtensorMap &mAi,
                       const CMatF &B, int M, int N, int K, int Kp, int Mp, int batch, Epi ep) {
     if (N <= 32) return launch_tf32<32, AMN>(s, mA, mAi, B, M, N, K, Kp, Mp, batch, ep);
-    if (N <= 64) return launch_tf32<64, AMN>(s, mA, mAi, B, M, N, K, Kp, Mp, batch, ep);
+    if (N <= 64 || g_cfg_bn.load(std::memory_order_relaxed) == 64)
+        return launch_tf32<64, AMN>(s, mA, mAi, B, M, N, K, Kp, Mp, batch, ep);
     return launch_tf32<128, AMN>(s, mA, mAi, B, M, N, K, Kp, Mp, batch, ep);
 }
 
@@ -919,6 +933,19 @@ extern "C" int mnpb_cgemm_tf32_ex(void *stream, int64_t m, int64_t n, int64_t k,
     return tc::cgemm_tf32(as_stream(stream), (int)m, (int)n, (int)k, (int)batch, alpha, a, b,
                           beta, c, (float *)work, work_bytes, (flags & MNPB_GEMM_ROUND_C) != 0,
                           a_tf32);
+}
+
+extern "C" int mnpb_gemm_config(int32_t bn_wide, int32_t persist_tiles_per_sm, int32_t stages) {
+    clear_error();
+    MNPB_REQUIRE(bn_wide == 64 || bn_wide == 128, "gemm_config: bn_wide must be 64 or 128");
+    MNPB_REQUIRE(persist_tiles_per_sm >= 0 && persist_tiles_per_sm <= 64,
+                 "gemm_config: persist_tiles_per_sm must be 0..64");
+    MNPB_REQUIRE(stages == 0 || (stages >= 2 && stages <= 4), "gemm_config: stages 0 or 2..4");
+    tc::g_cfg_bn.store(bn_wide);
+    tc::g_cfg_persist.store(persist_tiles_per_sm);
+    tc::g_cfg_stages.store(stages);
+    tc::g_cfg_epoch.fetch_add(1);
+    return MNPB_OK;
 }
 
 extern "C" int mnpb_tc_error(void *stream, int32_t *code) {

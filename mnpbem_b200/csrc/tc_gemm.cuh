@@ -27,6 +27,8 @@ int cgemm_tf32(cudaStream_t s, int M, int N, int K, int batch, float alpha, CMat
                float beta, CMatF C, float *work, int64_t work_bytes, bool round_out = false,
                bool a_tf32 = false);
 int tc_error_read_and_clear(cudaStream_t s, int *code);
+// Counter bumped by every mnpb_gemm_config call (launch configuration epoch).
+int64_t gemm_config_epoch();
 // Launches a one-thread kernel whose mbarrier wait (the tensor-core kernels'
 // bounded wait, limit `limit_ns`) can only time out; it records code 9.
 int wait_probe(cudaStream_t s, uint64_t limit_ns);

@@ -637,25 +637,96 @@ def load_mesh(name):
 
 
 def trisphere(n, diameter, interp='curv'):
-    """Curved sphere mesh of ``n`` vertices and the given diameter (nm).
+    """Curved sphere mesh of ``n`` vertices and the given diameter (nm), the
+    reference's ``trisphere(n, diameter)`` (mnpbem/geometry/mesh_generators.py:13).
 
-    Only the (n, diameter) pairs that are packaged are available; they are
-    the reference's ``trisphere(n, diameter)`` (mnpbem/geometry/mesh_generators.py:13).
+    Packaged (n, diameter) pairs are the reference's output itself; other
+    diameters scale the packaged unit-diameter mesh of the same ``n`` (equal to
+    the reference's to rounding).
     """
-    v, f = load_mesh('trisphere_{}_{:g}'.format(int(n), float(diameter)))
+    try:
+        v, f = load_mesh('trisphere_{}_{:g}'.format(int(n), float(diameter)))
+    except KeyError:
+        v, f = load_mesh('trisphere_{}_1'.format(int(n)))
+        v = v * float(diameter)
     if interp == 'curv':
         return Particle(v, f, interp='curv')
     return Particle(v, f, interp='curv')._as_flat()
 
 
 def trirod(diameter, height, n):
-    """Flat rod mesh (cylinder with hemispherical caps), quads + triangles.
-
-    Only the packaged parameter sets are available; they are the reference's
-    ``trirod(diameter, height, n)`` (mnpbem/geometry/mesh_generators.py:592).
-    """
-    v, f = load_mesh('trirod_{:g}_{:g}_{}_{}_{}'.format(float(diameter), float(height), *n))
+    """Flat rod mesh (cylinder with hemispherical caps), quads + triangles,
+    the reference's ``trirod(diameter, height, n)`` (mnpbem/geometry/
+    mesh_generators.py:592).  Packaged parameter sets are the reference's
+    output itself; others are built by ``rod_mesh``."""
+    try:
+        v, f = load_mesh('trirod_{:g}_{:g}_{}_{}_{}'.format(float(diameter), float(height), *n))
+    except KeyError:
+        v, f = rod_mesh(diameter, height, n)
     return Particle(v, f, interp='flat')
+
+
+def rod_mesh(diameter, height, n=(15, 20, 20)):
+    """Vertices and faces of a rod along z: a cylinder of the given diameter
+    with hemispherical caps, total length ``height`` (nm), centred at the
+    origin -- the surface of the reference's ``trirod`` (mnpbem/geometry/
+    mesh_generators.py:549-636): ``n = (nphi, ntheta, nz)`` grid points in
+    azimuth (0..2 pi, the last equal to the first), in polar angle per cap
+    (pole to equator) and along the cylinder.  Faces are quadrilaterals
+    ordered outward, with triangles around the two poles; face count
+    (nphi - 1) (2 (ntheta - 1) + nz - 1).
+
+    Returns (verts (nv, 3), faces (nf, 4) 0-based, NaN in column 3 of the
+    triangles).
+    """
+    nphi, ntheta, nz = (int(v) for v in n)
+    if nphi < 4 or ntheta < 2 or nz < 2:
+        raise ValueError("rod_mesh: n = (nphi >= 4, ntheta >= 2, nz >= 2)")
+    if not height > diameter > 0:
+        raise ValueError("rod_mesh: needs height > diameter > 0")
+    r, h = 0.5 * diameter, 0.5 * (height - diameter)
+    na = nphi - 1
+    phi = np.linspace(0.0, 2.0 * np.pi, nphi)[:na]
+    theta = np.linspace(0.0, 0.5 * np.pi, ntheta)
+    zc = h * np.linspace(1.0, -1.0, nz)
+    # rings from the top pole down: cap rings theta_1 .. theta_{ntheta-2}, the
+    # cylinder rings (top one = upper cap equator, bottom one = lower cap
+    # equator), then the lower cap rings mirrored
+    rings = []
+    for t in theta[1:-1]:
+        rings.append((r * np.sin(t), h + r * np.cos(t)))
+    for z in zc:
+        rings.append((r, z))
+    for t in theta[-2:0:-1]:
+        rings.append((r * np.sin(t), -h - r * np.cos(t)))
+    nr = len(rings)
+    verts = [np.array([[0.0, 0.0, h + r]])]
+    for rad, z in rings:
+        verts.append(np.column_stack([rad * np.cos(phi), rad * np.sin(phi), np.full(na, z)]))
+    verts.append(np.array([[0.0, 0.0, -h - r]]))
+    verts = np.vstack(verts)
+    top, bot = 0, 1 + nr * na
+    ring = lambda k, a: 1 + k * na + (a % na)
+    faces = []
+    for a in range(na):
+        faces.append([top, ring(0, a), ring(0, a + 1), np.nan])
+    for k in range(nr - 1):
+        for a in range(na):
+            faces.append([ring(k, a), ring(k + 1, a), ring(k + 1, a + 1), ring(k, a + 1)])
+    for a in range(na):
+        faces.append([ring(nr - 1, a), bot, ring(nr - 1, a + 1), np.nan])
+    faces = np.array(faces, dtype=float)
+    # vertex order as the reference meshes: (v1 - v0) x (v2 - v0) points
+    # into the body (Particle turns that into an outward normal)
+    for f in faces:
+        idx = f[~np.isnan(f)].astype(int)
+        p = verts[idx]
+        nrm = np.cross(p[1] - p[0], p[2] - p[0])
+        c = p.mean(axis=0)
+        out = np.array([c[0], c[1], 0.0 if abs(c[2]) <= h else c[2] - np.sign(c[2]) * h])
+        if np.dot(nrm, out) > 0:
+            f[:len(idx)] = idx[::-1]
+    return verts, faces
 
 
 def _as_flat(self):

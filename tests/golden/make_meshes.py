@@ -9,7 +9,8 @@ The meshes are the reference's own mesh-generator outputs (the BEM path takes
 a ready surface mesh as input; mesh generation is not part of it):
 
 * ``trisphere(n, d)`` -- mnpbem/geometry/mesh_generators.py:13, stored with its
-  curved midpoint vertices (``verts2``/``faces2``, 9 face columns).  The
+  curved midpoint vertices (``verts2``/``faces2``, 9 face columns); also
+  unit-diameter spheres of several n, which other diameters scale.  The
   underlying point sets are the reference's ``mnpbem/data/sphere*_tri.bin``.
 * ``trirod(d, h, n)`` -- mnpbem/geometry/mesh_generators.py:592 (flat quads +
   triangles).
@@ -29,6 +30,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 DATA = os.path.join(HERE, '..', '..', 'mnpbem_b200', 'data')
 
 SPHERES = [(32, 10.0), (60, 10.0), (144, 10.0), (144, 20.0), (256, 20.0), (1444, 40.0)]
+# unit-diameter spheres: trisphere(n, D) for other diameters scales these
+UNIT_SPHERES = (144, 256, 400, 576, 784, 1024, 1225)
 RODS = [(20.0, 80.0, (31, 21, 41)), (20.0, 80.0, (61, 31, 101)), (20.0, 80.0, (97, 47, 171))]
 
 
@@ -42,6 +45,11 @@ def main(ref_root):
     for n, d in SPHERES:
         p = trisphere(n, d)
         key = 'trisphere_{}_{:g}'.format(n, d)
+        out[key + '_verts'] = np.asarray(p.verts2, dtype=np.float64)
+        out[key + '_faces'] = np.asarray(p.faces2, dtype=np.float64)
+    for n in UNIT_SPHERES:
+        p = trisphere(n, 1.0)
+        key = 'trisphere_{}_1'.format(n)
         out[key + '_verts'] = np.asarray(p.verts2, dtype=np.float64)
         out[key + '_faces'] = np.asarray(p.faces2, dtype=np.float64)
     for d, h, n in RODS:
