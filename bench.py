@@ -68,6 +68,13 @@ def parse():
                     choices=['tc_gemm', 'tc_gemm_packed', 'assemble', 'solve', 'hmat', 'lu'],
                     help='run one representative kernel on a small case (profiling target) '
                          'and print its timing instead of the benchmark')
+    ap.add_argument('--no-batched', action='store_true',
+                    help='skip the 64-particle uneven batched section')
+    ap.add_argument('--batch-particles', type=int, default=64)
+    ap.add_argument('--batch-nlam', type=int, default=41)
+    ap.add_argument('--iter-accuracy-tols', default='1e-6,1e-8,1e-10',
+                    help='GMRES tolerances whose 25k-face extinction is compared with the '
+                         'dense FP64 GPU solve (empty: skip)')
     ap.add_argument('--fp64-steps', type=int, default=None,
                     help='timed sweeps of the plain FP64 GPU path (default: --steps)')
     return ap.parse_args()
@@ -253,7 +260,95 @@ def iterative_section(args):
                                    "achieved_GBs": nbytes / (hm_ms / cnt) / 1e6}
     out["compression"] = [round(c, 4) for c in bem.compression()]
     out["wavelengths"] = [float(e) for e in eneis]
-    del bem
+    tols = [float(t) for t in args.iter_accuracy_tols.split(',') if t.strip()]
+    if tols:
+        # extinction of the H-matrix / GMRES solve at several tolerances
+        # against the dense FP64 GPU solve of the same mesh and wavelength
+        lam = eneis[0]
+        acc = {"wavelength": lam, "runs": []}
+        ext_it = {}
+        for tol in tols:
+            bem.tol = tol
+            bem.enei = None
+            sig, _ = bem.solve(exc.potential(cp, lam))
+            ext_it[tol] = (float(exc.extinction(sig)), int(bem.matvec_counts()[-1]),
+                           int(bem.info()[0][-1]))
+        del bem, sig
+        torch.cuda.empty_cache()
+        from mnpbem_b200.bem import BEMRet
+        t0 = time.time()
+        dense = BEMRet(cp)
+        sd, _ = dense.solve(exc.potential(cp, lam))
+        ext_d = float(exc.extinction(sd))
+        torch.cuda.synchronize()
+        acc["dense_fp64_ext"] = ext_d
+        acc["dense_fp64_s"] = time.time() - t0
+        for tol in tols:
+            e, mv, flag = ext_it[tol]
+            acc["runs"].append({"gmres_tol": tol, "ext": e, "operator_applications": mv,
+                                "converged": flag == 0,
+                                "ext_rel_err_vs_dense": abs(e - ext_d) / abs(ext_d)})
+        ok = [r["gmres_tol"] for r in acc["runs"] if r["ext_rel_err_vs_dense"] <= 1e-6]
+        acc["largest_tol_within_1e-6"] = max(ok) if ok else None
+        out["accuracy_vs_dense"] = acc
+        del dense, sd
+    else:
+        del bem
+    torch.cuda.empty_cache()
+    return out
+
+
+BATCH_WORKLOAD = ("Batched uneven solves: 64 seed-random gold particles (seed 0; spheres "
+                  "D 10-60 nm, rods D 10-30 nm x L 30-120 nm, sphere dimers with 1-5 nm gaps; "
+                  "284-2446 faces), Drude Au in eps 1.77, 41 wavelengths linspace(400, 800) nm, "
+                  "x/y/z polarisations as 3 right-hand sides, mixed precision + FP64 "
+                  "refinement 1e-8, autotuned GEMM launches")
+
+
+def batched_section(args):
+    """lambda-solves/s of the 64-particle uneven set (one lambda-solve = one
+    particle at one wavelength with its 3 right-hand sides), after one
+    untimed sweep that also runs the launch autotuner."""
+    import torch
+    from mnpbem_b200.autotune import GemmTuner
+    from mnpbem_b200.batch import BatchedBEMRet
+    from mnpbem_b200.excitation import PlaneWaveRet
+    from mnpbem_b200.shapes import random_particles
+    ps = random_particles(args.batch_particles, seed=0)
+    eneis = list(np.linspace(400, 800, args.batch_nlam))
+    exc = PlaneWaveRet([[1.0, 0, 0], [0, 1.0, 0], [0, 0, 1.0]],
+                       [[0, 0, 1.0], [0, 0, 1.0], [1.0, 0, 0]])
+    t0 = time.time()
+    tuner = GemmTuner()
+    solver = BatchedBEMRet([cp for cp, _ in ps], refine_tol=1e-8, tuner=tuner)
+    torch.cuda.synchronize()
+    ctor = time.time() - t0
+    t0 = time.time()
+    solver.solve_spectrum(exc, eneis)                  # warm-up: tuning, graphs
+    torch.cuda.synchronize()
+    warm = time.time() - t0
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    res = solver.solve_spectrum(exc, eneis)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    faces = np.array([d['faces'] for _, d in ps])
+    flops = float(np.sum(104.0 / 3.0 * faces.astype(float) ** 3)) * len(eneis)
+    out = {"workload": BATCH_WORKLOAD, "particles": len(ps),
+           "faces_min_max": [int(faces.min()), int(faces.max())],
+           "face_count_groups": len(solver.groups), "wavelengths": len(eneis),
+           "lambda_solves_per_s": len(ps) * len(eneis) / (ms / 1000.0), "ms": ms,
+           "factorisation_TFLOPs": flops / (ms / 1000.0) / 1e12,
+           "constructor_s": ctor, "warmup_with_tuning_s": warm,
+           "refine_corrections_mean": float(res['iters'].mean()),
+           "refine_corrections_max": int(res['iters'].max()),
+           "launch_batches": [{"faces": st['n'], "entries": st['entries'],
+                               "batch": st['batch'], "gemm_config": st['config']}
+                              for st in solver.stats],
+           "tuner_ms": tuner.timings,
+           "timing": "CUDA events around one full sweep after the untimed tuning sweep"}
+    del solver
     torch.cuda.empty_cache()
     return out
 
@@ -649,6 +744,10 @@ def main():
             iterative["hmat_product"]["frac"] = (iterative["hmat_product"]["achieved_GBs"] /
                                                  peaks['hbm_gbs'])
 
+    batched = None
+    if rank == 0 and world == 1 and not args.no_batched:
+        batched = batched_section(args)
+
     if rank == 0:
         out = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
@@ -674,6 +773,7 @@ def main():
             "cpu_baseline": cpu,
             "clocks": ck,
             "iterative": iterative,
+            "batched": batched,
         }
         print(json.dumps(out))
     if world > 1:

@@ -53,13 +53,23 @@ def _norm(v, stream=None):
 
 
 def gmres(apply_A, b, tol=1e-6, maxit=200, restart=None, x0=None, apply_M=None,
-          stream=None, counter=None, r0=None):
+          stream=None, counter=None, r0=None, augment=None):
     """Restarted, right-preconditioned GMRES on complex128 device vectors.
 
     ``apply_A(v) -> A v`` and ``apply_M(v) -> M v`` take and return flat
     complex128 device tensors.  Stops when |b - A x| <= tol |b| (scipy
     semantics, bem_iter.py:79-89: restart = min(n, maxit), at most ``maxit``
     restart cycles).  ``r0``: b - A x0 when the caller already has it.
+
+    ``augment``: optional list of flat device vectors U whose span is searched
+    together with the Krylov space (GCRO augmentation, de Sturler 1999):
+    C = A U is orthonormalised (U R^-1 alongside), the residual is projected
+    off range(C) and Arnoldi runs on (I - C C^H) A M, so the solution
+    minimises |b - A x| over x0 + range(U) + M K_m.  C occupies the first
+    columns of the Arnoldi basis, so each CGS2 step projects against C and
+    the Krylov vectors together.  Costs one operator application per vector
+    of U; nearly dependent vectors are dropped.
+
     Returns (x, flag, relres, [cycles, iterations]).
     """
     dev = b.device
@@ -82,17 +92,57 @@ def gmres(apply_A, b, tol=1e-6, maxit=200, restart=None, x0=None, apply_M=None,
         r = b.clone()
     else:
         r = r0.clone() if r0 is not None else b - A(x)
-    V = torch.empty((restart + 1, L), dtype=torch.complex128, device=dev)
+    kmax = len(augment) if augment else 0
+    W = torch.empty((kmax + restart + 1, L), dtype=torch.complex128, device=dev)
+    hcol = torch.zeros(kmax + restart + 2, dtype=torch.complex128, device=dev)
+    nrm = torch.zeros(1, dtype=torch.float64, device=dev)
+    wb = int(_lib.lib().mnpb_gmres_workspace(L, kmax + restart))
+    work = torch.empty(wb, dtype=torch.uint8, device=dev)
+    # augmentation: C = A U orthonormalised in W[0:kc], Uc = U R^-1
+    Uc = []
+    kc = 0
+    for u in (augment or []):
+        u = u.reshape(-1)
+        c = A(u).reshape(-1).contiguous()
+        cn = float(_norm(c, stream).item())
+        if cn == 0.0:
+            continue
+        if kc == 0:
+            W[0].copy_(c / cn)
+            coef, diag = [], cn
+        else:
+            call('mnpb_gmres_arnoldi', sh, L, kc - 1, ptr(W), L, ptr(c), ptr(hcol), ptr(nrm),
+                 ptr(work), wb)
+            diag = float(nrm.item())
+            if diag <= 1e-10 * cn:
+                continue                               # (nearly) in the span already
+            coef = hcol[:kc].clone()
+        v = u.clone()
+        for i in range(len(coef)):
+            v -= coef[i] * Uc[i]
+        Uc.append(v / diag)
+        kc += 1
+    C = W[:kc]
+
+    def project(x, r):
+        """x += Uc z, r -= C z with z = C^H r (r off range(C))."""
+        if kc == 0:
+            return x, r
+        z = torch.mv(C.conj(), r)
+        for i in range(kc):
+            x = x + z[i] * Uc[i]
+        return x, r - torch.mv(C.transpose(0, 1), z)
+
+    V = W[kc:]
     H = torch.zeros((restart, restart + 1), dtype=torch.complex128, device=dev)
+    Bm = torch.zeros((restart, max(kc, 1)), dtype=torch.complex128, device=dev)
     cs = torch.zeros(restart, dtype=torch.float64, device=dev)
     sn = torch.zeros(restart, dtype=torch.complex128, device=dev)
     g = torch.zeros(restart + 1, dtype=torch.complex128, device=dev)
     y = torch.zeros(restart, dtype=torch.complex128, device=dev)
     res = torch.zeros(1, dtype=torch.float64, device=dev)
-    nrm = torch.zeros(1, dtype=torch.float64, device=dev)
-    wb = int(_lib.lib().mnpb_gmres_workspace(L, restart))
-    work = torch.empty(wb, dtype=torch.uint8, device=dev)
     flag, cycles, iters = 1, 0, 0
+    x, r = project(x, r)
     beta = float(_norm(r, stream).item())
     for cycle in range(maxit):
         if beta <= tol * bnorm:
@@ -106,8 +156,14 @@ def gmres(apply_A, b, tol=1e-6, maxit=200, restart=None, x0=None, apply_M=None,
         m = 0
         for j in range(restart):
             w = A(M(V[j])).reshape(-1).contiguous()
-            call('mnpb_gmres_arnoldi', sh, L, j, ptr(V), L, ptr(w), ptr(H[j]), ptr(nrm), ptr(work),
-                 wb)
+            if kc == 0:
+                call('mnpb_gmres_arnoldi', sh, L, j, ptr(V), L, ptr(w), ptr(H[j]), ptr(nrm),
+                     ptr(work), wb)
+            else:
+                call('mnpb_gmres_arnoldi', sh, L, kc + j, ptr(W), L, ptr(w), ptr(hcol),
+                     ptr(nrm), ptr(work), wb)
+                Bm[j, :kc].copy_(hcol[:kc])
+                H[j, :j + 2].copy_(hcol[kc:kc + j + 2])
             call('mnpb_gmres_givens', sh, j, ptr(H), restart + 1, ptr(cs), ptr(sn), ptr(g),
                  ptr(res))
             iters += 1
@@ -118,7 +174,12 @@ def gmres(apply_A, b, tol=1e-6, maxit=200, restart=None, x0=None, apply_M=None,
         call('mnpb_gmres_update', sh, L, m, ptr(H), restart + 1, ptr(g), ptr(V), L, ptr(y),
              ptr(z))
         x = x + M(z)
+        if kc:
+            t = torch.mv(Bm[:m, :kc].transpose(0, 1), y[:m])
+            for i in range(kc):
+                x = x - t[i] * Uc[i]
         r = b - A(x)
+        x, r = project(x, r)
         beta = float(_norm(r, stream).item())
     if beta <= tol * bnorm:
         flag = 0
@@ -331,12 +392,14 @@ class BEMRetIter(object):
         or a trained ``mnpbem_b200.learned.LearnedWarmStart`` (which corrects
         the quadratic extrapolation).  The first wavelengths fall back to the
         previous solution / linear extrapolation until the history is long
-        enough.  ``deflate``: start from
-        the minimal-residual point of span{start, x_{i-1}, x_{i-2}}.
-        Returns (list of CompStruct, list of per-wavelength statistics dicts,
-        list of packed device solutions).
+        enough.  ``deflate``: False, or the number m of previous solutions
+        (True: 6) that, with the start vector, span the GCRO augmentation
+        space of each solve (``gmres(augment=...)``): GMRES then minimises the
+        residual over that span and the Krylov space of the operator
+        deflated by it.  Returns (list of CompStruct, list of per-wavelength
+        statistics dicts, list of packed device solutions).
         """
-        from .learned import LearnedWarmStart, face_geometry, minres_start
+        from .learned import LearnedWarmStart, face_geometry
         n = self.tables.n
         learned = isinstance(warm, LearnedWarmStart)
         geo = face_geometry(self.p, self.device) if learned else None
@@ -359,14 +422,15 @@ class BEMRetIter(object):
                                       [xs[i - 1], xs[i - 2], xs[i - 3]], K, geo)
                 else:
                     raise ValueError("solve_spectrum: unknown warm start {!r}".format(warm))
-                if deflate and i >= 2:
-                    basis = [x0, xs[i - 1], xs[i - 2]] if warm != 'previous' else \
-                        [xs[i - 1], xs[i - 2]]
-                    x0, r0 = minres_start(A, b, basis, counter=cnt)
+            aug = None
+            if deflate and i >= 1:
+                m = 6 if deflate is True else int(deflate)
+                aug = ([x0] if x0 is not None else []) + xs[max(0, i - m):i]
+                x0 = None
             M = (lambda v: self._apply_precond(v, K)) if self._pre is not None else None
             x, flag, relres, it = gmres(A, b, tol=self.tol, maxit=self.maxit,
                                         restart=self.restart, x0=x0, apply_M=M, counter=cnt,
-                                        r0=r0)
+                                        r0=r0, augment=aug)
             self._flag.append(flag)
             self._relres.append(relres)
             self._iter.append(np.array(it))

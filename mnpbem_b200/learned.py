@@ -14,12 +14,13 @@ by its own rms).  Scaling the target by s2 makes the network learn the
 relative extrapolation error, so it helps equally where the spectrum is
 flat and where it bends.
 
-It supplies the GMRES start vector.  With ``deflate=True`` the start is the
-minimal-residual combination of span {prediction, x_{i-1}, x_{i-2}} (three
-extra operator applications): the solution's component in that subspace is
-removed before GMRES builds its Krylov space.  GMRES still converges to the
-same tolerance, so the network changes the cost of a solve, never its
-answer; the zero-start GMRES (or the dense LU) result judges its error.
+It supplies the GMRES start vector and, with ``deflate=m``, the first
+direction of a GCRO augmentation space {prediction, x_{i-1}, ..., x_{i-m}}
+(``bem_iter.gmres(augment=...)``, m + 1 extra operator applications): GMRES
+minimises the residual over that span and runs its Krylov space on the
+operator deflated by it.  GMRES still converges to the same tolerance, so
+the network changes the cost of a solve, never its answer; the zero-start
+GMRES (or the dense LU) result judges its error.
 
 Network: 4 dense layers (67 -> 256 -> 256 -> 256 -> 16), SiLU, bf16 weights
 with FP32 accumulation, trained with Adam on the GPU by the kernels of
@@ -275,32 +276,3 @@ class LearnedWarmStart(object):
         d = (Y * s2.repeat_interleave(n)[:, None]).double()              # (K*n, 16)
         d = torch.view_as_complex(d.reshape(K, n, 8, 2)).permute(2, 0, 1)   # (8, K, n)
         return (q + d).reshape(-1).contiguous()
-
-
-def minres_start(apply_A, b, W, counter=None):
-    """x0 = W c minimising |b - A W c| over the columns of W (list of flat
-    device vectors); returns (x0, r0 = b - A x0).  FP64 normal equations on
-    the k x k Gram matrix of A W (k <= 4, columns nearly independent)."""
-    AW = []
-    for w in W:
-        AW.append(apply_A(w))
-        if counter is not None:
-            counter.matvecs += 1
-    k = len(W)
-    G = torch.empty((k, k), dtype=torch.complex128, device=b.device)
-    r = torch.empty(k, dtype=torch.complex128, device=b.device)
-    for i in range(k):
-        r[i] = torch.vdot(AW[i], b)
-        for j in range(k):
-            G[i, j] = torch.vdot(AW[i], AW[j])
-    # scale to unit diagonal for conditioning, then solve on the host (k x k)
-    Gh, rh = G.cpu().numpy(), r.cpu().numpy()
-    dsc = 1.0 / np.sqrt(np.maximum(np.real(np.diag(Gh)), 1e-300))
-    c = np.linalg.lstsq(Gh * dsc[:, None] * dsc[None, :], rh * dsc, rcond=1e-12)[0] * dsc
-    x0 = torch.zeros_like(b)
-    r0 = b.clone()
-    for i in range(k):
-        ci = complex(c[i])
-        x0 += ci * W[i]
-        r0 -= ci * AW[i]
-    return x0, r0
