@@ -75,6 +75,9 @@ def parse():
     ap.add_argument('--iter-accuracy-tols', default='1e-6,1e-8,1e-10',
                     help='GMRES tolerances whose 25k-face extinction is compared with the '
                          'dense FP64 GPU solve (empty: skip)')
+    ap.add_argument('--mn-min-n', type=int, default=None,
+                    help='GEMM knob: TF32 A operands of products with 64 < N < this are '
+                         'packed instead of read in place (library default 256)')
     ap.add_argument('--fp64-steps', type=int, default=None,
                     help='timed sweeps of the plain FP64 GPU path (default: --steps)')
     return ap.parse_args()
@@ -520,6 +523,8 @@ def main():
                                 device_id=torch.device('cuda', local))
     import mnpbem_b200 as M
     from mnpbem_b200 import _lib, bem, excitation
+    if args.mn_min_n is not None:
+        _lib.call('mnpb_gemm_config_mn', int(args.mn_min_n))
 
     v, f = M.load_mesh('trisphere_1444_40')
     s = M.Particle(v, f, interp='curv')

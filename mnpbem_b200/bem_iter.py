@@ -114,7 +114,7 @@ def gmres(apply_A, b, tol=1e-6, maxit=200, restart=None, x0=None, apply_M=None,
             call('mnpb_gmres_arnoldi', sh, L, kc - 1, ptr(W), L, ptr(c), ptr(hcol), ptr(nrm),
                  ptr(work), wb)
             diag = float(nrm.item())
-            if diag <= 1e-10 * cn:
+            if diag <= 1e-6 * cn:
                 continue                               # (nearly) in the span already
             coef = hcol[:kc].clone()
         v = u.clone()
@@ -142,12 +142,15 @@ def gmres(apply_A, b, tol=1e-6, maxit=200, restart=None, x0=None, apply_M=None,
     y = torch.zeros(restart, dtype=torch.complex128, device=dev)
     res = torch.zeros(1, dtype=torch.float64, device=dev)
     flag, cycles, iters = 1, 0, 0
-    x, r = project(x, r)
     beta = float(_norm(r, stream).item())
     for cycle in range(maxit):
+        # convergence is judged on the true residual b - A x; the projection
+        # off range(C) only prepares the next cycle
         if beta <= tol * bnorm:
             flag = 0
             break
+        x, r = project(x, r)
+        beta = float(_norm(r, stream).item())
         cycles += 1
         V[0].copy_(r / beta)
         g.zero_()
@@ -179,7 +182,6 @@ def gmres(apply_A, b, tol=1e-6, maxit=200, restart=None, x0=None, apply_M=None,
             for i in range(kc):
                 x = x - t[i] * Uc[i]
         r = b - A(x)
-        x, r = project(x, r)
         beta = float(_norm(r, stream).item())
     if beta <= tol * bnorm:
         flag = 0

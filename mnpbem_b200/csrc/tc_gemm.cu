@@ -769,6 +769,11 @@ static int num_sms() { return device_sms(); }
 // stage count of the operand ring (0: as many as fit).  Every change bumps
 // an epoch that cached launch sequences (CUDA graphs) are keyed on.
 static std::atomic<int> g_cfg_bn{128}, g_cfg_persist{2}, g_cfg_stages{0};
+// TF32-exact A operands are read in place (MN-major) when N >= this, else
+// packed K-major first (exact for TF32 values).  Narrow products (N of one or
+// two 128-column tiles) stream their tall A only once per tile column, where
+// the MN-major boxes reach about half the HBM rate of the packed layout.
+static std::atomic<int> g_cfg_mn_min_n{256};
 static std::atomic<int64_t> g_cfg_epoch{0};
 
 int64_t gemm_config_epoch() { return g_cfg_epoch.load(); }
@@ -842,7 +847,11 @@ int cgemm_tf32(cudaStream_t s, int M, int N, int K, int batch, float alpha, CMat
     }
     const int Mp = (M + BM - 1) / BM * BM, Kp = (K + BK - 1) / BK * BK;
     Epi ep{C.p, C.ld, C.plane, C.stride, alpha, beta, M, N, Kp / BK, round_out ? 1 : 0};
-    if (a_tf32 && aligned16(A)) {
+    // narrow products of the 128-wide tile (96 < N < mn_min_n) pack A even when it
+    // could be read in place; the 32/64-wide tiles and wide products read it in place
+    const bool pack_narrow = N > 64 && N < g_cfg_mn_min_n.load(std::memory_order_relaxed) &&
+                             work && work_bytes >= cgemm_tf32_workspace(M, K, batch);
+    if (a_tf32 && aligned16(A) && !pack_narrow) {
         // A already holds TF32 values: the tensor cores read it in place (MN-major)
         CUtensorMap mAr, mAi;
         MNPB_TRY(make_map(&mAr, A.p, M, K, batch, A.ld, A.stride, 32,
@@ -933,6 +942,14 @@ extern "C" int mnpb_cgemm_tf32_ex(void *stream, int64_t m, int64_t n, int64_t k,
     return tc::cgemm_tf32(as_stream(stream), (int)m, (int)n, (int)k, (int)batch, alpha, a, b,
                           beta, c, (float *)work, work_bytes, (flags & MNPB_GEMM_ROUND_C) != 0,
                           a_tf32);
+}
+
+extern "C" int mnpb_gemm_config_mn(int32_t mn_min_n) {
+    clear_error();
+    MNPB_REQUIRE(mn_min_n >= 0, "gemm_config_mn: mn_min_n must be >= 0");
+    tc::g_cfg_mn_min_n.store(mn_min_n);
+    tc::g_cfg_epoch.fetch_add(1);
+    return MNPB_OK;
 }
 
 extern "C" int mnpb_gemm_config(int32_t bn_wide, int32_t persist_tiles_per_sm, int32_t stages) {

@@ -89,13 +89,15 @@ def test_aca_ranks_and_factors(rod_setup):
     print('same input as the reference: %d of %d blocks differ: %s'
           % (len(diff), len(g['aca_rank']), diff))
     assert all(d[3] is not None for d in diff), diff
-    assert len(diff) <= 0.05 * len(g['aca_rank'])
+    # measured on B200: every rank equal on both inputs
+    assert np.array_equal(hm_ref.rank_h, g['aca_rank'])
     # 2. the GPU-assembled G (what BEMRetIter uses) against the oracle on it
     gpu_rank = hms[0].rank_h
     orc = HMatrixOracle(dense[0], tree, part, htol=1e-6, kmax=100)
     diff = _explain(gpu_rank, orc)
     print('GPU-assembled input: %d blocks differ: %s' % (len(diff), diff))
     assert all(d[3] is not None for d in diff), diff
+    assert np.array_equal(gpu_rank, g['aca_rank'])
     # 3. factors of the first 12 blocks against the reference's, where ranks agree
     ou = ov = 0
     for i in range(12):
@@ -224,11 +226,14 @@ def test_bemretiter_hmatrix_rod9600(gpu_ok):
     GMRES tol 1e-6) and its dense BEMRet (golden_rod9600.npz).
 
     * The two GMRES runs walk the same Krylov process: operator applications
-      within 10 % of the reference's, and sigma / h / extinction close to the
-      reference's iterative solution.
-    * GMRES tol 1e-6 is not an extinction tolerance on this operator: the
-      reference's own iterative extinction sits 21 % from its dense one.  With
-      tol 1e-10 the GPU solve reaches the dense extinction to the ACA accuracy."""
+      within 3 % of the reference's, extinction within 1e-6 and sigma within
+      1e-4 of the reference's iterative solution (measured 1.1e-7 / 4e-6).
+    * The GPU dense FP64 solve gives the reference's dense extinction to 1e-9.
+    * The H-matrix solve (both implementations) sits 21 % from the dense one
+      on this rod at htol 1e-6 -- a property of the ACA approximation, not of
+      the GMRES tolerance (tol 1e-10 leaves it unchanged): the GPU path must
+      reproduce the reference's deviation to 1e-5 of the dense value."""
+    from mnpbem_b200 import BEMRet
     from mnpbem_b200.bem_iter import BEMRetIter
     from mnpbem_b200.excitation import PlaneWaveRet
     from mnpbem_b200.geometry import ComParticle, trirod
@@ -247,17 +252,16 @@ def test_bemretiter_hmatrix_rod9600(gpu_ok):
     ext = exc.extinction(sig)
     ref_it, ref_d = float(g['iter_ext']), float(g['dense_ext'])
     errs = {name: _rel(getattr(sig, name), g['iter_' + name]) for name in ('sig1', 'sig2')}
+    del bem, sig
+    torch.cuda.empty_cache()
+    dense, _ = BEMRet(cp).solve(exc.potential(cp, enei))
+    ext_d = exc.extinction(dense)
     print('rod 9600, tol 1e-6: matvecs %d (reference %d), ext %.10g (reference iterative '
-          '%.10g, dense %.10g), sigma vs reference iterative %s'
-          % (nmv, int(g['iter_matvecs']), ext, ref_it, ref_d, errs))
+          '%.10g), sigma vs reference iterative %s; dense ext %.10g (reference dense %.10g)'
+          % (nmv, int(g['iter_matvecs']), ext, ref_it, errs, ext_d, ref_d))
     assert flag[-1] == 0 and relres[-1] <= 1e-6
-    assert abs(nmv - int(g['iter_matvecs'])) <= 0.1 * int(g['iter_matvecs'])
-    assert abs(ext - ref_it) / abs(ref_it) < 2e-2
-    assert max(errs.values()) < 5e-2
-    bem.tol = 1e-10
-    sig, _ = bem.solve(exc.potential(cp, enei))
-    ext10 = exc.extinction(sig)
-    print('rod 9600, tol 1e-10: matvecs %d, ext %.10g (reference dense %.10g, rel %.2e)'
-          % (bem.matvec_counts()[-1], ext10, ref_d, abs(ext10 - ref_d) / abs(ref_d)))
-    assert bem.info()[0][-1] == 0
-    assert abs(ext10 - ref_d) / abs(ref_d) < 1e-2
+    assert abs(nmv - int(g['iter_matvecs'])) <= 0.03 * int(g['iter_matvecs'])
+    assert abs(ext - ref_it) / abs(ref_it) < 1e-6
+    assert max(errs.values()) < 1e-4
+    assert abs(ext_d - ref_d) / abs(ref_d) < 1e-9
+    assert abs((ext - ext_d) - (ref_it - ref_d)) < 1e-5 * abs(ref_d)
