@@ -143,14 +143,23 @@ def gmres(apply_A, b, tol=1e-6, maxit=200, restart=None, x0=None, apply_M=None,
     res = torch.zeros(1, dtype=torch.float64, device=dev)
     flag, cycles, iters = 1, 0, 0
     beta = float(_norm(r, stream).item())
+    checked = False
     for cycle in range(maxit):
         # convergence is judged on the true residual b - A x; the projection
         # off range(C) only prepares the next cycle
         if beta <= tol * bnorm:
             flag = 0
             break
-        x, r = project(x, r)
-        beta = float(_norm(r, stream).item())
+        if kc:
+            x, r = project(x, r)
+            beta = float(_norm(r, stream).item())
+            if beta <= tol * bnorm and not checked:
+                # the augmentation space alone solves the system: confirm it on
+                # the true residual (once) instead of iterating on rounding noise
+                checked = True
+                r = b - A(x)
+                beta = float(_norm(r, stream).item())
+                continue
         cycles += 1
         V[0].copy_(r / beta)
         g.zero_()

@@ -172,10 +172,51 @@ def _rms(x):
     return torch.sqrt(torch.mean(torch.abs(x) ** 2, dim=(0, 2))).clamp_min(1e-300)
 
 
-class LearnedWarmStart(object):
-    """Trainable corrector of the quadratic extrapolation of the solution."""
+def surface_modes(p, count, device='cuda'):
+    """The ``count`` smoothest surface functions of a particle: eigenvectors
+    of the smallest eigenvalues of a graph Laplacian over the face centroids
+    (Gaussian weights exp(-d^2 / 2 h^2), h the median distance of a face to
+    its six nearest neighbours; all pairs up to 4000 faces, the 32 nearest
+    neighbours of each face above).  Returns an orthonormal (n, count) FP32
+    device tensor."""
+    from scipy.spatial import cKDTree
+    pos = np.asarray(p.pos, dtype=np.float64)
+    n = pos.shape[0]
+    count = min(count, n - 1)
+    d6, _ = cKDTree(pos).query(pos, k=min(7, n))
+    h = float(np.median(d6[:, 1:]))
+    if n <= 4000:
+        d2 = ((pos[:, None, :] - pos[None, :, :]) ** 2).sum(axis=2)
+        W = np.exp(-d2 / (2.0 * h * h))
+        np.fill_diagonal(W, 0.0)
+        ev, E = np.linalg.eigh(np.diag(W.sum(axis=1)) - W)
+        E = E[:, :count]
+    else:
+        import scipy.sparse as sp
+        from scipy.sparse.linalg import eigsh
+        kk = min(33, n)
+        dk, jk = cKDTree(pos).query(pos, k=kk)
+        w = np.exp(-dk[:, 1:] ** 2 / (2.0 * h * h))
+        W = sp.coo_matrix((w.ravel(), (np.repeat(np.arange(n), kk - 1), jk[:, 1:].ravel())),
+                          shape=(n, n)).tocsr()
+        W = 0.5 * (W + W.T)
+        L = sp.diags(np.asarray(W.sum(axis=1)).ravel()) - W
+        ev, E = eigsh(L, k=count, sigma=-1e-6, which='LM')
+        E = E[:, np.argsort(ev)]
+    return torch.from_numpy(np.ascontiguousarray(E, dtype=np.float32)).to(device)
 
-    def __init__(self, width=256, depth=4, device='cuda', seed=0):
+
+class LearnedWarmStart(object):
+    """Trainable corrector of the quadratic extrapolation of the solution.
+
+    ``smooth_modes``: the network's correction is restricted to the span of
+    that many smoothest surface functions of the particle (``surface_modes``;
+    0 keeps it per face).  GMRES resolves the smooth part of a start-vector
+    error quickly and the per-face part slowly; the network's per-face
+    scatter would otherwise cost more iterations than its gain in accuracy
+    saves."""
+
+    def __init__(self, width=256, depth=4, device='cuda', seed=0, smooth_modes=30):
         sizes = [NFEAT] + [width] * (depth - 1) + [NOUT]
         self.mlp = MLP(sizes, device=device, seed=seed)
         self.device = self.mlp.device
@@ -183,6 +224,30 @@ class LearnedWarmStart(object):
         self.sd = torch.ones(NFEAT, device=self.device)
         self._X, self._T = [], []
         self.trained = False
+        self.smooth_modes = int(smooth_modes)
+        self._modes = {}
+
+    def _smooth(self, p, Y, K, n):
+        """Project every column of each polarisation's (n, 16) block of the
+        network output onto the smooth surface modes: E (E^T Y), two FP32
+        products by the network's own GEMM kernel."""
+        key = id(p)
+        if key not in self._modes:
+            self._modes[key] = (p, surface_modes(p, self.smooth_modes, self.device))
+        E = self._modes[key][1]
+        m = E.shape[1]
+        sh = _lib.stream_handle()
+        out = torch.empty_like(Y)
+        coef = torch.empty((m, 16), dtype=torch.float32, device=self.device)
+        nsplit = max(1, min(64, n // 512))
+        work = torch.empty(nsplit * m * 16, dtype=torch.float32, device=self.device)
+        for k in range(K):
+            Yk, Ok = Y[k * n:(k + 1) * n], out[k * n:(k + 1) * n]
+            call('mnpb_mlp_gemm', sh, m, 16, n, ptr(E), 1, m, ptr(Yk), 16, 1, 0, ptr(coef), 16,
+                 1, None, 0, None, nsplit, ptr(work) if nsplit > 1 else None)
+            call('mnpb_mlp_gemm', sh, n, 16, m, ptr(E), m, 1, ptr(coef), 16, 1, 0, ptr(Ok), 16,
+                 1, None, 0, None, 1, None)
+        return out
 
     # ---------------------------------------------------------------- data
     @staticmethod
@@ -273,6 +338,8 @@ class LearnedWarmStart(object):
         n = geo.shape[0]
         F, q, s2 = self.features(p, geo, eneis3, hist, K)
         Y = self.mlp.forward(((F - self.mu) / self.sd).contiguous())
+        if self.smooth_modes > 0:
+            Y = self._smooth(p, Y, K, n)
         d = (Y * s2.repeat_interleave(n)[:, None]).double()              # (K*n, 16)
         d = torch.view_as_complex(d.reshape(K, n, 8, 2)).permute(2, 0, 1)   # (8, K, n)
         return (q + d).reshape(-1).contiguous()
