@@ -262,6 +262,15 @@ int64_t mnpb_f32_workspace(int64_t n, int64_t batch);
 int mnpb_getrf_c32p(void *stream, int64_t n, int64_t batch, float *A, int64_t ld, int64_t plane,
                     int64_t stride, int32_t *piv, int64_t pstride, int32_t *info, void *work,
                     int64_t work_bytes);
+/* X = A^-1 from mnpb_getrf_c32p's output (U^-1 L^-1 P^T): the forward solve
+ * against the identity skips the identity's zero upper part and takes the
+ * leaves from the diagonal-block inverses.  Replaces the Delta^-1 of
+ * mnpbem/bem/bem_ret.py:476-479 (lu_solve on the identity).  Same layout
+ * rules and workspace as mnpb_getrs_c32p. */
+int mnpb_getri_c32p(void *stream, int64_t n, int64_t batch, const float *LU, int64_t ld,
+                    int64_t plane, int64_t stride, const int32_t *piv, int64_t pstride, float *X,
+                    int64_t ldx, int64_t planeX, int64_t xstride, void *work,
+                    int64_t work_bytes);
 int mnpb_getrs_c32p(void *stream, int64_t n, int64_t batch, int64_t nrhs, const float *LU,
                     int64_t ld, int64_t plane, int64_t stride, const int32_t *piv,
                     int64_t pstride, float *B, int64_t ldb, int64_t planeB, int64_t bstride,

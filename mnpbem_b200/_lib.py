@@ -40,6 +40,8 @@ SIGNATURES = {
     'mnpb_bemret_solve_refine': [_P, _I64, _I64, _I64, _P, _P, _P, _P, _P, _I64, _P, _P, _P, _P, _P, _P, _P, _P, _P, _I64, _P, _P, _I, _D, _P, _P, _P, _I64],
     'mnpb_f32_workspace': [_I64, _I64],
     'mnpb_getrf_c32p': [_P, _I64, _I64, _P, _I64, _I64, _I64, _P, _I64, _P, _P, _I64],
+    'mnpb_getri_c32p': [_P, _I64, _I64, _P, _I64, _I64, _I64, _P, _I64, _P, _I64, _I64, _I64,
+                        _P, _I64],
     'mnpb_getrs_c32p': [_P, _I64, _I64, _I64, _P, _I64, _I64, _I64, _P, _I64, _P, _I64, _I64,
                         _I64, _P, _I64],
     'mnpb_bemret_workspace_f64': [_I64, _I64],

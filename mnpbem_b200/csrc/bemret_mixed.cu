@@ -380,8 +380,7 @@ static int init_mixed_body(cudaStream_t s, int64_t n, int64_t batch, float *G1, 
     form_delta_p<<<grid, 128, 0, s>>>(N, H1, H2, D, ld, plane, stride, eps, kvac);
     MNPB_LAUNCH_CHECK("form_delta_p");
     MNPB_TRY(f32::getrf(c, N, d, pivD, n, info));
-    MNPB_TRY(f32::set_identity(c, N, w));
-    MNPB_TRY(f32::getrs(c, N, N, d, pivD, n, w));
+    MNPB_TRY(f32::lu_inverse(c, N, d, pivD, n, w));
     form_sigma_p<<<grid, 128, 0, s>>>(N, H2, W, D, ld, plane, stride, eps, kvac, nvec);
     MNPB_LAUNCH_CHECK("form_sigma_p");
     MNPB_TRY(f32::getrf(c, N, h2, pivS, ps, info));

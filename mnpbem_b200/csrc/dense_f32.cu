@@ -1472,6 +1472,75 @@ static int trsm(Ctx &c, int mode, int n, int m, CMatF T, CMatF B) {
     return trsm_rec(c2, mode, n, m, T, B, &iv, 0);
 }
 
+// ---- inverse of an LU factorisation: A^-1 = U^-1 L^-1 P^T ---------------------
+// Copy of each matrix's n x n diagonal-block inverse (planar, ld TL) into X.
+__global__ void copy_inv_block_kernel(int n, const float *__restrict__ inv, int64_t sinv,
+                                      float *X, int64_t ldx, int64_t plane, int64_t sX) {
+    const int64_t b = blockIdx.z;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y;
+    if (i >= n) return;
+    const float *src = inv + b * sinv + (int64_t)j * TL + i;
+    float *dst = X + b * sX + (int64_t)j * ldx + i;
+    dst[0] = src[0];
+    dst[plane] = src[(int64_t)TL * TL];
+}
+
+// X <- L^-1 for the unit lower factor in T, with X holding the identity on
+// entry: the rows of an identity column above its diagonal stay zero, so
+// X11 = L11^-1 (recursively), X21 = -L22^-1 (L21 X11) (one product and one
+// general solve with n1 right-hand sides), X22 = L22^-1 (recursively), and a
+// leaf is the stored inverse of its diagonal block -- a quarter fewer flops
+// than solving against the full identity.
+static int trsm_llu_eye_rec(Ctx &c, int n, CMatF T, CMatF X, const InvSet &iv, int blk0) {
+    if (n <= TL) {
+        const CMatF I = inv_block(iv, blk0);
+        dim3 grid(ceil_div(n, 128), n, c.batch);
+        copy_inv_block_kernel<<<grid, 128, 0, c.s>>>(n, I.p, I.stride, X.p, X.ld, X.plane,
+                                                     X.stride);
+        MNPB_LAUNCH_CHECK("copy_inv_block_kernel");
+        return MNPB_OK;
+    }
+    const int n1 = split_tl(n);
+    const int blk1 = blk0 + n1 / TL;
+    MNPB_TRY(trsm_llu_eye_rec(c, n1, T, X, iv, blk0));
+    MNPB_TRY(gemm(c, n - n1, n1, n1, -1.f, T.sub(n1, 0), X, 0.f, X.sub(n1, 0), false, true));
+    MNPB_TRY(trsm_rec(c, 0, n - n1, n1, T.sub(n1, n1), X.sub(n1, 0), &iv, blk1));
+    return trsm_llu_eye_rec(c, n - n1, T.sub(n1, n1), X.sub(n1, n1), iv, blk1);
+}
+
+int lu_inverse(Ctx &c, int n, CMatF LU, const int32_t *ipiv, int64_t sP, CMatF X) {
+    MNPB_TRY(set_identity(c, n, X));
+    const int nb = ceil_div(n, TL);
+    const int64_t inv_bytes = ((int64_t)c.batch * nb * 2 * TL * TL * 4 + 255) / 256 * 256;
+    const int64_t keep = (c.work_bytes - inv_bytes) / 256 * 256;
+    if (n <= TL || keep < trsm_pack_bytes(0, n, n, c.batch)) {
+        // no room for the block inverses: the plain getrs on the permuted identity
+        MNPB_TRY(laswp(c, X, 0, n, ipiv, sP, 0, n, true));
+        MNPB_TRY(trsm_llu(c, n, n, LU, X));
+        return trsm_lun(c, n, n, LU, X);
+    }
+    MNPB_TRY(smem_opt_in(tri_inv_kernel, TL * TL * (int)sizeof(cf), "tri_inv_kernel"));
+    float *inv = (float *)((char *)c.work + keep);
+    {
+        dim3 grid(nb, c.batch);
+        ProfScope ps(c.s, PC_TRSM, 8.0 * TL * TL * TL / 3.0 * nb * c.batch);
+        prof_tag("tri_inv n=%d B=%d L", n, c.batch);
+        tri_inv_kernel<<<grid, TINV_THREADS, TL * TL * sizeof(cf), c.s>>>(
+            n, 1, LU.p, LU.ld, LU.plane, LU.stride, inv, nb);
+        MNPB_LAUNCH_CHECK("tri_inv_kernel");
+    }
+    Ctx c2(c.s, c.batch, c.work, keep);
+    MNPB_TRY(trsm_llu_eye_rec(c2, n, LU, X, InvSet{inv, nb}, 0));
+    MNPB_TRY(trsm_lun(c, n, n, LU, X));
+    // X <- X P^T: the row interchanges of the factorisation, as column
+    // interchanges in reverse order
+    dim3 grid(ceil_div(n, 128), c.batch);
+    ProfScope ps(c.s, PC_SWAP, 0.0);
+    colswp_kernel<<<grid, 128, 0, c.s>>>(X.p, X.ld, X.plane, X.stride, n, ipiv, sP, n);
+    MNPB_LAUNCH_CHECK("colswp_kernel(f32)");
+    return MNPB_OK;
+}
+
 int trsm_llu(Ctx &c, int n, int m, CMatF L, CMatF B) { return trsm(c, 0, n, m, L, B); }
 int trsm_lun(Ctx &c, int n, int m, CMatF U, CMatF B) { return trsm(c, 1, n, m, U, B); }
 int trsm_run(Ctx &c, int n, int m, CMatF U, CMatF B) { return trsm(c, 2, n, m, U, B); }
@@ -1737,6 +1806,24 @@ extern "C" int mnpb_getrf_c32p(void *stream, int64_t n, int64_t batch, float *A,
                  "aligned");
     f32::Ctx c(as_stream(stream), (int)batch, (float *)work, work_bytes);
     return f32::getrf(c, (int)n, tc::CMatF{A, ld, plane, stride}, piv, pstride, info);
+}
+
+extern "C" int mnpb_getri_c32p(void *stream, int64_t n, int64_t batch, const float *LU,
+                               int64_t ld, int64_t plane, int64_t stride, const int32_t *piv,
+                               int64_t pstride, float *X, int64_t ldx, int64_t planeX,
+                               int64_t xstride, void *work, int64_t work_bytes) {
+    clear_error();
+    MNPB_REQUIRE(n > 0 && batch > 0 && ld >= n && ldx >= n, "getri_c32p: bad sizes");
+    MNPB_REQUIRE(ld % 4 == 0 && plane % 4 == 0 && stride % 4 == 0 && ldx % 4 == 0 &&
+                     planeX % 4 == 0 && xstride % 4 == 0 && ((uintptr_t)LU & 15) == 0 &&
+                     ((uintptr_t)X & 15) == 0,
+                 "getri_c32p: leading dimensions, planes and strides must be multiples of 4 "
+                 "floats and base pointers 16-byte aligned");
+    MNPB_REQUIRE(LU && piv && X && work, "getri_c32p: null pointer");
+    MNPB_REQUIRE(work_bytes >= mnpb_f32_workspace(n, batch), "getri_c32p: workspace too small");
+    f32::Ctx c(as_stream(stream), (int)batch, (float *)work, work_bytes);
+    return f32::lu_inverse(c, (int)n, tc::CMatF{(float *)LU, ld, plane, stride}, piv, pstride,
+                           tc::CMatF{X, ldx, planeX, xstride});
 }
 
 extern "C" int mnpb_getrs_c32p(void *stream, int64_t n, int64_t batch, int64_t nrhs,

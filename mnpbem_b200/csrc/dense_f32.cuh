@@ -28,6 +28,9 @@ int getrf(Ctx &c, int n, tc::CMatF A, int32_t *ipiv, int64_t sP, int32_t *info);
 int getrs(Ctx &c, int n, int nrhs, tc::CMatF LU, const int32_t *ipiv, int64_t sP, tc::CMatF B);
 int right_solve(Ctx &c, int n, int m, tc::CMatF LU, const int32_t *ipiv, int64_t sP, tc::CMatF B);
 int set_identity(Ctx &c, int n, tc::CMatF W);
+// X <- A^-1 from the LU factorisation of A (getrf output and pivots), the
+// forward solve exploiting the identity's zero upper part.
+int lu_inverse(Ctx &c, int n, tc::CMatF LU, const int32_t *ipiv, int64_t sP, tc::CMatF X);
 
 // Inverses of the 32 x 32 diagonal blocks of an LU factor (for getrs_few).
 int64_t diag_inv_floats(int n, int batch);

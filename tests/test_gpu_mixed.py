@@ -120,3 +120,37 @@ def test_mixed_c1_sigma_five_wavelengths(gpu_ok):
     sca = np.array([exc.scattering(sg)[0] for sg in sols]).ravel()
     assert np.max(np.abs(ext - z['ext']) / np.abs(z['ext'])) < 1e-6
     assert np.max(np.abs(sca - z['sca']) / np.abs(z['sca'])) < 1e-6
+
+
+@pytest.mark.parametrize('n,batch', [(100, 2), (300, 3), (700, 2), (1000, 4)])
+def test_getri_c32p(gpu_ok, n, batch):
+    """Inverse from the TF32 LU (structured forward solve on the identity,
+    diagonal-block inverses as leaves, column interchanges): A X = I to the
+    TF32 bound of a cond ~ 3 matrix (relative Frobenius error < 1e-2)."""
+    ld = (n + 3) // 4 * 4
+    g = torch.Generator().manual_seed(n)
+    Ac = (torch.randn((batch, n, n), generator=g, dtype=torch.float64) +
+          1j * torch.randn((batch, n, n), generator=g, dtype=torch.float64)) / (2 * n ** 0.5)
+    Ac = Ac + 2 * torch.eye(n)
+    A = torch.zeros((batch, 2, n, ld), dtype=torch.float32)
+    A[:, 0, :, :n] = Ac.real.transpose(1, 2).float()
+    A[:, 1, :, :n] = Ac.imag.transpose(1, 2).float()
+    A = A.cuda()
+    X = torch.zeros_like(A)
+    piv = torch.zeros((batch, n), dtype=torch.int32, device='cuda')
+    info = torch.zeros(batch, dtype=torch.int32, device='cuda')
+    wb = int(_lib.lib().mnpb_f32_workspace(n, batch))
+    work = torch.empty(wb, dtype=torch.uint8, device='cuda')
+    sh = _lib.stream_handle()
+    call('mnpb_getrf_c32p', sh, n, batch, ptr(A), ld, n * ld, 2 * n * ld, ptr(piv), n, ptr(info),
+         ptr(work), wb)
+    call('mnpb_getri_c32p', sh, n, batch, ptr(A), ld, n * ld, 2 * n * ld, ptr(piv), n, ptr(X),
+         ld, n * ld, 2 * n * ld, ptr(work), wb)
+    torch.cuda.synchronize()
+    Xc = (X[:, 0, :, :n].double() + 1j * X[:, 1, :, :n].double()).transpose(1, 2).cpu()
+    E = Ac @ Xc - torch.eye(n)
+    err = (E.abs().pow(2).sum() / n).sqrt().item()
+    assert err < 1e-2, err
+    ref = torch.linalg.inv(Ac)
+    rel = ((Xc - ref).abs().pow(2).sum() / ref.abs().pow(2).sum()).sqrt().item()
+    assert rel < 1e-2, rel
