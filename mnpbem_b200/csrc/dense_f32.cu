@@ -594,12 +594,20 @@ __global__ void __launch_bounds__(TINV_THREADS) tri_inv_kernel(int n, int lower,
 // place: the right-hand sides of a left leaf, read by the tensor cores as the
 // B operand (which would otherwise drop the low mantissa bits, a bias towards
 // zero) and overwritten by the leaf's result right after.
-__global__ void round_tf32_kernel(float *B, int64_t ldb, int64_t plane, int64_t sB, int rows) {
+// One CTA rounds RT_COLS columns of `rows` (<= 128) entries, both planes.
+constexpr int RT_COLS = 8;
+__global__ void __launch_bounds__(128) round_tf32_kernel(float *B, int64_t ldb, int64_t plane,
+                                                         int64_t sB, int rows, int cols) {
     const int i = threadIdx.x;
     if (i >= rows) return;
-    float *p = B + blockIdx.y * sB + (int64_t)blockIdx.x * ldb + i;
-    p[0] = tf32_rna(p[0]);
-    p[plane] = tf32_rna(p[plane]);
+    const int c0 = blockIdx.x * RT_COLS, c1 = min(cols, c0 + RT_COLS);
+    float *base = B + blockIdx.y * sB + i;
+#pragma unroll
+    for (int c = c0; c < c1; ++c) {
+        float *p = base + (int64_t)c * ldb;
+        p[0] = tf32_rna(p[0]);
+        p[plane] = tf32_rna(p[plane]);
+    }
 }
 
 // Skinny GEMM C = alpha A B + beta C for at most NC (<= 16) columns (matrix
@@ -1414,8 +1422,13 @@ static int trsm_rec(Ctx &c, int mode, int n, int m, CMatF T, CMatF B, const InvS
         const CMatF I = inv_block(*iv, blk0);
         // right leaf: A is the not-yet-rounded right-hand side, packed with rounding
         if (mode >= 2) return gemm(c, m, n, n, 1.f, B, I, 0.f, B, true);
-        round_tf32_kernel<<<dim3(m, c.batch), TL, 0, c.s>>>(B.p, B.ld, B.plane, B.stride, n);
-        MNPB_LAUNCH_CHECK("round_tf32_kernel");
+        {
+            ProfScope ps(c.s, PC_PACK, 16.0 * (double)n * m * c.batch);   // bytes read + written
+            prof_tag("round n=%d m=%d B=%d", n, m, c.batch);
+            round_tf32_kernel<<<dim3(ceil_div(m, RT_COLS), c.batch), TL, 0, c.s>>>(
+                B.p, B.ld, B.plane, B.stride, n, m);
+            MNPB_LAUNCH_CHECK("round_tf32_kernel");
+        }
         return gemm(c, n, m, n, 1.f, I, B, 0.f, B, true, true);
     }
     const int n1 = iv ? split_tl(n) : split_point(n);
