@@ -70,7 +70,9 @@ int mnpb_prof_dump(const char *path);
 /* Near/self classification of face pairs, host side, integer-exact.
  * Replaces mnpbem/greenfun/refine_utils.py:29 refinematrix (and its twin
  * mnpbem/greenfun/utils.py:43).  pos*: n x 3 row-major doubles, rad*:
- * boundary-element radii.  Writes CSR rows (row_ptr n1+1), column indices
+ * boundary-element radii (rad1 may be NULL: sources without a radius, such as
+ * points, are measured in units of rad2, the reference's fallback at
+ * refine_utils.py:97-101).  Writes CSR rows (row_ptr n1+1), column indices
  * and kinds (1 near, 2 self) for up to `cap` pairs; *nnz receives the total
  * count.  Returns MNPB_ENOMEM (after setting *nnz) if cap is too small. */
 int mnpb_refinematrix(int64_t n1, int64_t n2, const double *pos1, const double *pos2,
@@ -432,6 +434,82 @@ int mnpb_green_apply(void *stream, int64_t n, const double *pos, const double *n
                      const double *sblk, const int64_t *rptr, const int32_t *cols,
                      const double *g, const double *fn, const double *f, int key, int mode,
                      int64_t m, const double *x, double *y);
+
+/* ---------------------------------------------------------------------------
+ * Points off the surface: dipole excitations and point-face Green functions
+ *
+ * Media are 1-based indices into per-wavelength tables of nmed complex values
+ * (eps, k = 2 pi / lambda sqrt(eps), nb = sqrt(eps)), laid out (batch, nmed);
+ * face_med (n x 2) holds the inside and outside medium of every face, pt_med
+ * the medium of every point (0: not in any medium, contributes nothing).
+ * Dipole moments dip are (npt x 3 x ndip); excitation column K index
+ * q * ndip + idip, K = npt * ndip.
+ * ------------------------------------------------------------------------- */
+
+/* Potentials of the dipoles at the faces, pots (batch x 16 x K x n) in the
+ * layout of mnpb_bemret_excitation.  Replaces
+ * mnpbem/simulation/dipole_ret.py:319-515 (DipoleRet.potential / _pot). */
+int mnpb_dipole_potential(void *stream, int64_t n, int64_t batch, int64_t npt, int64_t ndip,
+                          const double *pos, const double *nvec, const int32_t *face_med,
+                          const double *ptpos, const int32_t *pt_med, const double *dip,
+                          int nmed, const double *eps, const double *k, const double *k0,
+                          double *pots);
+
+/* The dipoles' own fields at nobs observation positions in media obs_med:
+ * e, h (batch x nobs x 3 x K).  Replaces dipole_ret.py:163-317
+ * (DipoleRet.field / _dipolefield, Jackson 9.18). */
+int mnpb_dipole_field(void *stream, int64_t nobs, int64_t batch, int64_t npt, int64_t ndip,
+                      const double *obs, const int32_t *obs_med, const double *ptpos,
+                      const int32_t *pt_med, const double *dip, int nmed, const double *eps,
+                      const double *k, const double *nb, double *e, double *h);
+
+/* Adds the far fields of the dipoles whose pt_on flag is set (points in the
+ * embedding medium) to e, h (batch x K x ndir x 3, the layout of
+ * mnpb_farfield).  emb: per wavelength eps, k, nb of the embedding medium
+ * (batch x 3 complex).  Replaces dipole_ret.py:602-672 (DipoleRet.farfield). */
+int mnpb_dipole_farfield(void *stream, int64_t ndir, int64_t batch, int64_t npt, int64_t ndip,
+                         const double *ptpos, const int8_t *pt_on, const double *dip,
+                         const double *dirs, const double *emb, double *e, double *h);
+
+/* Refined Taylor coefficients (order 5, Cartesian derivative) of nref
+ * point-face pairs (rows: points, cols: faces; from mnpb_refinematrix with
+ * rad1 = NULL), integrated over the faces' quadrature points (qpos, qw, qoff
+ * as for mnpb_refine_coefficients): g (nref x 6), f (nref x 3 x 6).
+ * Replaces greenfun/greenret_refined.py:287-442 with a point set as p1. */
+int mnpb_refine_points(void *stream, int64_t npt, const double *ptpos, int64_t n,
+                       const double *pos, int64_t nref, const int32_t *rows, const int32_t *cols,
+                       const double *qpos, const double *qw, const int64_t *qoff, double *g,
+                       double *f);
+
+/* Fields (mode 0) or potentials (mode 1) at the points from surface charges
+ * and currents sol (batch x 8 x K x n, the solver's output layout), entries
+ * computed on the fly (far formula, refined pairs from the CSR rptr / cols
+ * with columns ascending and coefficients g, f of mnpb_refine_points).
+ * k: (batch x nmed) wavenumbers, k0: (batch) 2 pi / lambda.
+ *   mode 0: o1 = e, o2 = h (batch x npt x 3 x KC);
+ *           e = i k0 sum_j G h_s - Gp sig_s, h = sum_j Gp x h_s
+ *   mode 1: o1 = phi (batch x npt x KC), o2 = a (batch x npt x 3 x KC)
+ * over faces j and their sides s that border the point's medium.  diag = 0:
+ * all K columns (KC = K); diag > 0: point q reads only its own columns
+ * [q diag, (q + 1) diag) and KC = diag (what decay rates need).  Replaces
+ * greenfun/compgreen_ret.py:912-1036 (CompGreenRet(points, particle).field /
+ * potential). */
+int mnpb_point_green(void *stream, int64_t npt, const double *ptpos, const int32_t *pt_med,
+                     int64_t n, const double *pos, const double *area, const int32_t *face_med,
+                     int nmed, const double *k, const int64_t *rptr, const int32_t *cols,
+                     const double *g, const double *f, int mode, int64_t batch, int64_t K,
+                     int64_t diag, const double *k0, const double *sol, double *o1, double *o2);
+
+/* Entries of the point-face region pair (points, side `side` of the faces)
+ * for one wavelength: G (vec = 0, out npt x ncol) or Gp = H1p = H2p (vec = 1,
+ * out npt x 3 x ncol) for face columns [col_start, col_start + ncol).
+ * Replaces compgreen_ret.py:507-553 eval with a point set as p1. */
+int mnpb_point_green_eval(void *stream, int64_t npt, const double *ptpos, const int32_t *pt_med,
+                          int64_t n, const double *pos, const double *area,
+                          const int32_t *face_med, int nmed, const double *k,
+                          const int64_t *rptr, const int32_t *cols, const double *g,
+                          const double *f, int side, int vec, int64_t col_start, int64_t ncol,
+                          double *out);
 
 /* ---------------------------------------------------------------------------
  * Plane-wave excitation and cross sections (batched over wavelengths)

@@ -89,6 +89,16 @@ SIGNATURES = {
                          _P, _P],
     'mnpb_planewave_potential': [_P, _I64, _I64, _I64, _P, _P, _P, _P, _P, _P, _P, _P, _P],
     'mnpb_farfield': [_P, _I64, _I64, _I64, _I64, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P],
+    'mnpb_dipole_potential': [_P, _I64, _I64, _I64, _I64, _P, _P, _P, _P, _P, _P, _I, _P, _P,
+                              _P, _P],
+    'mnpb_dipole_field': [_P, _I64, _I64, _I64, _I64, _P, _P, _P, _P, _P, _I, _P, _P, _P, _P,
+                          _P],
+    'mnpb_dipole_farfield': [_P, _I64, _I64, _I64, _I64, _P, _P, _P, _P, _P, _P, _P],
+    'mnpb_refine_points': [_P, _I64, _P, _I64, _P, _I64, _P, _P, _P, _P, _P, _P, _P],
+    'mnpb_point_green': [_P, _I64, _P, _P, _I64, _P, _P, _P, _I, _P, _P, _P, _P, _P, _I, _I64,
+                         _I64, _I64, _P, _P, _P, _P],
+    'mnpb_point_green_eval': [_P, _I64, _P, _P, _I64, _P, _P, _P, _I, _P, _P, _P, _P, _P, _I,
+                              _I, _I64, _I64, _P],
 }
 _RESTYPE = {'mnpb_last_error': C.c_char_p, 'mnpb_launch_count': C.c_int64,
             'mnpb_cgemm_tf32_workspace': C.c_int64, 'mnpb_bemret_workspace_mixed': C.c_int64,

@@ -245,7 +245,8 @@ extern "C" int64_t mnpb_launch_count(void) { return g_launches.load(); }
 //
 // d = sqrt(|p1|^2 + |p2|^2 - 2 p1.p2) with d^2 < 1e-10 -> 0; kind 2 where
 // d == 0, kind 1 where (d - rad2_j < abs_cutoff) or ((d - rad2_j)/rad1_i <
-// rel_cutoff).  The norms are summed x, y, z in order; the cross term is the
+// rel_cutoff); rad1 == NULL divides by rad2_j instead (sources without a
+// boundary radius, such as points).  The norms are summed x, y, z in order; the cross term is the
 // 3-term dot product summed in the same order.  This file is compiled without
 // floating-point contraction so no fused multiply-add changes the rounding.
 // ---------------------------------------------------------------------------
@@ -255,7 +256,7 @@ extern "C" int mnpb_refinematrix(int64_t n1, int64_t n2, const double *pos1, con
                                  int32_t *cols, int8_t *kinds) {
     clear_error();
     MNPB_REQUIRE(n1 >= 0 && n2 >= 0, "refinematrix: negative size");
-    MNPB_REQUIRE(pos1 && pos2 && rad1 && rad2 && nnz && row_ptr, "refinematrix: null pointer");
+    MNPB_REQUIRE(pos1 && pos2 && rad2 && nnz && row_ptr, "refinematrix: null pointer");
     std::vector<double> sq2(n2);
     for (int64_t j = 0; j < n2; ++j) {
         const double *q = pos2 + 3 * j;
@@ -284,7 +285,7 @@ extern "C" int mnpb_refinematrix(int64_t n1, int64_t n2, const double *pos1, con
                 kind = 2;
             } else {
                 double dd = d - rad2[j];
-                double idr = dd / rad1[i];
+                double idr = dd / (rad1 ? rad1[i] : rad2[j]);
                 if (dd < abs_cutoff || idr < rel_cutoff) kind = 1;
             }
             if (kind) {

@@ -73,11 +73,13 @@ def _points(p, which):
 
 
 def refinematrix_csr(pos1, pos2, rad1, rad2, abs_cutoff=0.0, rel_cutoff=3.0):
-    """Near/self pair list as CSR (row_ptr, cols, kinds) via the C classifier."""
+    """Near/self pair list as CSR (row_ptr, cols, kinds) via the C classifier.
+    ``rad1=None``: sources without a boundary radius (points), distances in
+    units of the column face's radius."""
     L = _lib.lib()
     pos1 = np.ascontiguousarray(pos1, dtype=np.float64)
     pos2 = np.ascontiguousarray(pos2, dtype=np.float64)
-    rad1 = np.ascontiguousarray(rad1, dtype=np.float64)
+    rad1 = None if rad1 is None else np.ascontiguousarray(rad1, dtype=np.float64)
     rad2 = np.ascontiguousarray(rad2, dtype=np.float64)
     n1, n2 = pos1.shape[0], pos2.shape[0]
     row_ptr = np.zeros(n1 + 1, dtype=np.int64)
@@ -331,6 +333,13 @@ class CompGreenRet(object):
     entries (no n x n matrix is stored for them).
     """
 
+    def __new__(cls, p1, p2=None, **options):
+        # a point set as p1 (the reference's CompGreenRet(ComPoint, particle))
+        from .points import is_point_set, CompGreenRetPoints
+        if is_point_set(p1) and p2 is not None:
+            return CompGreenRetPoints(p1, p2, **options)
+        return super(CompGreenRet, cls).__new__(cls)
+
     def __init__(self, p1, p2=None, **options):
         if p2 is not None and p2 is not p1:
             raise NotImplementedError("CompGreenRet: only p1 is p2 (the BEM matrices) is supported")
@@ -483,6 +492,13 @@ class CompGreenStat(object):
     H1, H2, Gp, H1p, H2p (mnpbem/greenfun/compgreen_stat.py:219-294, 466-528,
     678-990).  Entries come from the retarded entry kernel at k = 0, where the
     phase is 1 and only the order-0 refined coefficients remain."""
+
+    def __new__(cls, p1, p2=None, **options):
+        # a point set as p1 (the reference's CompGreenRet(ComPoint, particle))
+        from .points import is_point_set, CompGreenRetPoints
+        if is_point_set(p1) and p2 is not None:
+            return CompGreenRetPoints(p1, p2, **options)
+        return super(CompGreenRet, cls).__new__(cls)
 
     def __init__(self, p1, p2=None, **options):
         if p2 is not None and p2 is not p1:
