@@ -512,6 +512,59 @@ int mnpb_point_green_eval(void *stream, int64_t npt, const double *ptpos, const 
                           double *out);
 
 /* ---------------------------------------------------------------------------
+ * Electron beams (EELS, retarded)
+ *
+ * Beams run along z through impact parameters impact (nimp x 2) with width
+ * `width` (> 0) and velocity vel (units of c, 0 < vel < 1).  Faces with
+ * indquad[i * nimp + j] set are integrated over their quadrature points
+ * (qpos, qw, qoff as for mnpb_refine_coefficients, weights divided by the
+ * face area), the others take their centroid.  K0 and K1 of complex argument
+ * are evaluated for |arg z| <= 1.2 (the caller checks 1/gamma).
+ * ------------------------------------------------------------------------- */
+
+/* BEM excitation pots (batch x 16 x nimp x n): face side s with medium m gets
+ * the infinite-beam potential of medium m (1/gamma_m = igam, eps_m) for every
+ * impact with beam_in[(m - 1) * nimp + j] set, if med_on[m - 1]:
+ * phi / eps, phi' / eps and vel z^ phi, vel z^ phi'.  q: (batch) 2 pi /
+ * (lambda vel); eps, igam: (batch x nmed) complex.  Replaces
+ * mnpbem/simulation/eels_ret.py:149-294 with eels_base.py:315-416. */
+int mnpb_eels_potential(void *stream, int64_t n, int64_t batch, int64_t nimp, const double *pos,
+                        const double *nvec, const double *area, const int32_t *face_med,
+                        int nmed, const int8_t *med_on, const int8_t *beam_in,
+                        const double *impact, const int8_t *indquad, const double *qpos,
+                        const double *qw, const int64_t *qoff, double width, double vel,
+                        const double *q, const double *eps, const double *igam, double *pots);
+
+/* Infinite-beam potentials phi, phip (nimp x n complex) of one medium
+ * (1/gamma = igam) at faces with face_on set, 0 elsewhere
+ * (eels_base.py:315-416, potinfty). */
+int mnpb_eels_infty(void *stream, int64_t n, int64_t nimp, const double *pos, const double *nvec,
+                    const double *area, const int8_t *face_on, const double *impact,
+                    const int8_t *indquad, const double *qpos, const double *qw,
+                    const int64_t *qoff, double width, double vel, double q, double igam_re,
+                    double igam_im, double *phi, double *phip);
+
+/* Potentials phi (nseg x n complex) of beam segments [seg[2c], seg[2c+1]] of
+ * impact seg_imp[c] inside particles, -1/vel times the charged-wire integral
+ * with wavenumbers q (beam) and k (medium) on the 11 Legendre-Gauss-Lobatto
+ * nodes lgl_x / weights lgl_w (host arrays) (eels_base.py:418-523 and
+ * 713-783, potinside / potwire). */
+int mnpb_eels_wire(void *stream, int64_t n, int64_t nimp, const double *pos, const double *nvec,
+                   const double *area, const int8_t *face_on, const double *impact,
+                   const int8_t *indquad, const double *qpos, const double *qw,
+                   const int64_t *qoff, double width, double vel, int64_t nseg,
+                   const double *seg, const int32_t *seg_imp, double q, double k_re, double k_im,
+                   const double *lgl_x, const double *lgl_w, double *phi);
+
+/* Fields of the beams at nobs positions in media obs_med: e, h (nobs x 3 x
+ * nimp complex); mtab (nmed x 3 complex): eps, q = k / (vel sqrt(eps)) and
+ * 1/gamma of every medium (eels_ret.py:506-637). */
+int mnpb_eels_field(void *stream, int64_t nobs, int64_t nimp, const double *obs,
+                    const int32_t *obs_med, int nmed, const int8_t *beam_in,
+                    const double *impact, double width, double vel, const double *mtab,
+                    double *e, double *h);
+
+/* ---------------------------------------------------------------------------
  * Plane-wave excitation and cross sections (batched over wavelengths)
  * ------------------------------------------------------------------------- */
 

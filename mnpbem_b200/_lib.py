@@ -97,6 +97,13 @@ SIGNATURES = {
     'mnpb_refine_points': [_P, _I64, _P, _I64, _P, _I64, _P, _P, _P, _P, _P, _P, _P],
     'mnpb_point_green': [_P, _I64, _P, _P, _I64, _P, _P, _P, _I, _P, _P, _P, _P, _P, _I, _I64,
                          _I64, _I64, _P, _P, _P, _P],
+    'mnpb_eels_potential': [_P, _I64, _I64, _I64, _P, _P, _P, _P, _I, _P, _P, _P, _P, _P, _P,
+                            _P, _D, _D, _P, _P, _P, _P],
+    'mnpb_eels_infty': [_P, _I64, _I64, _P, _P, _P, _P, _P, _P, _P, _P, _P, _D, _D, _D, _D, _D,
+                        _P, _P],
+    'mnpb_eels_wire': [_P, _I64, _I64, _P, _P, _P, _P, _P, _P, _P, _P, _P, _D, _D, _I64, _P, _P,
+                       _D, _D, _D, _P, _P, _P],
+    'mnpb_eels_field': [_P, _I64, _I64, _P, _P, _I, _P, _P, _D, _D, _P, _P, _P],
     'mnpb_point_green_eval': [_P, _I64, _P, _P, _I64, _P, _P, _P, _I, _P, _P, _P, _P, _P, _I,
                               _I, _I64, _I64, _P],
 }
