@@ -3,7 +3,7 @@
 Drop-in classes with the reference call surface (``BEMRet``, ``BEMStat``,
 ``BEMRetIter``,
 ``CompGreenRet``, ``CompGreenStat``, ``PlaneWaveRet``, ``PlaneWaveStat``,
-``CompStruct``, ``ComParticle``) backed by hand-written sm_100a CUDA kernels
+``DipoleRet``, ``EELSRet``, ``ComPoint``, ``CompStruct``, ``ComParticle``) backed by hand-written sm_100a CUDA kernels
 in ``libmnpbem_b200.so`` (C ABI: include/mnpbem_b200.h).  There is no CPU
 fallback: importing the solvers requires the built library.
 """
@@ -30,4 +30,10 @@ def __getattr__(name):
     if name in ('PlaneWaveRet', 'PlaneWaveStat'):
         from . import excitation
         return getattr(excitation, name)
+    if name in ('DipoleRet', 'ComPoint', 'Point'):
+        from . import points
+        return getattr(points, name)
+    if name in ('EELSRet',):
+        from . import eels
+        return getattr(eels, name)
     raise AttributeError(name)
