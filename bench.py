@@ -51,11 +51,12 @@ def parse():
     ap.add_argument('--path', default='mixed', choices=['fp64', 'mixed'])
     ap.add_argument('--no-accuracy', action='store_true')
     ap.add_argument('--batch', type=int, default=81)
-    ap.add_argument('--refine-tol', type=float, default=1e-8,
+    ap.add_argument('--refine-tol', type=float, default=1e-6,
                     help='FP64 refinement stops per wavelength once its last correction is '
-                         'below this fraction of the solution (mixed path).  1e-8 keeps the '
-                         'extinction within ~2e-9 of the FP64 path, 500x inside the metric\'s '
-                         '1e-6 bound (the library default, 1e-11, gives 1e-11)')
+                         'below this fraction of the solution (mixed path).  1e-6 keeps the '
+                         'extinction within ~2e-8 and sigma within ~1e-8 of the FP64 path over '
+                         'the 81 wavelengths (measured), 50x inside the metric\'s 1e-6 bound '
+                         '(the library default, 1e-11, gives 1e-11)')
     ap.add_argument('--streams', type=int, default=1,
                     help='sub-batches of --batch wavelengths solved concurrently')
     ap.add_argument('--nlam', type=int, default=81)
@@ -77,7 +78,7 @@ def parse():
                          'dense FP64 GPU solve (empty: skip)')
     ap.add_argument('--mn-min-n', type=int, default=None,
                     help='GEMM knob: TF32 A operands of products with 64 < N < this are '
-                         'packed instead of read in place (library default 256)')
+                         'packed instead of read in place (library default 0: never)')
     ap.add_argument('--fp64-steps', type=int, default=None,
                     help='timed sweeps of the plain FP64 GPU path (default: --steps)')
     return ap.parse_args()

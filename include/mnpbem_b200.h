@@ -339,9 +339,9 @@ int mnpb_cgemm_tf32_ex(void *stream, int64_t m, int64_t n, int64_t k, int64_t ba
 int mnpb_gemm_config(int32_t bn_wide, int32_t persist_tiles_per_sm, int32_t stages);
 /* A operand that holds TF32 values (MNPB_GEMM_A_TF32 and the factorisation's
  * stored factors) is packed K-major first instead of being read in place
- * when 64 < N < mn_min_n (default 256) and a workspace is at hand (exact for
- * TF32 values; the 128-wide tile streams a tall in-place A at about half the
- * packed layout's rate).  0: always in place. */
+ * when 64 < N < mn_min_n and a workspace is at hand (exact for TF32 values).
+ * Default 0: always in place (over the 2884-face, 81-wavelength sweep the
+ * packing costs more than the in-place reads lose). */
 int mnpb_gemm_config_mn(int32_t mn_min_n);
 
 /* Same GEMM as mnpb_cgemm_tf32, but it allocates nothing and takes no

@@ -773,7 +773,7 @@ static std::atomic<int> g_cfg_bn{128}, g_cfg_persist{2}, g_cfg_stages{0};
 // packed K-major first (exact for TF32 values).  Narrow products (N of one or
 // two 128-column tiles) stream their tall A only once per tile column, where
 // the MN-major boxes reach about half the HBM rate of the packed layout.
-static std::atomic<int> g_cfg_mn_min_n{256};
+static std::atomic<int> g_cfg_mn_min_n{0};
 static std::atomic<int64_t> g_cfg_epoch{0};
 
 int64_t gemm_config_epoch() { return g_cfg_epoch.load(); }

@@ -378,7 +378,7 @@ class DipoleRet(object):
         self.h_pos, self.h_med = h_pos, h_med
         self._dev = None
         self._faces = {}
-        self._green = {}
+        self._greens = {}
 
     @property
     def ndip(self):
@@ -531,9 +531,9 @@ class DipoleRet(object):
 
     def _green(self, p):
         key = id(p)
-        if key not in self._green:
-            self._green[key] = (p, CompGreenRetPoints(self.pt, p, **self.varargin))
-        return self._green[key][1]
+        if key not in self._greens:
+            self._greens[key] = (p, CompGreenRetPoints(self.pt, p, **self.varargin))
+        return self._greens[key][1]
 
     def decayrate(self, sig):
         """Total, radiative and free-space decay rates (npt, ndip)
