@@ -73,7 +73,7 @@ def parse():
                     help='skip the 64-particle uneven batched section')
     ap.add_argument('--batch-particles', type=int, default=64)
     ap.add_argument('--batch-nlam', type=int, default=41)
-    ap.add_argument('--iter-accuracy-tols', default='1e-6,1e-8,1e-10',
+    ap.add_argument('--iter-accuracy-tols', default='1e-6,1e-8',
                     help='GMRES tolerances whose 25k-face extinction is compared with the '
                          'dense FP64 GPU solve (empty: skip)')
     ap.add_argument('--mn-min-n', type=int, default=None,
