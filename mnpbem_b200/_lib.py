@@ -104,11 +104,23 @@ SIGNATURES = {
     'mnpb_eels_wire': [_P, _I64, _I64, _P, _P, _P, _P, _P, _P, _P, _P, _P, _D, _D, _I64, _P, _P,
                        _D, _D, _D, _P, _P, _P],
     'mnpb_eels_field': [_P, _I64, _I64, _P, _P, _I, _P, _P, _D, _D, _P, _P, _P],
+    'mnpb_mirror_contract': [_P, _I64, _I64, _I64, _I64, _P, _I64, _I64, _P, _P, _I64, _I64],
+    'mnpb_bemret_mirror_workspace': [_I64, _I64],
+    'mnpb_bemret_init_mirror_f64': [_P, _I64, _I64, _P, _P, _P, _P, _I64, _I64, _P, _P, _P, _P,
+                                    _I64],
+    'mnpb_bemret_sigma_mirror_f64': [_P, _I64, _I64, _I64, _P, _P, _P, _I64, _I64, _P, _P, _P,
+                                     C.c_int32, C.c_int32, C.c_int32, _P, _I64, _P, _P],
+    'mnpb_bemret_solve_mirror_workspace': [_I64, _I64, _I64],
+    'mnpb_bemret_solve_mirror_f64': [_P, _I64, _I64, _I64, _I64, _P, _P, _P, _P, _I64, _I64, _P,
+                                     _P, _I64, _P, C.c_int32, C.c_int32, C.c_int32, _P, _P, _P,
+                                     _P, _P, _P, _I64],
     'mnpb_point_green_eval': [_P, _I64, _P, _P, _I64, _P, _P, _P, _I, _P, _P, _P, _P, _P, _I,
                               _I, _I64, _I64, _P],
 }
 _RESTYPE = {'mnpb_last_error': C.c_char_p, 'mnpb_launch_count': C.c_int64,
             'mnpb_cgemm_tf32_workspace': C.c_int64, 'mnpb_bemret_workspace_mixed': C.c_int64,
+            'mnpb_bemret_mirror_workspace': C.c_int64,
+            'mnpb_bemret_solve_mirror_workspace': C.c_int64,
             'mnpb_bemret_refine_workspace': C.c_int64, 'mnpb_f32_workspace': C.c_int64, 'mnpb_bemret_dinv_floats': C.c_int64,
             'mnpb_bemret_workspace_f64': C.c_int64, 'mnpb_gmres_workspace': C.c_int64}
 

@@ -1,0 +1,386 @@
+"""Particles with mirror symmetry: the retarded BEM solver on the irreducible
+part of a mirror-symmetric particle.
+
+``ComParticleMirror``, ``CompStructMirror``, ``PlaneWaveRetMirror`` and
+``BEMRetMirror`` mirror mnpbem/geometry/comparticle_mirror.py,
+mnpbem/simulation/planewave_ret_mirror.py and mnpbem/bem/bem_ret_mirror.py:
+the user gives the part of the particle with x >= 0 (sym 'x'), y >= 0
+('y') or both ('xy'); the full particle is that part and its 1 or 3 mirror
+images.  Every excitation is split into components with definite parity
+under the mirror planes (symmetry values, rows of ``symtable``), and each
+component is solved on the irreducible part alone: 2 or 4 BEM systems of
+size n instead of one of size 2n or 4n.
+
+GPU work (``libmnpbem_b200.so``): the full particle's Green functions
+(``mnpb_assemble_ret``, rows of the irreducible part used), their
+contraction to one n x n matrix per symmetry value (``mnpb_mirror_contract``),
+the per-symmetry-value factorisations (``mnpb_bemret_init_mirror_f64``),
+the Sigma matrix of every (x, y, z) symmetry-value combination
+(``mnpb_bemret_sigma_mirror_f64``) and the solves
+(``mnpb_bemret_solve_mirror_f64``), all in FP64.
+"""
+
+import numpy as np
+import torch
+
+from . import _lib
+from ._lib import call, ptr
+from .compstruct import CompStruct
+from .geometry import Particle, ComParticle
+from .greenfun import SurfaceTables
+from .excitation import PlaneWaveRet
+
+__all__ = ["flip", "ComParticleMirror", "CompStructMirror", "PlaneWaveRetMirror",
+           "BEMRetMirror"]
+
+
+def flip(p, dirs):
+    """The particle mirrored at the planes normal to ``dirs`` (0 x, 1 y, 2 z)
+    with its faces' vertex order reversed so the normals point outwards
+    again (mnpbem/geometry/particle.py:843-905, flip / flipfaces)."""
+    dirs = [dirs] if np.isscalar(dirs) else list(dirs)
+    if p.faces2 is not None:
+        v = np.array(p.verts2, dtype=float)
+        f = np.array(p.faces2, dtype=float)
+        for d in dirs:
+            v[:, d] = -v[:, d]
+        tri = np.isnan(f[:, 3])
+        g = f.copy()
+        g[np.ix_(tri, [0, 1, 2, 4, 5, 6])] = f[np.ix_(tri, [2, 1, 0, 5, 4, 6])]
+        g[np.ix_(~tri, [0, 1, 2, 3, 4, 5, 6, 7])] = f[np.ix_(~tri, [3, 2, 1, 0, 6, 5, 4, 7])]
+        return Particle(v, g, interp=p.interp)
+    v = np.array(p.verts, dtype=float)
+    f = np.array(p.faces, dtype=float)
+    for d in dirs:
+        v[:, d] = -v[:, d]
+    tri = np.isnan(f[:, 3])
+    g = f.copy()
+    g[np.ix_(tri, [0, 1, 2])] = f[np.ix_(tri, [2, 1, 0])]
+    g[np.ix_(~tri, [0, 1, 2, 3])] = f[np.ix_(~tri, [3, 2, 1, 0])]
+    return Particle(v, g, interp=p.interp)
+
+
+_SYMVAL = {'+': [1, 1], '-': [1, -1],
+           '++': [1, 1, 1, 1], '+-': [1, 1, -1, -1], '-+': [1, -1, 1, -1], '--': [1, -1, -1, 1]}
+
+
+class ComParticleMirror(object):
+    """Irreducible part of a mirror-symmetric particle
+    (mnpbem/geometry/comparticle_mirror.py:110-404).
+
+    ``ComParticleMirror(eps, particles, inout, sym='x', closed_args=None)``:
+    ``closed_args`` (e.g. ``(1,)``) marks particles whose surface, together
+    with its mirror images, is closed; without it every piece is taken as
+    its own closed surface, as the reference does.  ``full()`` is the full particle: the given particles,
+    then their x images, then (sym 'y' / 'xy') the y images of all of those.
+    Face data (pos, nvec, area) are those of the irreducible part, the first
+    n faces of the full particle.
+    """
+
+    def __init__(self, eps, particles, inout, sym='x', closed_args=None, **kwargs):
+        if not isinstance(sym, str):
+            if closed_args is not None:
+                raise ValueError("ComParticleMirror: cannot pass both numeric sym and "
+                                 "closed_args")
+            closed_args = tuple(sym) if hasattr(sym, '__iter__') else (sym,)
+            sym = kwargs.pop('sym', 'x')
+        closed = tuple(closed_args) if closed_args is not None else ()
+        if sym not in ('x', 'y', 'xy'):
+            raise ValueError("ComParticleMirror: 'sym' must be one of 'x', 'y', 'xy'; got {!r}"
+                             .format(sym))
+        self.eps = list(eps)
+        self.p = list(particles)
+        self.inout = np.atleast_2d(np.asarray(inout, dtype=int))
+        self.sym = sym
+        if sym in ('x', 'y'):
+            self.symtable = np.array([[1, 1], [1, -1]], dtype=np.float64)
+        else:
+            self.symtable = np.array([[1, 1, 1, 1], [1, 1, -1, -1], [1, -1, 1, -1],
+                                      [1, -1, -1, 1]], dtype=np.float64)
+        plist, io = list(self.p), [list(r) for r in self.inout]
+        if sym in ('x', 'xy'):
+            m = len(plist)
+            plist += [flip(plist[i], 0) for i in range(m)]
+            io += [io[i] for i in range(m)]
+        if sym in ('y', 'xy'):
+            m = len(plist)
+            plist += [flip(plist[i], 1) for i in range(m)]
+            io += [io[i] for i in range(m)]
+        self.pfull = ComParticle(self.eps, plist, io)
+        nk = self.symtable.shape[1]
+        m = len(self.p)
+        if closed:
+            # particle c together with its mirror images forms a closed surface
+            full_closed = [None] * (m * nk)
+            for c in closed:
+                for c1 in np.atleast_1d(c):
+                    c1 = int(c1)
+                    imgs = [c1 + k * m for k in range(nk)]
+                    for j in imgs:
+                        full_closed[j - 1] = imgs
+            self.pfull.closed = [c if c is not None else [j + 1]
+                                 for j, c in enumerate(full_closed)]
+        self._n = sum(q.nfaces for q in self.p)
+
+    @property
+    def nk(self):
+        return self.symtable.shape[1]
+
+    def full(self):
+        return self.pfull
+
+    @property
+    def n(self):
+        return self._n
+
+    nfaces = n
+
+    @property
+    def pos(self):
+        return np.asarray(self.pfull.pos)[:self._n]
+
+    @property
+    def nvec(self):
+        return np.asarray(self.pfull.nvec)[:self._n]
+
+    @property
+    def area(self):
+        return np.asarray(self.pfull.area)[:self._n]
+
+    def eps1(self, enei):
+        return np.asarray(self.pfull.eps1(enei))[:self._n]
+
+    def eps2(self, enei):
+        return np.asarray(self.pfull.eps2(enei))[:self._n]
+
+    def symvalue(self, key):
+        """Symmetry values of ``key`` ('+', '-' for sym x / y; '++', '+-',
+        '-+', '--' for xy), one row per key (comparticle_mirror.py:318-345)."""
+        keys = [key] if isinstance(key, str) else list(key)
+        for k in keys:
+            if k not in _SYMVAL or len(_SYMVAL[k]) != self.nk:
+                raise ValueError("Unknown symmetry key: {}".format(k))
+        return np.array([_SYMVAL[k] for k in keys], dtype=np.float64)
+
+    def symindex(self, tab):
+        """Row of ``symtable`` equal to the symmetry values ``tab``."""
+        tab = np.atleast_1d(tab)
+        for i in range(self.symtable.shape[0]):
+            if np.allclose(self.symtable[i], tab):
+                return i
+        raise ValueError("Symmetry values {} not found in table".format(tab))
+
+
+_SCALARS = ('phi', 'phip', 'phi1', 'phi2', 'phi1p', 'phi2p', 'sig', 'sig1', 'sig2')
+_VECTORS = ('a1', 'a1p', 'a2', 'a2p', 'e', 'h', 'h1', 'h2')
+
+
+class CompStructMirror(object):
+    """Values of the irreducible part, one ``CompStruct`` per symmetry
+    combination in ``val`` (each with a 3 x nk ``symval``: rows x, y, z)
+    (comparticle_mirror.py:9-106)."""
+
+    def __init__(self, p, enei, fun=None):
+        self.p = p
+        self.enei = enei
+        self.fun = fun
+        self.val = []
+
+    def full(self):
+        return self.fun(self) if self.fun is not None else self
+
+    def expand(self):
+        """Every value on the full particle: image k of a scalar is
+        symval[z, k] times the value, component l of a vector
+        symval[l, k] times its component l."""
+        out = []
+        pf = self.p.full()
+        for v in self.val:
+            sv = v.symval
+            nk = sv.shape[1]
+            r = CompStruct(pf, self.enei)
+            for name, a in v.val.items():
+                if name == 'symval' or not isinstance(a, np.ndarray):
+                    continue
+                if name in _SCALARS:
+                    r[name] = np.concatenate([a] + [sv[-1, k] * a for k in range(1, nk)])
+                elif name in _VECTORS:
+                    parts = [a]
+                    for k in range(1, nk):
+                        b = a.copy()
+                        for l in range(3):
+                            b[:, l] = sv[l, k] * a[:, l]
+                        parts.append(b)
+                    r[name] = np.concatenate(parts)
+            out.append(r)
+        return tuple(out)
+
+
+class PlaneWaveRetMirror(object):
+    """Plane waves along +-z on a mirror-symmetric particle
+    (mnpbem/simulation/planewave_ret_mirror.py:8-198): pol in the xy plane."""
+
+    def __init__(self, pol, dir, medium=1, **options):
+        pol = np.atleast_2d(np.asarray(pol, dtype=float))
+        dir = np.atleast_2d(np.asarray(dir, dtype=float))
+        if not np.allclose(pol[:, 2], 0):
+            raise AssertionError("pol[:, 2] must be 0 for mirror symmetry")
+        self.pol, self.dir = pol, dir
+        self.exc = PlaneWaveRet(pol, dir, medium=medium, **options)
+
+    def potential(self, p, enei):
+        """Two components: x- and y-polarised waves along +z and -z (2
+        columns each), with the symmetry values of their x, y, z parts."""
+        pot = CompStructMirror(p, enei, lambda s: self.full(s))
+        for i in range(2):
+            pb = np.zeros((2, 3))
+            pb[:, i] = 1.0
+            db = np.array([[0, 0, 1.0], [0, 0, -1.0]])
+            pot.val.append(PlaneWaveRet(pb, db, medium=self.exc.medium).potential(p, enei))
+        keys = {'x': (['+', '-', '-'], ['-', '+', '+']),
+                'y': (['+', '-', '+'], ['-', '+', '-']),
+                'xy': (['++', '--', '-+'], ['--', '++', '+-'])}[p.sym]
+        pot.val[0].symval = p.symvalue(keys[0])
+        pot.val[1].symval = p.symvalue(keys[1])
+        return pot
+
+    __call__ = potential
+
+    def full(self, val):
+        """Values on the full particle for the requested polarisations:
+        pol_x times the x component plus pol_y times the y component, column
+        of the matching propagation direction."""
+        v1, v2 = val.expand()[:2]
+        pf = v1.p
+        out = CompStruct(pf, val.enei)
+        npol = self.pol.shape[0]
+        for name in v1.val:
+            if name not in v2.val or not isinstance(v1.val[name], np.ndarray):
+                continue
+            a, b = v1.val[name], v2.val[name]
+            shape = a.shape[:-1] + (npol,) if a.ndim > 1 else a.shape + (npol,)
+            r = np.zeros(shape, dtype=complex)
+            for ip in range(npol):
+                j = 0 if self.dir[ip, 2] > 0 else 1
+                r[..., ip] = self.pol[ip, 0] * a[..., j] + self.pol[ip, 1] * b[..., j]
+            out[name] = r
+        return out, pf
+
+    def extinction(self, sig):
+        return self.exc.extinction(self.full(sig)[0])
+
+    def scattering(self, sig):
+        return self.exc.scattering(self.full(sig)[0])
+
+    def absorption(self, sig):
+        return self.exc.absorption(self.full(sig)[0])
+
+
+class BEMRetMirror(object):
+    """Retarded BEM solver on the irreducible part of a mirror-symmetric
+    particle, FP64 on the GPU (mnpbem/bem/bem_ret_mirror.py:147-815)."""
+
+    def __init__(self, p, enei=None, **options):
+        if not isinstance(p, ComParticleMirror):
+            raise TypeError("BEMRetMirror: expected a ComParticleMirror")
+        self.p = p
+        self.device = torch.device('cuda')
+        self.tables = SurfaceTables(p.pfull, rel_cutoff=options.get('RelCutoff', 3),
+                                    abs_cutoff=options.get('AbsCutoff', 0))
+        self.enei = None
+        self.nvec = torch.from_numpy(np.ascontiguousarray(p.nvec, dtype=np.float64)).to(self.device)
+        if enei is not None:
+            self.init(enei)
+
+    def init(self, enei):
+        """Matrices of every symmetry value at ``enei`` (bem_ret_mirror.py:182-328)."""
+        if self.enei is not None and self.enei == enei:
+            return self
+        from .bem import _scalar_eps
+        p, t, dev = self.p, self.tables, self.device
+        n, nf, nk = p.n, t.n, p.nk
+        nsym = p.symtable.shape[0]
+        sh = _lib.stream_handle()
+        c128 = dict(dtype=torch.complex128, device=dev)
+        kblk, sblk = t.k_tables([enei])
+        full = [torch.empty((1, nf, nf), **c128) for _ in range(4)]   # G1, H1, G2, H2
+        t.assemble(kblk, sblk, tuple(full), mode=0)
+        G = torch.empty((2, nsym, n, n), **c128)
+        H = torch.empty((2, nsym, n, n), **c128)
+        tab = np.ascontiguousarray(p.symtable, dtype=np.float64)
+        for src, dst in ((full[0], G[0]), (full[2], G[1]), (full[1], H[0]), (full[3], H[1])):
+            call('mnpb_mirror_contract', sh, n, nk, nsym, 1, ptr(src), nf, nf * nf, ptr(tab),
+                 ptr(dst), n, n * n)
+        del full
+        self.G, self.H = G, H
+        self.Dinv = torch.empty((nsym, n, n), **c128)
+        self.piv = torch.empty((3, nsym, n), dtype=torch.int32, device=dev)
+        info = torch.zeros(3 * nsym, dtype=torch.int32, device=dev)
+        wb = int(_lib.lib().mnpb_bemret_mirror_workspace(n, nsym))
+        work = torch.empty(wb, dtype=torch.uint8, device=dev)
+        call('mnpb_bemret_init_mirror_f64', sh, n, nsym, ptr(G[0]), ptr(G[1]), ptr(H[0]),
+             ptr(H[1]), n, n * n, ptr(self.Dinv), ptr(self.piv), ptr(info), ptr(work), wb)
+        if info.any():
+            raise _lib.MNPBError('BEMRetMirror', 3, 'zero pivot in a symmetry block')
+        e1, e2 = _scalar_eps(p, enei)
+        self.eps = torch.tensor([[e1.real, e1.imag, e2.real, e2.imag]], dtype=torch.float64,
+                                device=dev)
+        self.kvac = torch.tensor([2 * np.pi / enei], dtype=torch.float64, device=dev)
+        self._sigma = {}
+        self.enei = enei
+        return self
+
+    def _sigma_lu(self, x, y, z):
+        key = (x, y, z)
+        if key not in self._sigma:
+            n = self.p.n
+            S = torch.empty((1, n, n), dtype=torch.complex128, device=self.device)
+            piv = torch.empty((1, n), dtype=torch.int32, device=self.device)
+            info = torch.zeros(1, dtype=torch.int32, device=self.device)
+            nsym = self.p.symtable.shape[0]
+            call('mnpb_bemret_sigma_mirror_f64', _lib.stream_handle(), n, nsym, 1,
+                 ptr(self.H[0]), ptr(self.H[1]), ptr(self.Dinv), n, n * n, ptr(self.eps),
+                 ptr(self.kvac), ptr(self.nvec), x, y, z, ptr(S), n * n, ptr(piv), ptr(info))
+            if info.any():
+                raise _lib.MNPBError('BEMRetMirror', 3, 'zero pivot in Sigma')
+            self._sigma[key] = (S, piv)
+        return self._sigma[key]
+
+    def solve(self, exc):
+        """Surface charges and currents of every symmetry component
+        (bem_ret_mirror.py:654-760): a ``CompStructMirror``."""
+        from .bem import BEMRet
+        self.init(exc.enei)
+        p = self.p
+        n = p.n
+        nsym = p.symtable.shape[0]
+        sh = _lib.stream_handle()
+        sig = CompStructMirror(p, exc.enei, exc.fun)
+        for v in exc.val:
+            sv = v.symval
+            x, y, z = (p.symindex(sv[0]), p.symindex(sv[1]), p.symindex(sv[2]))
+            S, pivS = self._sigma_lu(x, y, z)
+            pots, K = BEMRet._pots(v, n)
+            d_pots = torch.from_numpy(pots).to(self.device).unsqueeze(0)
+            xin = torch.empty((1, 8, K, n), dtype=torch.complex128, device=self.device)
+            xout = torch.empty_like(xin)
+            call('mnpb_bemret_excitation', sh, n, 1, K, ptr(d_pots), ptr(self.eps),
+                 ptr(self.kvac), ptr(self.nvec), 0, ptr(xin))
+            wb = int(_lib.lib().mnpb_bemret_solve_mirror_workspace(n, 1, K))
+            work = torch.empty(wb, dtype=torch.uint8, device=self.device)
+            call('mnpb_bemret_solve_mirror_f64', sh, n, nsym, 1, K, ptr(self.G[0]),
+                 ptr(self.G[1]), ptr(self.H[0]), ptr(self.Dinv), n, n * n, ptr(self.piv),
+                 ptr(S), n * n, ptr(pivS), x, y, z, ptr(self.eps), ptr(self.kvac),
+                 ptr(self.nvec), ptr(xin), ptr(xout), ptr(work), wb)
+            X = xout[0].cpu().numpy()
+            val = CompStruct(p, exc.enei, sig1=X[0].T.copy(), h1=X[1:4].transpose(2, 0, 1).copy(),
+                             sig2=X[4].T.copy(), h2=X[5:8].transpose(2, 0, 1).copy())
+            val.symval = sv
+            sig.val.append(val)
+        return sig, self
+
+    def __truediv__(self, exc):
+        return self.solve(exc)
+
+    def __call__(self, enei):
+        return self.init(enei)

@@ -1,0 +1,62 @@
+"""Mirror-symmetric solves on the GPU against the reference
+(golden_mirror.npz, made by running the reference's BEMRetMirror on CPU),
+and against this package's own full-particle solve.
+
+Tolerances, max-norm relative: surface charges and currents of every
+symmetry component 1e-10, cross sections 1e-10 (FP64 throughout); the
+mirror decomposition against the full-particle BEMRet 1e-9."""
+import numpy as np
+import pytest
+
+from conftest import golden
+import mnpbem_b200 as M
+from mnpbem_b200 import bem
+from mnpbem_b200.excitation import PlaneWaveRet
+from mnpbem_b200.mirror import ComParticleMirror, BEMRetMirror, PlaneWaveRetMirror
+
+pytestmark = pytest.mark.gpu
+
+DRUDE = M.EpsDrude(10.0, 9.065, 0.0708)
+POL = [[1.0, 0, 0], [0, 1.0, 0]]
+DIR = [[0, 0, 1.0], [0, 0, 1.0]]
+
+
+def rel(a, b):
+    a, b = np.asarray(a), np.asarray(b)
+    return np.abs(a - b).max() / np.abs(b).max()
+
+
+def mirror_particle(z, sym):
+    p = M.Particle(z[sym + '_verts2'], z[sym + '_faces2'], interp='flat')
+    return ComParticleMirror([M.EpsConst(1.0), DRUDE], [p], [[2, 1]], sym, (1,))
+
+
+@pytest.mark.parametrize('sym', ['x', 'xy'])
+def test_mirror_solve(gpu_ok, sym):
+    z = golden('golden_mirror')
+    cpm = mirror_particle(z, sym)
+    b = BEMRetMirror(cpm)
+    exc = PlaneWaveRetMirror(POL, DIR)
+    for i, lam in enumerate(z['lams']):
+        sig, _ = b.solve(exc.potential(cpm, float(lam)))
+        assert len(sig.val) == 2
+        for v, s in enumerate(sig.val):
+            pre = '%s_%d_%d_' % (sym, i, v)
+            assert np.array_equal(s.symval, z[pre + 'symval'])
+            for key in ('sig1', 'sig2', 'h1', 'h2'):
+                assert rel(getattr(s, key), z[pre + key]) < 1e-10, (sym, lam, v, key)
+        assert rel(exc.extinction(sig), z['%s_%d_ext' % (sym, i)]) < 1e-10
+        assert rel(exc.scattering(sig)[0], z['%s_%d_sca' % (sym, i)]) < 1e-10
+
+
+def test_mirror_equals_full_particle(gpu_ok):
+    z = golden('golden_mirror')
+    cpm = mirror_particle(z, 'xy')
+    exc_m = PlaneWaveRetMirror(POL, DIR)
+    exc = PlaneWaveRet(POL, DIR)
+    sig_m, _ = BEMRetMirror(cpm).solve(exc_m.potential(cpm, 550.0))
+    full, pf = exc_m.full(sig_m)
+    sig, _ = bem.BEMRet(pf).solve(exc.potential(pf, 550.0))
+    assert rel(full.sig2, sig.sig2) < 1e-9
+    assert rel(full.h2, sig.h2) < 1e-9
+    assert rel(exc_m.extinction(sig_m), exc.extinction(sig)) < 1e-9
