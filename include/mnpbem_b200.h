@@ -436,6 +436,58 @@ int mnpb_green_apply(void *stream, int64_t n, const double *pos, const double *n
                      int64_t m, const double *x, double *y);
 
 /* ---------------------------------------------------------------------------
+ * Mirror symmetry (FP64): the irreducible part (n faces) of a particle that
+ * its nk = 2 or 4 mirror images complete.  An "entry" is one wavelength and
+ * one symmetry value, entry e = b * nsym + s; matrices of an entry are
+ * `stride` complex elements apart, column-major with leading dimension ld.
+ * ------------------------------------------------------------------------- */
+
+/* out(b, s)[i, j] = sum_k tab[s * nk + k] full(b)[i, j + k n] for i, j < n:
+ * the Green function of symmetry value s from the full particle's matrix
+ * (ldf >= nk n, batch stride sf); tab (nsym x nk) is a host array.
+ * Replaces mnpbem/greenfun/compgreen_ret_mirror.py:36-95 (eval). */
+int mnpb_mirror_contract(void *stream, int64_t n, int64_t nk, int64_t nsym, int64_t batch,
+                         const double *full, int64_t ldf, int64_t sf, const double *tab,
+                         double *out, int64_t ld, int64_t stride);
+
+/* Workspace of mnpb_bemret_init_mirror_f64 in bytes. */
+int64_t mnpb_bemret_mirror_workspace(int64_t n, int64_t entries);
+/* Per entry: LU(G1), LU(G2) in place, H1 <- Sigma1 = H1 G1^-1, H2 <- Sigma2 =
+ * H2 G2^-1, Dinv = (Sigma1 - Sigma2)^-1.  piv: 3 x entries x n (G1, G2,
+ * Delta), info: 3 x entries.  G2 / H2 directly after G1 / H1 (entries x
+ * stride) run as one batch.  Replaces mnpbem/bem/bem_ret_mirror.py:182-328. */
+int mnpb_bemret_init_mirror_f64(void *stream, int64_t n, int64_t entries, double *G1,
+                                double *G2, double *H1, double *H2, int64_t ld, int64_t stride,
+                                double *Dinv, int32_t *piv, int32_t *info, void *work,
+                                int64_t work_bytes);
+/* For the symmetry-value rows (ix, iy, iz) of an excitation's x, y, z parts:
+ * S(b) = eps1 Sigma1_iz - eps2 Sigma2_iz + k^2 (eps1 - eps2)^2
+ *        sum_d n_d n_d^T o Dinv_{i_d}, then LU(S) (pivS: batch x n, info:
+ * batch).  H1, H2, Dinv as left by mnpb_bemret_init_mirror_f64; eps (batch x
+ * 4: eps1, eps2 complex), kvac (batch), nvec (n x 3) of the irreducible part.
+ * Replaces bem_ret_mirror.py:568-619 (_init_sigma_lu). */
+int mnpb_bemret_sigma_mirror_f64(void *stream, int64_t n, int64_t nsym, int64_t batch,
+                                 const double *H1, const double *H2, const double *Dinv,
+                                 int64_t ld, int64_t stride, const double *eps,
+                                 const double *kvac, const double *nvec, int32_t ix, int32_t iy,
+                                 int32_t iz, double *S, int64_t sS, int32_t *pivS, int32_t *info);
+/* Workspace of mnpb_bemret_solve_mirror_f64 in bytes. */
+int64_t mnpb_bemret_solve_mirror_workspace(int64_t n, int64_t batch, int64_t nrhs);
+/* BEMRet solve (layout of mnpb_bemret_solve_f64: x_in from
+ * mnpb_bemret_excitation, x_out = [sig1 | h1 | sig2 | h2]) with the matrices
+ * of component d (x, y, z) taken at symmetry row i_d and those of the scalar
+ * parts at iz; S, pivS from mnpb_bemret_sigma_mirror_f64 for the same rows.
+ * Replaces bem_ret_mirror.py:654-760 (solve). */
+int mnpb_bemret_solve_mirror_f64(void *stream, int64_t n, int64_t nsym, int64_t batch,
+                                 int64_t nrhs, const double *G1, const double *G2,
+                                 const double *H1, const double *Dinv, int64_t ld,
+                                 int64_t stride, const int32_t *piv, const double *S,
+                                 int64_t sS, const int32_t *pivS, int32_t ix, int32_t iy,
+                                 int32_t iz, const double *eps, const double *kvac,
+                                 const double *nvec, const double *x_in, double *x_out,
+                                 void *work, int64_t work_bytes);
+
+/* ---------------------------------------------------------------------------
  * Points off the surface: dipole excitations and point-face Green functions
  *
  * Media are 1-based indices into per-wavelength tables of nmed complex values
