@@ -249,7 +249,8 @@ struct HMats {
 // block in segments of at most a few hundred columns; one warp per item,
 // lane = factor column q (V is stored transposed: element (j, q) at
 // V[q + j * rank], so the lanes of one j read consecutive words), x in
-// cluster order read as a broadcast.  The item's partial t goes to
+// cluster order read as a broadcast.  Blocks of rank <= 16 put 2 or 4
+// columns in flight per warp (groups of 16 or 8 lanes).  The item's partial t goes to
 // TP + (offTP[block] + segment * rank) * NC; hm_vtx_reduce_kernel adds a
 // block's segments in order (deterministic).
 template <int NC>
@@ -268,6 +269,47 @@ __global__ void __launch_bounds__(256, 3) hm_vtx_kernel(HMats P, int n, int nc, 
     cd *out = H.TP + (H.offTP[b] + (int64_t)vi.w * r) * NC;
     const cd *xc = H.Xc + bk.z;
     constexpr int UN = 8;
+    if (r <= 16) {
+        // ranks up to 16 (most blocks): the warp splits into G groups of P
+        // lanes (lane = group * P + q) that take every G-th column, so most
+        // lanes work; the groups' sums are added in a fixed order at the end
+        const int P = r <= 8 ? 8 : 16, G = 32 / P;
+        const int g = l / P, q = l - g * P;
+        const bool live = q < r;
+        cd acc[NC];
+#pragma unroll
+        for (int c = 0; c < NC; ++c) acc[c] = cmk(0, 0);
+        constexpr int U4 = 4;
+        int j = vi.y + g;
+        for (; j + (U4 - 1) * G < vi.z; j += U4 * G) {
+            float2 v[U4];
+#pragma unroll
+            for (int u = 0; u < U4; ++u)
+                v[u] = live ? V[(int64_t)(j + u * G) * r + q] : make_float2(0.f, 0.f);
+#pragma unroll
+            for (int u = 0; u < U4; ++u)
+#pragma unroll
+                for (int c = 0; c < NC; ++c)
+                    if (c < nc)
+                        acc[c] = cfma(cmk(v[u].x, v[u].y), xc[(int64_t)c * n + j + u * G], acc[c]);
+        }
+        for (; j < vi.z; j += G) {
+            const float2 v = live ? V[(int64_t)j * r + q] : make_float2(0.f, 0.f);
+#pragma unroll
+            for (int c = 0; c < NC; ++c)
+                if (c < nc) acc[c] = cfma(cmk(v.x, v.y), xc[(int64_t)c * n + j], acc[c]);
+        }
+        for (int o = P; o < 32; o <<= 1)
+#pragma unroll
+            for (int c = 0; c < NC; ++c) {
+                acc[c].x += __shfl_xor_sync(0xffffffffu, acc[c].x, o);
+                acc[c].y += __shfl_xor_sync(0xffffffffu, acc[c].y, o);
+            }
+        if (g == 0 && live)
+#pragma unroll
+            for (int c = 0; c < NC; ++c) out[(int64_t)q * NC + c] = acc[c];
+        return;
+    }
     for (int q0 = 0; q0 < r; q0 += 32) {
         const int q = q0 + l;
         const bool live = q < r;
