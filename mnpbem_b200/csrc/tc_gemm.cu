@@ -180,6 +180,29 @@ struct Epi {
     int round_out;   // 1: store C rounded to nearest TF32
 };
 
+// Bulk prefetch of [p, p + bytes) into L2 (p 16-byte aligned, bytes a
+// multiple of 16); a hint only, nothing waits on it.
+__device__ __forceinline__ void prefetch_l2(const void *p, uint32_t bytes) {
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
+}
+
+// The C columns of a tile (rows m0.., BN columns from n0, both planes)
+// prefetched into L2 by the 128 epilogue threads, for an epilogue that
+// reads C (beta != 0): the loads then hit L2 instead of waiting on DRAM.
+__device__ __forceinline__ void prefetch_c_tile(const Epi &ep, int b, int m0, int n0, int bn,
+                                                int et) {
+    const int rows = min(128, ep.M - m0);
+    const uint32_t bytes = (uint32_t)(rows * 4) & ~15u;
+    if (bytes == 0) return;
+    const float *base = ep.C + (int64_t)b * ep.strideC + m0;
+    for (int c = et; c < 2 * bn; c += 128) {
+        const int col = n0 + (c >> 1);
+        if (col >= ep.N) continue;
+        const float *p = base + (int64_t)col * ep.ldc + ((c & 1) ? ep.planeC : 0);
+        if (((uintptr_t)p & 15) == 0) prefetch_l2(p, bytes);
+    }
+}
+
 __device__ __forceinline__ float rna_tf32(float v) {
     uint32_t t;
     asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(t) : "f"(v));
@@ -515,6 +538,12 @@ __global__ void __launch_bounds__(192, 1)
         int i = 0;
         for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++i) {
             const int buf = i & 1;
+            if (ep.beta != 0.f) {
+                // C of this tile into L2 while its main loop runs
+                const int pb = t / TPB, prem = t - pb * TPB;
+                const int pnt = prem / MT, pmt = prem - pnt * MT;
+                prefetch_c_tile(ep, pb, pmt * BM, pnt * BN, BN, q * 32 + lane);
+            }
             const bool acc_ok = mbar_wait(smem_u32(&bars[2 * STAGES + buf]), (i >> 1) & 1);
             if (!acc_ok) {
                 atomicCAS(&g_tc_error, 0, 3);
