@@ -178,6 +178,7 @@ struct Epi {
     float alpha, beta;
     int M, N, ktiles;
     int round_out;   // 1: store C rounded to nearest TF32
+    int prefetch_c;  // 1: the persistent kernel prefetches each tile's C into L2
 };
 
 // Bulk prefetch of [p, p + bytes) into L2 (p 16-byte aligned, bytes a
@@ -538,7 +539,7 @@ __global__ void __launch_bounds__(192, 1)
         int i = 0;
         for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++i) {
             const int buf = i & 1;
-            if (ep.beta != 0.f) {
+            if (ep.prefetch_c) {
                 // C of this tile into L2 while its main loop runs
                 const int pb = t / TPB, prem = t - pb * TPB;
                 const int pnt = prem / MT, pmt = prem - pnt * MT;
@@ -803,6 +804,7 @@ static std::atomic<int> g_cfg_bn{128}, g_cfg_persist{2}, g_cfg_stages{0};
 // two 128-column tiles) stream their tall A only once per tile column, where
 // the MN-major boxes reach about half the HBM rate of the packed layout.
 static std::atomic<int> g_cfg_mn_min_n{0};
+static std::atomic<int> g_cfg_prefetch{1};
 static std::atomic<int64_t> g_cfg_epoch{0};
 
 int64_t gemm_config_epoch() { return g_cfg_epoch.load(); }
@@ -875,7 +877,8 @@ int cgemm_tf32(cudaStream_t s, int M, int N, int K, int batch, float alpha, CMat
         return MNPB_EINVAL;
     }
     const int Mp = (M + BM - 1) / BM * BM, Kp = (K + BK - 1) / BK * BK;
-    Epi ep{C.p, C.ld, C.plane, C.stride, alpha, beta, M, N, Kp / BK, round_out ? 1 : 0};
+    Epi ep{C.p, C.ld, C.plane, C.stride, alpha, beta, M, N, Kp / BK, round_out ? 1 : 0,
+           (beta != 0.f && g_cfg_prefetch.load(std::memory_order_relaxed)) ? 1 : 0};
     // narrow products of the 128-wide tile (96 < N < mn_min_n) pack A even when it
     // could be read in place; the 32/64-wide tiles and wide products read it in place
     const bool pack_narrow = N > 64 && N < g_cfg_mn_min_n.load(std::memory_order_relaxed) &&
@@ -977,6 +980,14 @@ extern "C" int mnpb_gemm_config_mn(int32_t mn_min_n) {
     clear_error();
     MNPB_REQUIRE(mn_min_n >= 0, "gemm_config_mn: mn_min_n must be >= 0");
     tc::g_cfg_mn_min_n.store(mn_min_n);
+    tc::g_cfg_epoch.fetch_add(1);
+    return MNPB_OK;
+}
+
+extern "C" int mnpb_gemm_config_prefetch(int32_t on) {
+    clear_error();
+    MNPB_REQUIRE(on == 0 || on == 1, "gemm_config_prefetch: on must be 0 or 1");
+    tc::g_cfg_prefetch.store(on);
     tc::g_cfg_epoch.fetch_add(1);
     return MNPB_OK;
 }

@@ -4,7 +4,11 @@ and against this package's own full-particle solve.
 
 Tolerances, max-norm relative: surface charges and currents of every
 symmetry component 1e-10, cross sections 1e-10 (FP64 throughout); the
-mirror decomposition against the full-particle BEMRet 1e-9."""
+mirror decomposition against the full-particle BEMRet 1e-5: a flipped
+face's quadrature points are not the mirror images of the original face's
+(the face rule is not symmetric under the reversed vertex order; up to
+0.37 nm apart on this mesh), so the full particle's refined matrices are
+mirror-symmetric only to the quadrature error (~2e-6 measured)."""
 import numpy as np
 import pytest
 
@@ -57,6 +61,6 @@ def test_mirror_equals_full_particle(gpu_ok):
     sig_m, _ = BEMRetMirror(cpm).solve(exc_m.potential(cpm, 550.0))
     full, pf = exc_m.full(sig_m)
     sig, _ = bem.BEMRet(pf).solve(exc.potential(pf, 550.0))
-    assert rel(full.sig2, sig.sig2) < 1e-9
-    assert rel(full.h2, sig.h2) < 1e-9
-    assert rel(exc_m.extinction(sig_m), exc.extinction(sig)) < 1e-9
+    assert rel(full.sig2, sig.sig2) < 1e-5
+    assert rel(full.h2, sig.h2) < 1e-5
+    assert rel(exc_m.extinction(sig_m), exc.extinction(sig)) < 1e-5
