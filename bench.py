@@ -79,9 +79,6 @@ def parse():
     ap.add_argument('--mn-min-n', type=int, default=None,
                     help='GEMM knob: TF32 A operands of products with 64 < N < this are '
                          'packed instead of read in place (library default 0: never)')
-    ap.add_argument('--gemm-prefetch', type=int, default=None,
-                    help='GEMM knob: L2 prefetch of C in the persistent kernel when beta != 0 '
-                         '(library default 1)')
     ap.add_argument('--fp64-steps', type=int, default=None,
                     help='timed sweeps of the plain FP64 GPU path (default: --steps)')
     return ap.parse_args()
@@ -529,8 +526,6 @@ def main():
     from mnpbem_b200 import _lib, bem, excitation
     if args.mn_min_n is not None:
         _lib.call('mnpb_gemm_config_mn', int(args.mn_min_n))
-    if args.gemm_prefetch is not None:
-        _lib.call('mnpb_gemm_config_prefetch', int(args.gemm_prefetch))
 
     v, f = M.load_mesh('trisphere_1444_40')
     s = M.Particle(v, f, interp='curv')

@@ -343,10 +343,6 @@ int mnpb_gemm_config(int32_t bn_wide, int32_t persist_tiles_per_sm, int32_t stag
  * Default 0: always in place (over the 2884-face, 81-wavelength sweep the
  * packing costs more than the in-place reads lose). */
 int mnpb_gemm_config_mn(int32_t mn_min_n);
-/* 1 (default): when beta != 0 the persistent GEMM prefetches each tile's C
- * columns into L2 (cp.async.bulk.prefetch) while the tile's main loop runs,
- * so the epilogue's reads of C hit L2; 0: no prefetch. */
-int mnpb_gemm_config_prefetch(int32_t on);
 
 /* Same GEMM as mnpb_cgemm_tf32, but it allocates nothing and takes no
  * workspace: the packed TF32 copy of A goes into a fixed 64 MiB array of the

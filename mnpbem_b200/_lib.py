@@ -63,7 +63,6 @@ SIGNATURES = {
     'mnpb_tc_error': [_P, _P],
     'mnpb_gemm_config': [C.c_int32, C.c_int32, C.c_int32],
     'mnpb_gemm_config_mn': [C.c_int32],
-    'mnpb_gemm_config_prefetch': [C.c_int32],
     'mnpb_wait_probe': [_P, C.c_int32, _I64, _P],
     'mnpb_hmat_aca': [_P, _I64, _P, _I64, _P, _I64, _P, _P, _P, _I64, _I64, _D, _P, _P],
     'mnpb_hmat_gather_dense': [_P, _P, _I64, _P, _I64, _P, _P, _P],

@@ -178,31 +178,7 @@ struct Epi {
     float alpha, beta;
     int M, N, ktiles;
     int round_out;   // 1: store C rounded to nearest TF32
-    int prefetch_c;  // 1: the persistent kernel prefetches each tile's C into L2
 };
-
-// Bulk prefetch of [p, p + bytes) into L2 (p 16-byte aligned, bytes a
-// multiple of 16); a hint only, nothing waits on it.
-__device__ __forceinline__ void prefetch_l2(const void *p, uint32_t bytes) {
-    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
-}
-
-// The C columns of a tile (rows m0.., BN columns from n0, both planes)
-// prefetched into L2 by the 128 epilogue threads, for an epilogue that
-// reads C (beta != 0): the loads then hit L2 instead of waiting on DRAM.
-__device__ __forceinline__ void prefetch_c_tile(const Epi &ep, int b, int m0, int n0, int bn,
-                                                int et) {
-    const int rows = min(128, ep.M - m0);
-    const uint32_t bytes = (uint32_t)(rows * 4) & ~15u;
-    if (bytes == 0) return;
-    const float *base = ep.C + (int64_t)b * ep.strideC + m0;
-    for (int c = et; c < 2 * bn; c += 128) {
-        const int col = n0 + (c >> 1);
-        if (col >= ep.N) continue;
-        const float *p = base + (int64_t)col * ep.ldc + ((c & 1) ? ep.planeC : 0);
-        if (((uintptr_t)p & 15) == 0) prefetch_l2(p, bytes);
-    }
-}
 
 __device__ __forceinline__ float rna_tf32(float v) {
     uint32_t t;
@@ -539,12 +515,6 @@ __global__ void __launch_bounds__(192, 1)
         int i = 0;
         for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++i) {
             const int buf = i & 1;
-            if (ep.prefetch_c) {
-                // C of this tile into L2 while its main loop runs
-                const int pb = t / TPB, prem = t - pb * TPB;
-                const int pnt = prem / MT, pmt = prem - pnt * MT;
-                prefetch_c_tile(ep, pb, pmt * BM, pnt * BN, BN, q * 32 + lane);
-            }
             const bool acc_ok = mbar_wait(smem_u32(&bars[2 * STAGES + buf]), (i >> 1) & 1);
             if (!acc_ok) {
                 atomicCAS(&g_tc_error, 0, 3);
@@ -804,7 +774,6 @@ static std::atomic<int> g_cfg_bn{128}, g_cfg_persist{2}, g_cfg_stages{0};
 // two 128-column tiles) stream their tall A only once per tile column, where
 // the MN-major boxes reach about half the HBM rate of the packed layout.
 static std::atomic<int> g_cfg_mn_min_n{0};
-static std::atomic<int> g_cfg_prefetch{1};
 static std::atomic<int64_t> g_cfg_epoch{0};
 
 int64_t gemm_config_epoch() { return g_cfg_epoch.load(); }
@@ -877,8 +846,7 @@ int cgemm_tf32(cudaStream_t s, int M, int N, int K, int batch, float alpha, CMat
         return MNPB_EINVAL;
     }
     const int Mp = (M + BM - 1) / BM * BM, Kp = (K + BK - 1) / BK * BK;
-    Epi ep{C.p, C.ld, C.plane, C.stride, alpha, beta, M, N, Kp / BK, round_out ? 1 : 0,
-           (beta != 0.f && g_cfg_prefetch.load(std::memory_order_relaxed)) ? 1 : 0};
+    Epi ep{C.p, C.ld, C.plane, C.stride, alpha, beta, M, N, Kp / BK, round_out ? 1 : 0};
     // narrow products of the 128-wide tile (96 < N < mn_min_n) pack A even when it
     // could be read in place; the 32/64-wide tiles and wide products read it in place
     const bool pack_narrow = N > 64 && N < g_cfg_mn_min_n.load(std::memory_order_relaxed) &&
@@ -980,14 +948,6 @@ extern "C" int mnpb_gemm_config_mn(int32_t mn_min_n) {
     clear_error();
     MNPB_REQUIRE(mn_min_n >= 0, "gemm_config_mn: mn_min_n must be >= 0");
     tc::g_cfg_mn_min_n.store(mn_min_n);
-    tc::g_cfg_epoch.fetch_add(1);
-    return MNPB_OK;
-}
-
-extern "C" int mnpb_gemm_config_prefetch(int32_t on) {
-    clear_error();
-    MNPB_REQUIRE(on == 0 || on == 1, "gemm_config_prefetch: on must be 0 or 1");
-    tc::g_cfg_prefetch.store(on);
     tc::g_cfg_epoch.fetch_add(1);
     return MNPB_OK;
 }
