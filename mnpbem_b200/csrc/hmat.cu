@@ -378,20 +378,34 @@ template <int NC, int UN>
 __device__ __forceinline__ void rows_accumulate(const float2 *__restrict__ A, int64_t lda, int cnt,
                                                 const cd *__restrict__ B, int64_t bj, int64_t bc,
                                                 bool live, cd (&acc)[NC]) {
-    // acc += sum_j A[j * lda] * B[j * bj + c * bc]   (A per lane, B broadcast)
-    int j = 0;
-    for (; j + UN <= cnt; j += UN) {
+    // acc += sum_j A[j * lda] * B[j * bj + c * bc]   (A per lane, B broadcast).
+    // Software-pipelined: the loads of the next UN columns of A are issued
+    // before the current UN columns are multiplied, so two chunks of the
+    // matrix stream are in flight per lane.
+    const int full = cnt / UN;
+    if (full > 0) {
         float2 a[UN];
 #pragma unroll
-        for (int u = 0; u < UN; ++u) a[u] = live ? A[(int64_t)(j + u) * lda] : make_float2(0.f, 0.f);
+        for (int u = 0; u < UN; ++u) a[u] = live ? A[(int64_t)u * lda] : make_float2(0.f, 0.f);
+        for (int ch = 0; ch < full; ++ch) {
+            const int j = ch * UN;
+            const bool more = ch + 1 < full;
+            float2 nx[UN];
 #pragma unroll
-        for (int u = 0; u < UN; ++u) {
-            const cd av = cmk(a[u].x, a[u].y);
+            for (int u = 0; u < UN; ++u)
+                nx[u] = (live && more) ? A[(int64_t)(j + UN + u) * lda] : make_float2(0.f, 0.f);
 #pragma unroll
-            for (int c = 0; c < NC; ++c) acc[c] = cfma(av, B[(int64_t)(j + u) * bj + c * bc], acc[c]);
+            for (int u = 0; u < UN; ++u) {
+                const cd av = cmk(a[u].x, a[u].y);
+#pragma unroll
+                for (int c = 0; c < NC; ++c)
+                    acc[c] = cfma(av, B[(int64_t)(j + u) * bj + c * bc], acc[c]);
+            }
+#pragma unroll
+            for (int u = 0; u < UN; ++u) a[u] = nx[u];
         }
     }
-    for (; j < cnt; ++j) {
+    for (int j = full * UN; j < cnt; ++j) {
         const float2 a = live ? A[(int64_t)j * lda] : make_float2(0.f, 0.f);
         const cd av = cmk(a.x, a.y);
 #pragma unroll
@@ -399,8 +413,16 @@ __device__ __forceinline__ void rows_accumulate(const float2 *__restrict__ A, in
     }
 }
 
+// Launch-bound occupancy and software-pipelining width of the row sums.
+#ifndef HM_ROWS_MINB
+#define HM_ROWS_MINB 2
+#endif
+#ifndef HM_ROWS_UN
+#define HM_ROWS_UN 8
+#endif
+
 template <int NC>
-__global__ void __launch_bounds__(256, 3) hm_rows_kernel(HMats P, int n, int nitem,
+__global__ void __launch_bounds__(256, HM_ROWS_MINB) hm_rows_kernel(HMats P, int n, int nitem,
                                                          const int4 *__restrict__ items,
                                                          const int2 *__restrict__ chunks,
                                                          const int2 *__restrict__ leaf_rows,
@@ -424,12 +446,12 @@ __global__ void __launch_bounds__(256, 3) hm_rows_kernel(HMats P, int n, int nit
         const int id = lent[e];
         if (id >= 0) {
             const int4 bk = dn[id];
-            rows_accumulate<NC, 8>(H.D + H.offD[id] + (row - bk.x), bk.y, bk.w, H.Xc + bk.z, 1, n,
+            rows_accumulate<NC, HM_ROWS_UN>(H.D + H.offD[id] + (row - bk.x), bk.y, bk.w, H.Xc + bk.z, 1, n,
                                    live, acc);
         } else {
             const int b = -id - 1;
             const int4 bk = lr[b];
-            rows_accumulate<NC, 8>(H.U + H.offU[b] + (row - bk.x), bk.y, H.rank[b],
+            rows_accumulate<NC, HM_ROWS_UN>(H.U + H.offU[b] + (row - bk.x), bk.y, H.rank[b],
                                    H.T + H.offT[b] * NC, NC, 1, live, acc);
         }
     }
