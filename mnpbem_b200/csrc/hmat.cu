@@ -415,10 +415,10 @@ __device__ __forceinline__ void rows_accumulate(const float2 *__restrict__ A, in
 
 // Launch-bound occupancy and software-pipelining width of the row sums.
 #ifndef HM_ROWS_MINB
-#define HM_ROWS_MINB 2
+#define HM_ROWS_MINB 3
 #endif
 #ifndef HM_ROWS_UN
-#define HM_ROWS_UN 8
+#define HM_ROWS_UN 4
 #endif
 
 template <int NC>
