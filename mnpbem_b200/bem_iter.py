@@ -404,7 +404,7 @@ class BEMRetIter(object):
         the quadratic extrapolation).  The first wavelengths fall back to the
         previous solution / linear extrapolation until the history is long
         enough.  ``deflate``: False, or the number m of previous solutions
-        (True: 6) that, with the start vector, span the GCRO augmentation
+        (True: 3) that, with the start vector, span the GCRO augmentation
         space of each solve (``gmres(augment=...)``): GMRES then minimises the
         residual over that span and the Krylov space of the operator
         deflated by it.  Returns (list of CompStruct, list of per-wavelength
@@ -435,7 +435,7 @@ class BEMRetIter(object):
                     raise ValueError("solve_spectrum: unknown warm start {!r}".format(warm))
             aug = None
             if deflate and i >= 1:
-                m = 6 if deflate is True else int(deflate)
+                m = 3 if deflate is True else int(deflate)
                 aug = ([x0] if x0 is not None else []) + xs[max(0, i - m):i]
                 x0 = None
             M = (lambda v: self._apply_precond(v, K)) if self._pre is not None else None
