@@ -1331,6 +1331,76 @@ __global__ void set_identity_kernel(float *W, int64_t ldw, int64_t plane, int64_
 
 }  // namespace
 
+// Same product with four rows per thread and 16-byte loads (A's leading
+// dimension, planes and batch stride multiples of 4 floats, A 16-byte
+// aligned, m a multiple of 4): one vector load per plane brings four rows,
+// so a thread keeps more of the matrix stream in flight per instruction.
+template <int NC>
+__global__ void __launch_bounds__(128) skinny4_kernel(int m, int n, int k, float alpha,
+                                                      const float *__restrict__ A, int64_t lda,
+                                                      int64_t planeA, int64_t sA,
+                                                      const float *__restrict__ B, int64_t ldb,
+                                                      int64_t planeB, int64_t sB, float beta,
+                                                      float *__restrict__ C, int64_t ldc,
+                                                      int64_t planeC, int64_t sC, int rnd) {
+    __shared__ cf Bs[SK_KT][NC];
+    const int64_t b = blockIdx.y;
+    A += b * sA;
+    B += b * sB;
+    C += b * sC;
+    const int row = 4 * (blockIdx.x * blockDim.x + threadIdx.x);
+    cf acc[4][NC];
+#pragma unroll
+    for (int r = 0; r < 4; ++r)
+#pragma unroll
+        for (int j = 0; j < NC; ++j) acc[r][j] = fmk(0.f, 0.f);
+    for (int k0 = 0; k0 < k; k0 += SK_KT) {
+        __syncthreads();
+        for (int e = threadIdx.x; e < SK_KT * NC; e += blockDim.x) {
+            const int kk = e % SK_KT, j = e / SK_KT;
+            Bs[kk][j] = (k0 + kk < k && j < n) ? ld(B, planeB, (int64_t)j * ldb + k0 + kk)
+                                               : fmk(0.f, 0.f);
+        }
+        __syncthreads();
+        if (row < m) {
+            const int kend = min(SK_KT, k - k0);
+            const float *ar = A + (int64_t)k0 * lda + row;
+#pragma unroll 4
+            for (int kk = 0; kk < kend; ++kk) {
+                const float4 re = __ldg(reinterpret_cast<const float4 *>(ar + (int64_t)kk * lda));
+                const float4 im =
+                    __ldg(reinterpret_cast<const float4 *>(ar + (int64_t)kk * lda + planeA));
+                const float ar4[4] = {re.x, re.y, re.z, re.w}, ai4[4] = {im.x, im.y, im.z, im.w};
+#pragma unroll
+                for (int j = 0; j < NC; ++j) {
+                    const cf bv = Bs[kk][j];
+#pragma unroll
+                    for (int r = 0; r < 4; ++r) {
+                        acc[r][j].x = fmaf(ar4[r], bv.x, acc[r][j].x);
+                        acc[r][j].x = fmaf(-ai4[r], bv.y, acc[r][j].x);
+                        acc[r][j].y = fmaf(ar4[r], bv.y, acc[r][j].y);
+                        acc[r][j].y = fmaf(ai4[r], bv.x, acc[r][j].y);
+                    }
+                }
+            }
+        }
+    }
+    if (row >= m) return;
+#pragma unroll
+    for (int j = 0; j < NC; ++j) {
+        if (j < n) {
+#pragma unroll
+            for (int r = 0; r < 4; ++r) {
+                const int64_t o = (int64_t)j * ldc + row + r;
+                cf c = beta != 0.f ? ld(C, planeC, o) : fmk(0.f, 0.f);
+                cf v = fmk(alpha * acc[r][j].x + beta * c.x, alpha * acc[r][j].y + beta * c.y);
+                if (rnd) v = fmk(tf32_rna(v.x), tf32_rna(v.y));
+                st(C, planeC, o, v);
+            }
+        }
+    }
+}
+
 // ---------------------------------------------------------------------------
 // host orchestration
 // ---------------------------------------------------------------------------
@@ -1344,6 +1414,23 @@ int gemm(Ctx &c, int m, int n, int k, float alpha, CMatF A, CMatF B, float beta,
         if (beta == 1.f) return MNPB_OK;
         set_error("f32 gemm: k = 0 with beta != 1 is not supported");
         return MNPB_EINVAL;
+    }
+    const bool vec4 = n <= 4 && m % 4 == 0 && A.ld % 4 == 0 && A.plane % 4 == 0 &&
+                      A.stride % 4 == 0 && ((uintptr_t)A.p & 15) == 0;
+    if (vec4) {
+        dim3 grid(ceil_div(m, 512), c.batch);
+        ProfScope ps(c.s, PC_SGEMM, 8.0 * (double)m * k * c.batch);   // bytes of A streamed
+        prof_tag("M=%d N=%d K=%d B=%d v4", m, n, k, c.batch);
+#define MNPB_SKINNY4(NC)                                                                        \
+    skinny4_kernel<NC><<<grid, 128, 0, c.s>>>(m, n, k, alpha, A.p, A.ld, A.plane, A.stride,   \
+                                              B.p, B.ld, B.plane, B.stride, beta, C.p, C.ld,  \
+                                              C.plane, C.stride, round_out ? 1 : 0)
+        if (n <= 1) MNPB_SKINNY4(1);
+        else if (n <= 2) MNPB_SKINNY4(2);
+        else MNPB_SKINNY4(4);
+#undef MNPB_SKINNY4
+        MNPB_LAUNCH_CHECK("skinny4_kernel");
+        return MNPB_OK;
     }
     if (n <= SK_N) {
         dim3 grid(ceil_div(m, 128), c.batch);
@@ -1415,14 +1502,21 @@ static int split_tl(int n) {
     return h < TL ? TL : h;
 }
 
+// `fresh`: B still holds the caller's right-hand side (not TF32); otherwise
+// every update that wrote it stored its output rounded to nearest TF32, so a
+// leaf reads it as an exact tensor-core operand without a rounding pass.
 static int trsm_rec(Ctx &c, int mode, int n, int m, CMatF T, CMatF B, const InvSet *iv,
-                    int blk0) {
+                    int blk0, bool fresh = true) {
     if (!iv && n <= TS) return trsm_small(c, mode, n, T, B, m);
     if (iv && n <= TL) {
         const CMatF I = inv_block(*iv, blk0);
-        // right leaf: A is the not-yet-rounded right-hand side, packed with rounding
-        if (mode >= 2) return gemm(c, m, n, n, 1.f, B, I, 0.f, B, true);
-        {
+        if (mode >= 2) {
+            // right leaf: A is the right-hand-side block; packed with rounding
+            // while fresh, read in place once the updates have rounded it
+            if (fresh) return gemm(c, m, n, n, 1.f, B, I, 0.f, B, true);
+            return gemm(c, m, n, n, 1.f, B, I, 0.f, B, true, true);
+        }
+        if (fresh) {
             ProfScope ps(c.s, PC_PACK, 16.0 * (double)n * m * c.batch);   // bytes read + written
             prof_tag("round n=%d m=%d B=%d", n, m, c.batch);
             round_tf32_kernel<<<dim3(ceil_div(m, RT_COLS), c.batch), TL, 0, c.s>>>(
@@ -1435,24 +1529,27 @@ static int trsm_rec(Ctx &c, int mode, int n, int m, CMatF T, CMatF B, const InvS
     const int blk1 = blk0 + n1 / TL;
     // the A operand of every update is TF32 already: a factor block (stored
     // rounded by the LU) or right-hand-side rows a leaf has finished (stored
-    // rounded), so the tensor cores read it in place
+    // rounded), so the tensor cores read it in place.  With the block
+    // inverses (iv) the updates store their output rounded to TF32 as well,
+    // for the leaves that read it next.
+    const bool rnd = iv != nullptr;
     switch (mode) {
     case 0:
-        MNPB_TRY(trsm_rec(c, 0, n1, m, T, B, iv, blk0));
-        MNPB_TRY(gemm(c, n - n1, m, n1, -1.f, T.sub(n1, 0), B, 1.f, B.sub(n1, 0), false, true));
-        return trsm_rec(c, 0, n - n1, m, T.sub(n1, n1), B.sub(n1, 0), iv, blk1);
+        MNPB_TRY(trsm_rec(c, 0, n1, m, T, B, iv, blk0, fresh));
+        MNPB_TRY(gemm(c, n - n1, m, n1, -1.f, T.sub(n1, 0), B, 1.f, B.sub(n1, 0), rnd, true));
+        return trsm_rec(c, 0, n - n1, m, T.sub(n1, n1), B.sub(n1, 0), iv, blk1, fresh && !rnd);
     case 1:
-        MNPB_TRY(trsm_rec(c, 1, n - n1, m, T.sub(n1, n1), B.sub(n1, 0), iv, blk1));
-        MNPB_TRY(gemm(c, n1, m, n - n1, -1.f, T.sub(0, n1), B.sub(n1, 0), 1.f, B, false, true));
-        return trsm_rec(c, 1, n1, m, T, B, iv, blk0);
+        MNPB_TRY(trsm_rec(c, 1, n - n1, m, T.sub(n1, n1), B.sub(n1, 0), iv, blk1, fresh));
+        MNPB_TRY(gemm(c, n1, m, n - n1, -1.f, T.sub(0, n1), B.sub(n1, 0), 1.f, B, rnd, true));
+        return trsm_rec(c, 1, n1, m, T, B, iv, blk0, fresh && !rnd);
     case 2:
-        MNPB_TRY(trsm_rec(c, 2, n1, m, T, B, iv, blk0));
-        MNPB_TRY(gemm(c, m, n - n1, n1, -1.f, B, T.sub(0, n1), 1.f, B.sub(0, n1), false, true));
-        return trsm_rec(c, 2, n - n1, m, T.sub(n1, n1), B.sub(0, n1), iv, blk1);
+        MNPB_TRY(trsm_rec(c, 2, n1, m, T, B, iv, blk0, fresh));
+        MNPB_TRY(gemm(c, m, n - n1, n1, -1.f, B, T.sub(0, n1), 1.f, B.sub(0, n1), rnd, true));
+        return trsm_rec(c, 2, n - n1, m, T.sub(n1, n1), B.sub(0, n1), iv, blk1, fresh && !rnd);
     default:
-        MNPB_TRY(trsm_rec(c, 3, n - n1, m, T.sub(n1, n1), B.sub(0, n1), iv, blk1));
-        MNPB_TRY(gemm(c, m, n1, n - n1, -1.f, B.sub(0, n1), T.sub(n1, 0), 1.f, B, false, true));
-        return trsm_rec(c, 3, n1, m, T, B, iv, blk0);
+        MNPB_TRY(trsm_rec(c, 3, n - n1, m, T.sub(n1, n1), B.sub(0, n1), iv, blk1, fresh));
+        MNPB_TRY(gemm(c, m, n1, n - n1, -1.f, B.sub(0, n1), T.sub(n1, 0), 1.f, B, rnd, true));
+        return trsm_rec(c, 3, n1, m, T, B, iv, blk0, fresh && !rnd);
     }
 }
 
@@ -1516,8 +1613,8 @@ static int trsm_llu_eye_rec(Ctx &c, int n, CMatF T, CMatF X, const InvSet &iv, i
     const int n1 = split_tl(n);
     const int blk1 = blk0 + n1 / TL;
     MNPB_TRY(trsm_llu_eye_rec(c, n1, T, X, iv, blk0));
-    MNPB_TRY(gemm(c, n - n1, n1, n1, -1.f, T.sub(n1, 0), X, 0.f, X.sub(n1, 0), false, true));
-    MNPB_TRY(trsm_rec(c, 0, n - n1, n1, T.sub(n1, n1), X.sub(n1, 0), &iv, blk1));
+    MNPB_TRY(gemm(c, n - n1, n1, n1, -1.f, T.sub(n1, 0), X, 0.f, X.sub(n1, 0), true, true));
+    MNPB_TRY(trsm_rec(c, 0, n - n1, n1, T.sub(n1, n1), X.sub(n1, 0), &iv, blk1, false));
     return trsm_llu_eye_rec(c, n - n1, T.sub(n1, n1), X.sub(n1, n1), iv, blk1);
 }
 
