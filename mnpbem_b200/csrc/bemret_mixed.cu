@@ -78,26 +78,6 @@ __global__ void to_f32p(int n, int m, const cd *X, int64_t sx, float *Y, int64_t
     y[e] = (float)v.x;
     y[e + (int64_t)n * m] = (float)v.y;
 }
-// The same conversions for the G1 and G2 parts of a solution in one launch:
-// entry b < Bh is X + b sx, entry b >= Bh is X + (b - Bh) sx + off2.
-__global__ void to_f32p2(int n, int m, const cd *X, int64_t sx, int64_t off2, int Bh, float *Y,
-                         int64_t sy) {
-    const int64_t b = blockIdx.y;
-    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (e >= (int64_t)n * m) return;
-    const cd v = X[(b % Bh) * sx + (b / Bh) * off2 + e];
-    float *y = Y + b * sy;
-    y[e] = (float)v.x;
-    y[e + (int64_t)n * m] = (float)v.y;
-}
-__global__ void from_f32p2(int n, int m, const float *Y, int64_t sy, cd *X, int64_t sx,
-                           int64_t off2, int Bh) {
-    const int64_t b = blockIdx.y;
-    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (e >= (int64_t)n * m) return;
-    const float *y = Y + b * sy;
-    X[(b % Bh) * sx + (b / Bh) * off2 + e] = cmk((double)y[e], (double)y[e + (int64_t)n * m]);
-}
 __global__ void from_f32p(int n, int m, const float *Y, int64_t sy, cd *X, int64_t sx) {
     const int64_t b = blockIdx.y;
     const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -245,7 +225,6 @@ struct Factors {
     const float *iG1L, *iG1U, *iG2L, *iG2U, *iSL, *iSU;   // diagonal-block inverses
     int64_t n, dinv_per;                            // dinv_per: floats per entry
     int *trsv_state;      // flags + ticket of the one-launch triangular solves
-    bool trsv_pairs;      // trsv_state covers twice the batch (G1 and G2 solved together)
     // the same factors for batch entries b0, b0 + 1, ...
     Factors at(int b0) const {
         Factors f = *this;
@@ -344,30 +323,6 @@ static int msolve(f32::Ctx &c, int n, int K, const Factors &F, const double *eps
     MNPB_TRY(mgemm(c, n, 3 * K, F.D, F, AP, sAP, V, sAP, t1, t2));
     solve_out_kernel<<<g, 128, 0, s>>>(n, K, xin, sx, R, sR, V, sAP, xout, sx);
     MNPB_LAUNCH_CHECK("solve_out_kernel");
-    // G1 and G2 factors (pivots, diagonal-block inverses) stored back to back:
-    // both pairs of triangular solves as one launch sequence over 2 B entries,
-    // twice the CTAs of the one-CTA-per-matrix streamed solve
-    const bool pair = F.G2 == F.G1 + (int64_t)B * F.stride &&
-                      F.pivG2 == F.pivG1 + (int64_t)B * nn &&
-                      F.iG2L == F.iG1L + (int64_t)B * F.dinv_per &&
-                      F.iG2U == F.iG1U + (int64_t)B * F.dinv_per && F.trsv_pairs;
-    if (pair) {
-        const int m = 4 * K;
-        const int64_t pl = nn * m;
-        dim3 g2(ceil_div(pl, 256), 2 * B);
-        {
-            ProfScope ps(s, PC_REFINE_EW, 0.0);
-            to_f32p2<<<g2, 256, 0, s>>>(n, m, xout, sx, 4 * K * nn, B, t1, 2 * pl);
-            MNPB_LAUNCH_CHECK("to_f32p2");
-        }
-        f32::Ctx c2(s, 2 * B, c.work, c.work_bytes);
-        MNPB_TRY(f32::getrs_few(c2, n, m, CMatF{F.G1, F.ld, F.plane, F.stride}, F.pivG1, nn,
-                                F.iG1L, F.iG1U, CMatF{t1, n, pl, 2 * pl}, F.trsv_state));
-        ProfScope ps(s, PC_REFINE_EW, 0.0);
-        from_f32p2<<<g2, 256, 0, s>>>(n, m, t1, 2 * pl, xout, sx, 4 * K * nn, B);
-        MNPB_LAUNCH_CHECK("from_f32p2");
-        return MNPB_OK;
-    }
     MNPB_TRY(mgetrs(c, n, 4 * K, F.G1, F, F.pivG1, F.iG1L, F.iG1U, xout, sx, t1));
     return mgetrs(c, n, 4 * K, F.G2, F, F.pivG2, F.iG2L, F.iG2U, xout + 4 * K * nn, sx, t1);
 }
@@ -569,7 +524,7 @@ extern "C" int64_t mnpb_bemret_refine_workspace(int64_t n, int64_t batch, int64_
     const int64_t K = nrhs;
     // msolve scratch (15 K n c128 + 2 x 16 K n float... per entry) + r, d, P1..Q2 + norms
     return batch * n * K * (15 * 16 + 2 * 16 * 8 + 2 * 8 * 16 + 4 * 4 * 16) + 8 * 256 +
-           align_up(f32::trsv_state_bytes((int)n, 2 * (int)batch), 256) +
+           align_up(f32::trsv_state_bytes((int)n, (int)batch), 256) +
            align_up(tc::cgemm_tf32_workspace((int)n, 64, (int)batch), 256);
 }
 
@@ -603,7 +558,7 @@ extern "C" int mnpb_bemret_solve_refine(
     Factors F{(float *)G1p, (float *)G2p, (float *)S1p, (float *)Sp, (float *)Dp, ld, plane,
               2 * plane, piv, piv + Bn, piv + 2 * Bn, dinv + dv.gL(0, batch),
               dinv + dv.gU(0, batch), dinv + dv.gL(1, batch), dinv + dv.gU(1, batch),
-              dinv + dv.sL(batch), dinv + dv.sU(batch), n, dv.S, nullptr, false};
+              dinv + dv.sL(batch), dinv + dv.sU(batch), n, dv.S, nullptr};
     const int64_t per = n * K;
     char *wp = (char *)work;
     auto take = [&](int64_t bytes) {
@@ -617,8 +572,7 @@ extern "C" int mnpb_bemret_solve_refine(
     cd *dx = (cd *)take(batch * per * 8 * 16);
     cd *P = (cd *)take(batch * per * 4 * 4 * 16);
     double *nrm = (double *)take(batch * 4 * 8);
-    F.trsv_state = (int *)take(f32::trsv_state_bytes(N, 2 * B));
-    F.trsv_pairs = true;
+    F.trsv_state = (int *)take(f32::trsv_state_bytes(N, B));
     const int64_t tcw = (int64_t)((char *)work + work_bytes - wp);
     f32::Ctx c(s, B, (float *)wp, tcw);
     const int64_t sx = per * 8, sP4 = per * 4;
