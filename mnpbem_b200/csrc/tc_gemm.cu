@@ -26,6 +26,8 @@ namespace mnpb {
 namespace tc {
 
 constexpr int BM = 128, BK = 32;   // BK: TF32 elements per 128-byte row
+// persistent kernel: warp 0 TMA producer, warp 1 MMA issuer, warps 2..9 epilogue
+constexpr int EPI_THREADS = 256, PERSIST_THREADS = 64 + EPI_THREADS;
 constexpr int MAX_STAGES = 4;
 constexpr int TILE_A_BYTES = BM * BK * 4;   // 16 KB
 template <int BN> struct Tile {
@@ -365,13 +367,15 @@ __device__ __forceinline__ void mbar_arrive(uint32_t bar) {
 // (t = blockIdx.x, blockIdx.x + gridDim.x, ...; M fastest, then N, then the
 // batch).  Warp 0 issues the TMA loads of a stage ring that runs on across
 // tiles, warp 1 allocates all 512 TMEM columns and issues the MMAs into two
-// accumulator buffers (re + im, 2 x BN columns each), warps 2-5 drain a
-// finished buffer into C (warp w owns TMEM lanes 32 (w % 4) ..) while the MMAs
-// of the next tile fill the other one.  acc_full[b] (MMA -> epilogue, one
-// commit) and acc_empty[b] (epilogue -> MMA, 128 arrivals) hand the buffers
-// over.  Every wait is bounded as in cgemm_tf32_kernel.
+// accumulator buffers (re + im, 2 x BN columns each), warps 2-9 drain a
+// finished buffer into C (warp w owns TMEM lanes 32 (w % 4) .., two warps per
+// lane quadrant on alternate column chunks, so twice the C traffic is in
+// flight when the epilogue reads C) while the MMAs of the next tile fill the
+// other one.  acc_full[b] (MMA -> epilogue, one commit) and acc_empty[b]
+// (epilogue -> MMA, 256 arrivals) hand the buffers over.  Every wait is
+// bounded as in cgemm_tf32_kernel.
 template <int BN, bool AMN>
-__global__ void __launch_bounds__(192, 1)
+__global__ void __launch_bounds__(PERSIST_THREADS, 1)
     cgemm_tf32_persistent(const __grid_constant__ CUtensorMap tmA,
                           const __grid_constant__ CUtensorMap tmAi,
                           const __grid_constant__ CUtensorMap tmBr,
@@ -399,8 +403,8 @@ __global__ void __launch_bounds__(192, 1)
         }
         mbar_init(smem_u32(&bars[2 * STAGES + 0]), 1);
         mbar_init(smem_u32(&bars[2 * STAGES + 1]), 1);
-        mbar_init(smem_u32(&bars[2 * STAGES + 2]), 128);
-        mbar_init(smem_u32(&bars[2 * STAGES + 3]), 128);
+        mbar_init(smem_u32(&bars[2 * STAGES + 2]), EPI_THREADS);
+        mbar_init(smem_u32(&bars[2 * STAGES + 3]), EPI_THREADS);
         *abort_flag = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
@@ -509,8 +513,10 @@ __global__ void __launch_bounds__(192, 1)
             }
         }
     } else {
-        // epilogue warps 2..5
+        // epilogue warps 2..9: warp w reads TMEM lanes 32 (w % 4) .. +31 (its
+        // rows), the two warps of a lane quadrant take alternate column chunks
         const int q = warp & 3;
+        const int half = (warp - 2) >> 2;
         const uint32_t lane_base = (uint32_t)(q * 32) << 16;
         int i = 0;
         for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++i) {
@@ -533,7 +539,7 @@ __global__ void __launch_bounds__(192, 1)
             const bool row_ok = row < ep.M;
             constexpr int CH = 16;
 #pragma unroll 1
-            for (int c0 = 0; c0 < BN; c0 += CH) {
+            for (int c0 = half * CH; c0 < BN; c0 += 2 * CH) {
                 float vr[CH], vi[CH];
                 tmem_ld16(d_re + lane_base + c0, vr);
                 tmem_ld16(d_im + lane_base + c0, vi);
@@ -813,7 +819,7 @@ static int launch_tf32(cudaStream_t s, const CUtensorMap &mA, const CUtensorMap 
                              "cgemm_tf32_persistent"));
         const int pst = maxst;
         const int grid = (int)(ntiles < num_sms() ? ntiles : num_sms());
-        cgemm_tf32_persistent<BN, AMN><<<grid, 192, TL::smem_bytes(pst), s>>>(
+        cgemm_tf32_persistent<BN, AMN><<<grid, PERSIST_THREADS, TL::smem_bytes(pst), s>>>(
             mA, mAi, mBr, mBi, ep, pst, MT, NT, (int)ntiles);
         MNPB_LAUNCH_CHECK("cgemm_tf32_persistent");
         return MNPB_OK;
