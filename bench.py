@@ -73,6 +73,9 @@ def parse():
                     help='skip the 64-particle uneven batched section')
     ap.add_argument('--batch-particles', type=int, default=64)
     ap.add_argument('--batch-nlam', type=int, default=41)
+    ap.add_argument('--batch-pad-ratio', type=float, default=1.25,
+                    help='second batched sweep with face counts within this ratio padded to '
+                         'one size per group (0: skip)')
     ap.add_argument('--iter-accuracy-tols', default='1e-6,1e-8',
                     help='GMRES tolerances whose 25k-face extinction is compared with the '
                          'dense FP64 GPU solve (empty: skip)')
@@ -354,6 +357,26 @@ def batched_section(args):
            "timing": "CUDA events around one full sweep after the untimed tuning sweep"}
     del solver
     torch.cuda.empty_cache()
+    if args.batch_pad_ratio:
+        # the same set with face counts within pad_ratio padded to one size per group
+        solver = BatchedBEMRet([cp for cp, _ in ps], refine_tol=1e-8, tuner=GemmTuner(),
+                               pad_ratio=args.batch_pad_ratio)
+        solver.solve_spectrum(exc, eneis)
+        torch.cuda.synchronize()
+        e0.record()
+        res2 = solver.solve_spectrum(exc, eneis)
+        e1.record()
+        torch.cuda.synchronize()
+        ms2 = e0.elapsed_time(e1)
+        out["padded"] = {
+            "pad_ratio": args.batch_pad_ratio, "groups": len(solver.groups),
+            "lambda_solves_per_s": len(ps) * len(eneis) / (ms2 / 1000.0), "ms": ms2,
+            "ext_max_rel_diff_vs_exact_groups":
+                float(np.max(np.abs(res2['ext'] - res['ext']) / np.abs(res['ext']))),
+            "launch_batches": [{"faces": st['n'], "entries": st['entries'],
+                                "particle_faces": st['faces']} for st in solver.stats]}
+        del solver
+        torch.cuda.empty_cache()
     return out
 
 

@@ -178,6 +178,19 @@ int mnpb_bemret_init_f64(void *stream, int64_t n, int64_t batch, double *G1, dou
  * mnpbem/bem/bem_ret.py:1360-1429 (_excitation).  pots (device c128,
  * [batch][16][nrhs][n]): phi1, phi1p, a1 (x,y,z), a1p (x,y,z), phi2, phi2p,
  * a2 (x,y,z), a2p (x,y,z). */
+/* Entries of different face counts in one batch: entry e keeps its n_e x n_e
+ * matrices (n_of_entry, device int32) in the top-left corner of npad x npad
+ * buffers; everything else becomes identity padding -- G1 = G2 = H1 = I,
+ * H2 = 0 on the pad block, no coupling -- in the c128 matrices (ld, stride)
+ * and their planar FP32 copies (ldp, planep, stridep).  The factorisations
+ * and solves then treat the entries as one batch and return zeros on the
+ * pad (with zero normals and zero right-hand sides there).  No reference
+ * counterpart (the reference solves one particle at a time). */
+int mnpb_pad_entries(void *stream, int64_t npad, int64_t batch, const int32_t *n_of_entry,
+                     double *G1, double *G2, double *H1, double *H2, int64_t ld, int64_t stride,
+                     float *G1p, float *G2p, float *H1p, float *H2p, int64_t ldp,
+                     int64_t planep, int64_t stridep);
+
 int mnpb_bemret_excitation(void *stream, int64_t n, int64_t batch, int64_t nrhs,
                            const double *pots, const double *eps, const double *kvac,
                            const double *nvec, int64_t nvec_stride, double *x_in);

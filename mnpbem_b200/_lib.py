@@ -104,6 +104,8 @@ SIGNATURES = {
     'mnpb_eels_wire': [_P, _I64, _I64, _P, _P, _P, _P, _P, _P, _P, _P, _P, _D, _D, _I64, _P, _P,
                        _D, _D, _D, _P, _P, _P],
     'mnpb_eels_field': [_P, _I64, _I64, _P, _P, _I, _P, _P, _D, _D, _P, _P, _P],
+    'mnpb_pad_entries': [_P, _I64, _I64, _P, _P, _P, _P, _P, _I64, _I64, _P, _P, _P, _P, _I64,
+                         _I64, _I64],
     'mnpb_mirror_contract': [_P, _I64, _I64, _I64, _I64, _P, _I64, _I64, _P, _P, _I64, _I64],
     'mnpb_bemret_mirror_workspace': [_I64, _I64],
     'mnpb_bemret_init_mirror_f64': [_P, _I64, _I64, _P, _P, _P, _P, _I64, _I64, _P, _P, _P, _P,

@@ -7,7 +7,11 @@ mnpbem/utils/multi_gpu.py:81).  Here every (particle, wavelength) pair is one
 entry of a batched mixed-precision factorisation:
 
 * particles are grouped by face count; a group's (particle, wavelength)
-  entries are cut into launch batches sized to the device memory;
+  entries are cut into launch batches sized to the device memory.  With
+  ``pad_ratio`` particles whose face counts lie within that ratio share one
+  group: every entry is padded to the group's largest face count with an
+  identity block (``mnpb_pad_entries``; exact, the pad decouples), so
+  particles of different size go through one factorisation;
 * each particle's wavelengths are assembled into consecutive entries of the
   batch (one assembly launch per particle), with its own face normals
   (``nvec_stride`` of the C ABI) so one factorisation launch sequence serves
@@ -44,10 +48,13 @@ class BatchedBEMRet(object):
     entries per launch batch, ``mem_bytes`` the device memory the batch
     buffers may take (default: 70 % of the free memory at construction).
     ``tuner``: a ``GemmTuner`` (a new one by default; ``None`` keeps the
-    library's default launch configuration)."""
+    library's default launch configuration).  ``pad_ratio`` (e.g. 1.25):
+    particles whose face counts differ by at most that factor are padded to a
+    common size and solved in the same launches (default: equal face counts
+    only)."""
 
     def __init__(self, particles, refine_tol=1e-8, refine_maxit=20, max_batch=256,
-                 mem_bytes=None, tuner='auto'):
+                 mem_bytes=None, tuner='auto', pad_ratio=None):
         self.particles = list(particles)
         for p in self.particles:
             _check_particle(p, 'BatchedBEMRet')
@@ -60,13 +67,36 @@ class BatchedBEMRet(object):
             free, _ = torch.cuda.mem_get_info()
             mem_bytes = int(0.7 * free)
         self.mem_bytes = int(mem_bytes)
-        self.groups = {}
-        for i, t in enumerate(self.tables):
-            self.groups.setdefault(t.n, []).append(i)
+        self.groups = self.buckets([t.n for t in self.tables], pad_ratio)
         self._bufs = None
         self.stats = []
 
     # ------------------------------------------------------------------ sizes
+    @staticmethod
+    def buckets(sizes, pad_ratio=None):
+        """Groups of particle indices by face count: {size: [indices]}.  With
+        ``pad_ratio``, consecutive face counts (ascending) join a group while
+        they stay within pad_ratio of its smallest; the key is the group's
+        largest face count, the size its entries are padded to."""
+        groups = {}
+        if pad_ratio is None:
+            for i, n in enumerate(sizes):
+                groups.setdefault(int(n), []).append(i)
+            return groups
+        if pad_ratio < 1.0:
+            raise ValueError("BatchedBEMRet: pad_ratio must be >= 1")
+        bucket, lo = [], None
+        for i in sorted(range(len(sizes)), key=lambda i: sizes[i]):
+            if bucket and sizes[i] > lo * pad_ratio:
+                groups[int(max(sizes[j] for j in bucket))] = bucket
+                bucket = []
+            if not bucket:
+                lo = sizes[i]
+            bucket.append(i)
+        if bucket:
+            groups[int(max(sizes[j] for j in bucket))] = bucket
+        return groups
+
     @staticmethod
     def entry_bytes(n, K):
         """Device bytes one (particle, wavelength) entry of a batch takes."""
@@ -92,15 +122,15 @@ class BatchedBEMRet(object):
             return self._bufs[1]
         self._bufs = None
         torch.cuda.empty_cache()
-        t0 = self.tables[self.groups[n][0]]
-        bt = _MixedBatch(t0, [0.0] * B)
-        dev = t0.device
+        dev = self.tables[self.groups[n][0]].device
+        bt = _MixedBatch(type('Size', (), {'device': dev, 'n': n})(), [0.0] * B)
         bt.nv = torch.empty((B, n, 3), dtype=torch.float64, device=dev)
         bt.pots = torch.empty((B, 16, K, n), dtype=torch.complex128, device=dev)
         bt.xin = torch.empty((B, 8, K, n), dtype=torch.complex128, device=dev)
         bt.x = torch.empty_like(bt.xin)
         wb = int(_lib.lib().mnpb_bemret_refine_workspace(n, B, K))
         bt.rwork = torch.empty(wb, dtype=torch.uint8, device=dev)
+        bt.n_of = torch.empty(B, dtype=torch.int32, device=dev)
         self._bufs = (key, bt)
         return bt
 
@@ -120,6 +150,8 @@ class BatchedBEMRet(object):
         return out
 
     def _assemble(self, bt, runs, n):
+        """Each particle's matrices (its own face count) into the top-left
+        corner of the batch's n x n entries."""
         ld = bt.ld
         for m, off, lams in runs:
             t = self.tables[m]
@@ -129,7 +161,7 @@ class BatchedBEMRet(object):
             poff = np.ascontiguousarray(t.part_off, dtype=np.int64)
             nb = len(lams)
             sl = slice(off, off + nb)
-            call('mnpb_assemble_ret2', _lib.stream_handle(), n, nb, ptr(t.pos), ptr(t.nvec),
+            call('mnpb_assemble_ret2', _lib.stream_handle(), t.n, nb, ptr(t.pos), ptr(t.nvec),
                  ptr(t.area), t.nparts, ptr(poff), ptr(d_k), ptr(d_s), t.nref, ptr(t.rows),
                  ptr(t.cols), ptr(t.g), ptr(t.fn), ptr(bt.G1[sl]), ptr(bt.H1[sl]),
                  ptr(bt.G2[sl]), ptr(bt.H2[sl]), ld, ld * n, ptr(bt.G1p[sl]), ptr(bt.H1p[sl]),
@@ -166,22 +198,34 @@ class BatchedBEMRet(object):
                 runs = self._runs(members, eneis, s0, s1)
                 eps = np.zeros((B, 4))
                 kvac = np.ones(B)
+                n_of = np.zeros(B, dtype=np.int32)
                 for m, off, lams in runs:
                     for q, lam in enumerate(lams):
                         e1, e2 = _scalar_eps(self.particles[m], lam)
                         eps[off + q] = (e1.real, e1.imag, e2.real, e2.imag)
                         kvac[off + q] = 2 * np.pi / lam
-                    bt.nv[off:off + len(lams)] = self.tables[m].nvec
+                    nm = self.tables[m].n
+                    bt.nv[off:off + len(lams), :nm] = self.tables[m].nvec
+                    bt.nv[off:off + len(lams), nm:] = 0.0
+                    n_of[off:off + len(lams)] = nm
                 if nb < B:
                     # unused tail slots of the last batch: copies of the first entry
                     eps[nb:] = eps[0]
                     kvac[nb:] = kvac[0]
+                    n_of[nb:] = n_of[0]
                     bt.nv[nb:] = bt.nv[0]
                 bt.eps.copy_(torch.from_numpy(eps))
                 bt.kvac.copy_(torch.from_numpy(kvac))
+                bt.n_of.copy_(torch.from_numpy(n_of))
+                padded = bool((n_of[:nb] < n).any())
 
                 def factor():
                     self._assemble(bt, runs, n)
+                    if padded:
+                        call('mnpb_pad_entries', _lib.stream_handle(), n, nb, ptr(bt.n_of),
+                             ptr(bt.G1), ptr(bt.G2), ptr(bt.H1), ptr(bt.H2), bt.ld,
+                             bt.ld * n, ptr(bt.G1p), ptr(bt.G2p), ptr(bt.H1p), ptr(bt.H2p),
+                             bt.ld, bt.ld * n, 2 * bt.ld * n)
                     if nb < B:
                         for A in (bt.G1, bt.G2, bt.H1, bt.H2, bt.G1p, bt.G2p, bt.H1p, bt.H2p):
                             A[nb:] = A[0]
@@ -200,7 +244,7 @@ class BatchedBEMRet(object):
                 bt.pots.zero_()
                 for m, off, lams in runs:
                     pots, _ = exc.potential_device(self.particles[m], self.tables[m], lams)
-                    bt.pots[off:off + len(lams)] = pots
+                    bt.pots[off:off + len(lams), :, :, :self.tables[m].n] = pots
                 call('mnpb_bemret_excitation', _lib.stream_handle(), n, B, K, ptr(bt.pots),
                      ptr(bt.eps), ptr(bt.kvac), ptr(bt.nv), 3 * n, ptr(bt.xin))
                 it = np.zeros(B, dtype=np.int32)
@@ -214,7 +258,7 @@ class BatchedBEMRet(object):
                 # cross sections per particle
                 for m, off, lams in runs:
                     p, t = self.particles[m], self.tables[m]
-                    x = bt.x[off:off + len(lams)]
+                    x = bt.x[off:off + len(lams), :, :, :t.n].contiguous()
                     e, _ = exc.farfield_device(p, t, x, lams, exc.dir)
                     ef, hf = exc.farfield_device(p, t, x, lams, nvec_s)
                     e, ef, hf = e.cpu().numpy(), ef.cpu().numpy(), hf.cpu().numpy()
@@ -236,7 +280,8 @@ class BatchedBEMRet(object):
                             sols[mi][li0 + q] = CompStruct(
                                 p, lam, sig1=v[0].T.copy(), h1=v[1:4].transpose(2, 0, 1).copy(),
                                 sig2=v[4].T.copy(), h2=v[5:8].transpose(2, 0, 1).copy())
-                self.stats.append({'n': n, 'entries': nb, 'batch': B, 'config': list(cfg)})
+                self.stats.append({'n': n, 'entries': nb, 'batch': B, 'config': list(cfg),
+                                   'faces': sorted(set(int(v) for v in n_of[:nb]))})
         out = {'ext': ext, 'sca': sca, 'iters': iters}
         if keep_solutions:
             out['solutions'] = sols

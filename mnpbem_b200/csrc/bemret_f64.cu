@@ -143,3 +143,52 @@ extern "C" int mnpb_bemret_excitation(void *stream, int64_t n, int64_t batch, in
     MNPB_LAUNCH_CHECK("excitation_kernel");
     return MNPB_OK;
 }
+
+// ---------------------------------------------------------------------------
+// Entries of different face counts in one batch: entry e holds its particle's
+// n_e x n_e matrices in the top-left corner of npad x npad buffers.  The rest
+// becomes block-diagonal identity padding -- G1 = G2 = H1 = I, H2 = 0 on the
+// pad block, zero coupling -- so Sigma1 = I, Sigma2 = 0, Delta = I and
+// Sigma = eps1 I there, every factorisation stays exact for the particle's
+// block, and a zero right-hand side on the pad gives a zero solution there.
+// ---------------------------------------------------------------------------
+namespace {
+__global__ void pad_entries_kernel(int npad, const int32_t *__restrict__ n_of, cd *G1, cd *G2,
+                                   cd *H1, cd *H2, int64_t ld, int64_t st, float *G1p, float *G2p,
+                                   float *H1p, float *H2p, int64_t ldp, int64_t planep,
+                                   int64_t stp) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y;
+    const int64_t e = blockIdx.z;
+    const int ne = n_of[e];
+    if (i >= npad || (i < ne && j < ne)) return;
+    const double d = i == j ? 1.0 : 0.0;
+    const int64_t o = e * st + (int64_t)j * ld + i;
+    G1[o] = G2[o] = H1[o] = cmk(d, 0.0);
+    H2[o] = cmk(0.0, 0.0);
+    const int64_t op = e * stp + (int64_t)j * ldp + i;
+    G1p[op] = G2p[op] = H1p[op] = (float)d;
+    G1p[op + planep] = G2p[op + planep] = H1p[op + planep] = 0.f;
+    H2p[op] = H2p[op + planep] = 0.f;
+}
+}  // namespace
+
+extern "C" int mnpb_pad_entries(void *stream, int64_t npad, int64_t batch,
+                                const int32_t *n_of_entry, double *G1, double *G2, double *H1,
+                                double *H2, int64_t ld, int64_t stride, float *G1p, float *G2p,
+                                float *H1p, float *H2p, int64_t ldp, int64_t planep,
+                                int64_t stridep) {
+    clear_error();
+    MNPB_REQUIRE(npad > 0 && npad < 65536 && batch > 0 && batch < 65536 && ld >= npad &&
+                     stride >= ld * npad && ldp >= npad && planep >= ldp * npad &&
+                     stridep >= 2 * planep,
+                 "pad_entries: bad sizes");
+    MNPB_REQUIRE(n_of_entry && G1 && G2 && H1 && H2 && G1p && G2p && H1p && H2p,
+                 "pad_entries: null pointer");
+    dim3 grid(ceil_div(npad, 128), (unsigned)npad, (unsigned)batch);
+    pad_entries_kernel<<<grid, 128, 0, as_stream(stream)>>>(
+        (int)npad, n_of_entry, (cd *)G1, (cd *)G2, (cd *)H1, (cd *)H2, ld, stride, G1p, G2p, H1p,
+        H2p, ldp, planep, stridep);
+    MNPB_LAUNCH_CHECK("pad_entries_kernel");
+    return MNPB_OK;
+}

@@ -1415,8 +1415,12 @@ int gemm(Ctx &c, int m, int n, int k, float alpha, CMatF A, CMatF B, float beta,
         set_error("f32 gemm: k = 0 with beta != 1 is not supported");
         return MNPB_EINVAL;
     }
+    // four rows per thread only where that still leaves enough threads to
+    // keep the GPU's memory pipes full (small batches of small matrices keep
+    // one row per thread)
     const bool vec4 = n <= 4 && m % 4 == 0 && A.ld % 4 == 0 && A.plane % 4 == 0 &&
-                      A.stride % 4 == 0 && ((uintptr_t)A.p & 15) == 0;
+                      A.stride % 4 == 0 && ((uintptr_t)A.p & 15) == 0 &&
+                      (int64_t)c.batch * (m / 4) >= (int64_t)dev_sms() * 256;
     if (vec4) {
         dim3 grid(ceil_div(m, 512), c.batch);
         ProfScope ps(c.s, PC_SGEMM, 8.0 * (double)m * k * c.batch);   // bytes of A streamed

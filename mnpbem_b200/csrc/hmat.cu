@@ -253,11 +253,18 @@ struct HMats {
 // columns in flight per warp (groups of 16 or 8 lanes).  The item's partial t goes to
 // TP + (offTP[block] + segment * rank) * NC; hm_vtx_reduce_kernel adds a
 // block's segments in order (deterministic).
+// Warps per block of the product kernels (one work item per warp): small
+// blocks let the SM replace a finished warp's block sooner when the items'
+// lengths differ.
+#ifndef HM_WPB
+#define HM_WPB 8
+#endif
+
 template <int NC>
-__global__ void __launch_bounds__(256, 3) hm_vtx_kernel(HMats P, int n, int nc, int nvitem,
-                                                     const int4 *__restrict__ vitems,
-                                                     const int4 *__restrict__ lr) {
-    const int it = blockIdx.x * 8 + (threadIdx.x >> 5);
+__global__ void __launch_bounds__(32 * HM_WPB, 24 / HM_WPB) hm_vtx_kernel(
+    HMats P, int n, int nc, int nvitem, const int4 *__restrict__ vitems,
+    const int4 *__restrict__ lr) {
+    const int it = blockIdx.x * HM_WPB + (threadIdx.x >> 5);
     if (it >= nvitem) return;
     const HMat &H = P.h[blockIdx.y];
     const int l = threadIdx.x & 31;
@@ -415,14 +422,14 @@ __device__ __forceinline__ void rows_accumulate(const float2 *__restrict__ A, in
 
 // Launch-bound occupancy and software-pipelining width of the row sums.
 #ifndef HM_ROWS_MINB
-#define HM_ROWS_MINB 3
+#define HM_ROWS_MINB 4
 #endif
 #ifndef HM_ROWS_UN
 #define HM_ROWS_UN 4
 #endif
 
 template <int NC>
-__global__ void __launch_bounds__(256, HM_ROWS_MINB) hm_rows_kernel(HMats P, int n, int nitem,
+__global__ void __launch_bounds__(32 * HM_WPB, HM_ROWS_MINB * 8 / HM_WPB) hm_rows_kernel(HMats P, int n, int nitem,
                                                          const int4 *__restrict__ items,
                                                          const int2 *__restrict__ chunks,
                                                          const int2 *__restrict__ leaf_rows,
@@ -430,7 +437,7 @@ __global__ void __launch_bounds__(256, HM_ROWS_MINB) hm_rows_kernel(HMats P, int
                                                          const int4 *__restrict__ dn,
                                                          const int4 *__restrict__ lr,
                                                          cd *__restrict__ partial) {
-    const int it = blockIdx.x * 8 + (threadIdx.x >> 5);
+    const int it = blockIdx.x * HM_WPB + (threadIdx.x >> 5);
     if (it >= nitem) return;
     const HMat &H = P.h[blockIdx.y];
     const int l = threadIdx.x & 31;
@@ -630,18 +637,18 @@ extern "C" int mnpb_hmat_matvec(void *stream, int64_t n, int64_t nc, int64_t nma
             Q, (int)n, ncc, c2p);
         MNPB_LAUNCH_CHECK("hm permute_kernel");
         if (nlr > 0) {
-            dim3 g((unsigned)ceil_div(nvitem, 8), (unsigned)nmat);
-            hm::hm_vtx_kernel<4><<<g, 256, 0, s>>>(Q, (int)n, ncc, (int)nvitem,
+            dim3 g((unsigned)ceil_div(nvitem, HM_WPB), (unsigned)nmat);
+            hm::hm_vtx_kernel<4><<<g, 32 * HM_WPB, 0, s>>>(Q, (int)n, ncc, (int)nvitem,
                                                    (const int4 *)vitems, (const int4 *)lowrank);
             MNPB_LAUNCH_CHECK("hm_vtx_kernel");
             dim3 gr((unsigned)ceil_div(nlr, 8), (unsigned)nmat);
             hm::hm_vtx_reduce_kernel<4><<<gr, 256, 0, s>>>(Q, ncc, (int)nlr, vptr);
             MNPB_LAUNCH_CHECK("hm_vtx_reduce_kernel");
         }
-        dim3 g((unsigned)ceil_div(nitem, 8), (unsigned)nmat);
+        dim3 g((unsigned)ceil_div(nitem, HM_WPB), (unsigned)nmat);
         dim3 gr((unsigned)ceil_div(nchunk, 8), (unsigned)nmat);
 #define MNPB_HM_ROWS(NCV)                                                                       \
-    hm::hm_rows_kernel<NCV><<<g, 256, 0, s>>>(Q, (int)n, (int)nitem, (const int4 *)items,       \
+    hm::hm_rows_kernel<NCV><<<g, 32 * HM_WPB, 0, s>>>(Q, (int)n, (int)nitem, (const int4 *)items,       \
                                               (const int2 *)chunks, (const int2 *)leaf_rows,    \
                                               lent, (const int4 *)dense, (const int4 *)lowrank, \
                                               (cd *)partial);                                   \

@@ -56,3 +56,28 @@ def test_batched_uneven_particles(gpu_ok, tmp_path):
     # a second sweep reuses the stored choices and gives the same cross sections
     res2 = solver.solve_spectrum(exc, list(z['lams']))
     assert np.abs(res2['ext'] - ext).max() / np.abs(ext).max() < 1e-9
+
+
+def test_batched_padded_to_one_size(gpu_ok):
+    """Particles of 284, 448 and 568 faces in one group (pad_ratio 2): every
+    entry padded to 568 faces with an identity block, one factorisation for
+    all 15 (particle, wavelength) entries; the same cross sections and
+    charges as the reference."""
+    from mnpbem_b200.batch import BatchedBEMRet
+    from mnpbem_b200.excitation import PlaneWaveRet
+    z = golden('golden_batch')
+    ps = _particles()
+    exc = PlaneWaveRet([[1.0, 0, 0], [0, 1.0, 0], [0, 0, 1.0]],
+                       [[0, 0, 1.0], [0, 0, 1.0], [1.0, 0, 0]])
+    solver = BatchedBEMRet(ps, refine_tol=1e-8, tuner=None, pad_ratio=2.0)
+    assert list(solver.groups) == [568]
+    res = solver.solve_spectrum(exc, list(z['lams']), keep_solutions=True)
+    err_e = np.abs(res['ext'] - z['ext']) / np.abs(z['ext'])
+    err_s = np.abs(res['sca'] - z['sca']) / np.abs(z['sca'])
+    assert err_e.max() < 1e-6 and err_s.max() < 1e-6
+    for i in range(len(ps)):
+        s2 = res['solutions'][i][1].sig2[:, 0]
+        ref = z['sig2_%d' % i]
+        assert s2.shape == ref.shape
+        assert np.abs(s2 - ref).max() / np.abs(ref).max() < 1e-6, i
+    assert solver.stats[0]['entries'] == 15 and solver.stats[0]['faces'] == [284, 448, 568]

@@ -2,6 +2,7 @@
 (host only, no GPU): the rod generator against the reference's packaged
 trirod, closed outward surfaces, the seeded particle set, and how entries of
 a face-count group are cut into batches and per-particle runs."""
+import pytest
 import numpy as np
 
 from mnpbem_b200.geometry import Particle, rod_mesh, trirod, trisphere
@@ -77,3 +78,16 @@ def test_batches_and_runs():
     bs.mem_bytes = 40 * BatchedBEMRet.entry_bytes(2000, 3)
     spans, size = bs._batches(2000, 100, 3)
     assert size <= 40 and spans[-1][1] == 100 and all(b - a <= size for a, b in spans)
+
+
+def test_padding_buckets():
+    from mnpbem_b200.batch import BatchedBEMRet
+    sizes = [284, 300, 448, 284, 520, 700, 720, 2446]
+    assert BatchedBEMRet.buckets(sizes) == {284: [0, 3], 300: [1], 448: [2], 520: [4],
+                                            700: [5], 720: [6], 2446: [7]}
+    g = BatchedBEMRet.buckets(sizes, 1.25)
+    assert g == {300: [0, 3, 1], 520: [2, 4], 720: [5, 6], 2446: [7]}
+    assert all(max(sizes[i] for i in v) == k for k, v in g.items())
+    assert sorted(i for v in g.values() for i in v) == list(range(len(sizes)))
+    with pytest.raises(ValueError):
+        BatchedBEMRet.buckets(sizes, 0.9)
