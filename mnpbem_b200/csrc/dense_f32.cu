@@ -1420,7 +1420,7 @@ int gemm(Ctx &c, int m, int n, int k, float alpha, CMatF A, CMatF B, float beta,
     // one row per thread)
     const bool vec4 = n <= 4 && m % 4 == 0 && A.ld % 4 == 0 && A.plane % 4 == 0 &&
                       A.stride % 4 == 0 && ((uintptr_t)A.p & 15) == 0 &&
-                      (int64_t)c.batch * (m / 4) >= (int64_t)dev_sms() * 256;
+                      (int64_t)c.batch * (m / 4) >= (int64_t)device_sms() * 256;
     if (vec4) {
         dim3 grid(ceil_div(m, 512), c.batch);
         ProfScope ps(c.s, PC_SGEMM, 8.0 * (double)m * k * c.batch);   // bytes of A streamed
