@@ -189,11 +189,15 @@ class BatchedBEMRet(object):
         sols = [[None] * L for _ in range(P)] if keep_solutions else None
         nvec_s, area_s = pinfty()
         self.stats = []
+        bt = None
         for n in sorted(self.groups):
             members = self.groups[n]
             spans, B = self._batches(n, len(members) * L, K)
             for s0, s1 in spans:
                 nb = s1 - s0
+                # drop this frame's reference first: a new buffer shape must be
+                # able to free the previous set before it allocates its own
+                bt = None
                 bt = self._buffers(n, B, K)
                 runs = self._runs(members, eneis, s0, s1)
                 eps = np.zeros((B, 4))

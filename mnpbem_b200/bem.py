@@ -58,6 +58,28 @@ def _fields_by_wavelength(x, K):
     return sig1, sig2, h1, h2
 
 
+def _fields_device(x):
+    """The reordering of ``_fields_by_wavelength`` done on the device: one
+    flat tensor [sig1 (B, n, K) | sig2 | h1 (B, n, 3, K) | h2] from a batch of
+    solution vectors x (B, 8, K, n)."""
+    return torch.cat([x[:, 0].permute(0, 2, 1).reshape(-1),
+                      x[:, 4].permute(0, 2, 1).reshape(-1),
+                      x[:, 1:4].permute(0, 3, 1, 2).reshape(-1),
+                      x[:, 5:8].permute(0, 3, 1, 2).reshape(-1)])
+
+
+def _fields_host(flat, shape):
+    """Views sig1, sig2 (B, n, K) and h1, h2 (B, n, 3, K) of the flat host
+    array ``_fields_device`` made from solutions of shape (B, 8, K, n)."""
+    B, _, K, n = shape
+    s = B * n * K
+    sig1 = flat[:s].reshape(B, n, K)
+    sig2 = flat[s:2 * s].reshape(B, n, K)
+    h1 = flat[2 * s:5 * s].reshape(B, n, 3, K)
+    h2 = flat[5 * s:8 * s].reshape(B, n, 3, K)
+    return sig1, sig2, h1, h2
+
+
 class _RetBatch(object):
     """Device buffers of one factorised batch of wavelengths (FP64)."""
 
@@ -379,13 +401,15 @@ class BEMRet(object):
             bt = self._factor(chunk, stream=st)
             pots, K = self._spectrum_pots(exc, chunk, st)
             xout = self._solve_batch(bt, pots, K, stream=st)
-            # device -> pinned host copy (page-locked: full PCIe rate), then a
-            # numpy view of it
-            host = torch.empty(xout.shape, dtype=xout.dtype, pin_memory=True)
             with torch.cuda.stream(st):
-                host.copy_(xout, non_blocking=True)
+                # fields reordered on the device (each wavelength's fields
+                # contiguous), then one device -> pinned host copy
+                # (page-locked: full PCIe rate) that the host only views
+                dev = _fields_device(xout)
+                host = torch.empty(dev.shape, dtype=dev.dtype, pin_memory=True)
+                host.copy_(dev, non_blocking=True)
             st.synchronize()
-            return host.numpy(), K
+            return _fields_host(host.numpy(), xout.shape), K
 
         if streams > 1:
             res = self.pipeline(chunks, work, streams)
@@ -393,8 +417,10 @@ class BEMRet(object):
             cur = stream if stream is not None else torch.cuda.current_stream()
             res = [work(c, cur) for c in chunks]
         out = []
-        for chunk, (x, K) in zip(chunks, res):
-            sig1, sig2, h1, h2 = _fields_by_wavelength(x, K)
+        for chunk, (fields, K) in zip(chunks, res):
+            sig1, sig2, h1, h2 = fields
+            if K == 1:
+                sig1, sig2, h1, h2 = sig1[..., 0], sig2[..., 0], h1[..., 0], h2[..., 0]
             for b, enei in enumerate(chunk):
                 out.append(CompStruct(self.p, enei, sig1=sig1[b], sig2=sig2[b], h1=h1[b],
                                       h2=h2[b]))

@@ -33,3 +33,21 @@ def test_batched_fields_match_per_wavelength(K):
             assert got.shape == want.shape, name
             assert np.array_equal(got, want), name
             assert got.flags['C_CONTIGUOUS'], name
+
+
+@pytest.mark.parametrize('K', [1, 3])
+def test_device_reordering_matches_host(K):
+    """``solve_spectrum`` reorders on the device (torch ops, here on CPU
+    tensors) and only views the copied block on the host: the views equal
+    the host reordering and are contiguous per wavelength."""
+    import torch
+    from mnpbem_b200.bem import _fields_device, _fields_host
+    rng = np.random.default_rng(4)
+    B, n = 5, _Tables.n
+    x = rng.standard_normal((B, 8, K, n)) + 1j * rng.standard_normal((B, 8, K, n))
+    want = _fields_by_wavelength(x, K)
+    got = _fields_host(_fields_device(torch.from_numpy(x)).numpy(), x.shape)
+    for w, g in zip(want, got):
+        g = g[..., 0] if K == 1 else g
+        assert g.shape == w.shape and np.array_equal(g, w)
+        assert g[0].flags['C_CONTIGUOUS']
