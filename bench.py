@@ -76,9 +76,9 @@ def parse():
     ap.add_argument('--batch-pad-ratio', type=float, default=1.25,
                     help='second batched sweep with face counts within this ratio padded to '
                          'one size per group (0: skip)')
-    ap.add_argument('--iter-accuracy-tols', default='1e-6,1e-8',
-                    help='GMRES tolerances whose 25k-face extinction is compared with the '
-                         'dense FP64 GPU solve (empty: skip)')
+    ap.add_argument('--iter-accuracy', default='1e-6:1e-6,1e-6:1e-8,1e-8:1e-8,1e-10:1e-10',
+                    help='(ACA htol:GMRES tol) pairs of the iterative accuracy study against '
+                         'dense solves of the 25k-face rod at 500/700/900 nm ("" skips it)')
     ap.add_argument('--mn-min-n', type=int, default=None,
                     help='GEMM knob: TF32 A operands of products with 64 < N < this are '
                          'packed instead of read in place (library default 0: never)')
@@ -267,42 +267,79 @@ def iterative_section(args):
                                    "achieved_GBs": nbytes / (hm_ms / cnt) / 1e6}
     out["compression"] = [round(c, 4) for c in bem.compression()]
     out["wavelengths"] = [float(e) for e in eneis]
-    tols = [float(t) for t in args.iter_accuracy_tols.split(',') if t.strip()]
-    if tols:
-        # extinction of the H-matrix / GMRES solve at several tolerances
-        # against the dense FP64 GPU solve of the same mesh and wavelength
-        lam = eneis[0]
-        acc = {"wavelength": lam, "runs": []}
-        ext_it = {}
-        for tol in tols:
-            bem.tol = tol
-            bem.enei = None
-            sig, _ = bem.solve(exc.potential(cp, lam))
-            ext_it[tol] = (float(exc.extinction(sig)), int(bem.matvec_counts()[-1]),
-                           int(bem.info()[0][-1]))
-        del bem, sig
-        torch.cuda.empty_cache()
-        from mnpbem_b200.bem import BEMRet
-        t0 = time.time()
-        dense = BEMRet(cp)
-        sd, _ = dense.solve(exc.potential(cp, lam))
-        ext_d = float(exc.extinction(sd))
-        torch.cuda.synchronize()
-        acc["dense_fp64_ext"] = ext_d
-        acc["dense_fp64_s"] = time.time() - t0
-        for tol in tols:
-            e, mv, flag = ext_it[tol]
-            acc["runs"].append({"gmres_tol": tol, "ext": e, "operator_applications": mv,
-                                "converged": flag == 0,
-                                "ext_rel_err_vs_dense": abs(e - ext_d) / abs(ext_d)})
-        ok = [r["gmres_tol"] for r in acc["runs"] if r["ext_rel_err_vs_dense"] <= 1e-6]
-        acc["largest_tol_within_1e-6"] = max(ok) if ok else None
-        out["accuracy_vs_dense"] = acc
-        del dense, sd
-    else:
-        del bem
+    cases = [tuple(float(v) for v in c.split(':')) for c in args.iter_accuracy.split(',')
+             if c.strip()]
+    del bem
+    torch.cuda.empty_cache()
+    if cases:
+        out["accuracy_vs_dense"] = iterative_accuracy(cp, exc, cases)
     torch.cuda.empty_cache()
     return out
+
+
+def iterative_accuracy(cp, exc, cases, lams=(500.0, 700.0, 900.0)):
+    """Extinction of the H-matrix / GMRES solve of the 25k-face rod for
+    (ACA htol, GMRES tol) pairs at three wavelengths against dense solves of
+    the same mesh: the mixed-precision solver refined in FP64 to 1e-11 at
+    every wavelength, itself checked against the plain FP64 solver at the
+    first.  The error of the iterative solve is set by the ACA tolerance
+    (the operator is approximated to ~htol per block and the system's
+    conditioning near the plasmon amplifies that), not by the GMRES
+    tolerance once that is below it."""
+    import torch
+    from mnpbem_b200.bem import BEMRet
+    from mnpbem_b200.bem_iter import BEMRetIter
+    lams = [float(l) for l in lams]
+    acc = {"wavelengths": lams, "runs": []}
+    for htol in sorted(set(h for h, _ in cases), reverse=True):
+        bem = BEMRetIter(cp, hmatrix=True, cleaf=64, htol=htol, preconditioner='none',
+                         tol=1e-6, maxit=1000)
+        for h, gtol in cases:
+            if h != htol:
+                continue
+            bem.tol = gtol
+            run = {"htol": htol, "gmres_tol": gtol, "ext": [], "operator_applications": [],
+                   "converged": True}
+            for lam in lams:
+                bem.enei = None
+                sig, _ = bem.solve(exc.potential(cp, lam))
+                run["ext"].append(float(exc.extinction(sig)))
+                run["operator_applications"].append(int(bem.matvec_counts()[-1]))
+                run["converged"] &= int(bem.info()[0][-1]) == 0
+            run["compression"] = [round(c, 4) for c in bem.compression()]
+            run["stored_GB"] = sum(hm.stored_bytes() for hm in
+                                   (bem.G1, bem.G2, bem.H1, bem.H2)) / 1e9
+            acc["runs"].append(run)
+        del bem
+        torch.cuda.empty_cache()
+    t0 = time.time()
+    mixed = BEMRet(cp, precision='mixed', refine_tol=1e-11)
+    ext_d = []
+    for lam in lams:
+        sd, _ = mixed.solve(exc.potential(cp, lam))
+        ext_d.append(float(exc.extinction(sd)))
+        mixed.clear()
+    torch.cuda.synchronize()
+    acc["dense_ext"] = ext_d
+    acc["dense"] = "BEMRet mixed precision refined in FP64 to 1e-11 (per wavelength)"
+    acc["dense_s"] = time.time() - t0
+    del mixed
+    torch.cuda.empty_cache()
+    t0 = time.time()
+    f64 = BEMRet(cp)
+    sd, _ = f64.solve(exc.potential(cp, lams[0]))
+    e64 = float(exc.extinction(sd))
+    torch.cuda.synchronize()
+    acc["fp64_dense_ext_first_wavelength"] = e64
+    acc["fp64_dense_s"] = time.time() - t0
+    acc["mixed_vs_fp64_rel_diff"] = abs(ext_d[0] - e64) / abs(e64)
+    del f64, sd
+    for run in acc["runs"]:
+        run["ext_rel_err_vs_dense"] = [abs(e - d) / abs(d) for e, d in zip(run["ext"], ext_d)]
+    ok = [(r["htol"], r["gmres_tol"]) for r in acc["runs"]
+          if max(r["ext_rel_err_vs_dense"]) <= 1e-6]
+    acc["loosest_within_1e-6"] = list(max(ok)) if ok else None
+    return acc
 
 
 BATCH_WORKLOAD = ("Batched uneven solves: 64 seed-random gold particles (seed 0; spheres "

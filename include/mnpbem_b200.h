@@ -686,31 +686,35 @@ int mnpb_hmat_compact(void *stream, int64_t nblk, const int32_t *blocks, const i
                       const int64_t *outU, const int64_t *outV, float *U, float *V);
 
 /* Y_i = H_i X_i for nmat (<= 4) H-matrices of one block partition; descs
- * points to nmat host records of 14 pointers each: D, U, V, rank, offD,
- * offU, offV, offT, X, Y, T, Xc, offTP, TP (X, Y: complex128 n x nc, column
- * stride n, face order; T: FP64 scratch of 2 * min(nc, 4) * sum(rank)
- * doubles; Xc: FP64 scratch of 2 * n * min(nc, 4) doubles for X in cluster
- * order; offTP (int64 per low-rank block) and TP (FP64 scratch, 8 doubles
- * per entry) hold the per-segment partials of V^T x: block b's segments
- * start at TP + 8 * offTP[b], rank entries per segment).  vitems: nvitem
- * int32 quadruples (block, first column, end column, segment) covering
- * every low-rank block's columns; vptr (nlr + 1) the items of each block.
- * leaf_rows:
- * int32 (start, rows) per leaf cluster; lptr/lent: CSR list per leaf of
- * contributing blocks (e >= 0 dense block e, e < 0 low-rank block -e-1);
- * chunks: nchunk int32 pairs (leaf, first row) covering every leaf in
- * 32-row pieces; items: nitem int32 quadruples (chunk, first entry, end
- * entry, 0) splitting each chunk's list into short segments, cptr (nchunk +
- * 1) the items of each chunk; partial: FP64 scratch of nmat * nitem * 256
- * doubles.
+ * points to nmat host records of 13 pointers each: D, U, V, rank, offT, X,
+ * Y, T, Xc, offTP, TP, rent, vent.  X, Y: complex128 n x nc, column stride
+ * n, face order; T: FP64 scratch of 2 * min(nc, 4) * sum(rank) doubles
+ * (t_b = V_b^T x of block b at T + 2 * min(nc, 4) * offT[b]); Xc: FP64
+ * scratch of 2 * n * min(nc, 4) doubles for X in cluster order; offTP
+ * (int64 per low-rank block) and TP (FP64 scratch, 8 doubles per entry)
+ * hold the per-segment partials of V^T x (block b's segments start at TP +
+ * 8 * offTP[b], rank entries per segment).
+ * rent: one 32-byte record per entry of the leaves' contribution lists
+ * {int64 a, int64 xo, int32 lda, int32 cnt, int32 kind, int32 pad}: the
+ * leaf's rows of a dense block (kind 0: a = float2 offset in D of (leaf's
+ * first row, column 0), lda = block rows, cnt = block columns, xo = first
+ * column in cluster order) or of a low-rank factor U (kind 1: a in U, cnt =
+ * rank, xo = offT[b]).  vent: one 32-byte record per V^T x item {int64 v,
+ * int64 out, int32 xo, int32 cnt, int32 r, int32 pad}: a segment of <= 64
+ * columns of one low-rank block, V(j, q) at V + 2 * (v + (j - j0) * r + q),
+ * x columns from xo (cluster order), partial to TP + 8 * out; vptr (nlr + 1)
+ * the items of each block, in segment order.  leaf_rows: int32 (start,
+ * rows) per leaf cluster; chunks: nchunk int32 pairs (leaf, first row)
+ * covering every leaf in 32-row pieces; items: nitem int32 quadruples
+ * (chunk, first entry, end entry, first row in the leaf << 6 | rows) with
+ * at most 32 entries each, cptr (nchunk + 1) the items of each chunk;
+ * partial: FP64 scratch of nmat * nitem * 256 doubles.
  * Replaces HMatrix.mtimes_vec (mnpbem/greenfun/hmatrix.py:450-541). */
 int mnpb_hmat_matvec(void *stream, int64_t n, int64_t nc, int64_t nmat, const void *descs,
-                     const int32_t *c2p, int64_t ndense, const int32_t *dense, int64_t nlr,
-                     const int32_t *lowrank, int64_t nleaf, const int32_t *leaf_rows,
-                     const int32_t *lptr, const int32_t *lent, int64_t nchunk,
-                     const int32_t *chunks, int64_t nitem, const int32_t *items,
+                     const int32_t *c2p, int64_t nlr, int64_t nchunk, const int32_t *chunks,
+                     const int32_t *leaf_rows, int64_t nitem, const int32_t *items,
                      const int32_t *cptr, double *partial, int64_t nvitem,
-                     const int32_t *vitems, const int32_t *vptr);
+                     const int32_t *vptr);
 
 /* y = A x of the packed retarded operator from the four products P1 = G1 v1,
  * P2 = G2 v2, Q1 = H1 v1, Q2 = H2 v2 (n x 4*nrhs each, columns sig then h

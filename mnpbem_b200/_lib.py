@@ -67,8 +67,8 @@ SIGNATURES = {
     'mnpb_hmat_aca': [_P, _I64, _P, _I64, _P, _I64, _P, _P, _P, _I64, _I64, _D, _P, _P],
     'mnpb_hmat_gather_dense': [_P, _P, _I64, _P, _I64, _P, _P, _P],
     'mnpb_hmat_compact': [_P, _I64, _P, _P, _P, _P, _P, _P, _P, _P, _P],
-    'mnpb_hmat_matvec': [_P, _I64, _I64, _I64, _P, _P, _I64, _P, _I64, _P, _I64, _P, _P, _P,
-                         _I64, _P, _I64, _P, _P, _P, _I64, _P, _P],
+    'mnpb_hmat_matvec': [_P, _I64, _I64, _I64, _P, _P, _I64, _I64, _P, _P, _I64, _P, _P, _P,
+                         _I64, _P],
     'mnpb_bem_afun': [_P, _I64, _I64, _P, _P, _P, _P, _P, _D, _D, _D, _D, _D, _P],
     'mnpb_gmres_workspace': [_I64, _I64],
     'mnpb_gmres_arnoldi': [_P, _I64, _I64, _P, _I64, _P, _P, _P, _P, _I64],

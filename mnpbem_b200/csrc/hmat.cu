@@ -227,86 +227,139 @@ __global__ void compact_kernel(const int4 *__restrict__ blk, const int *__restri
 // ---------------------------------------------------------------------------
 // H-matrix times vectors
 // ---------------------------------------------------------------------------
+// Work records, built on the host once the ranks are known (one array per
+// matrix, since the low-rank offsets depend on the ranks):
+//
+// RowEnt, one per entry of a leaf's contribution list: the leaf's rows of a
+// dense block (kind 0, columns = the block's columns, x = X in cluster order
+// from column xo) or of a low-rank factor U (kind 1, columns = rank, x = the
+// block's t = V^T x at T + xo * NC).  a: float2 offset, in D or U, of the
+// entry (first row of the leaf, column 0); column stride lda.
+struct RowEnt {
+    long long a, xo;
+    int lda, cnt, kind, pad;
+};
+// VtxEnt, one per V^T x work item (a segment of <= 64 columns of one
+// low-rank block): V(j, q) of the segment at V + v + (j - j0) * r + q; its
+// x columns start at xo (cluster order); the item's partial t goes to
+// TP + out * 4 (r rows of 4 right-hand sides).
+struct VtxEnt {
+    long long v, out;
+    int xo, cnt, r, pad;
+};
+
 // Per matrix (up to 4 in one launch, blockIdx.y):
 struct HMat {
-    const float2 *D;      // dense blocks, column-major, at offD
-    const float2 *U, *V;  // low-rank factors, column-major, at offU / offV
+    const float2 *D;      // dense blocks, column-major
+    const float2 *U, *V;  // low-rank factors (U column-major, V transposed)
     const int *rank;      // per low-rank block
-    const int64_t *offD, *offU, *offV, *offT;   // offT: t_b at T + offT[b] * nc
+    const int64_t *offT;  // t_b at T + offT[b] * nc
     const cd *X;          // n x nc input (face order), column stride n
     cd *Y;                // n x nc output (face order)
     cd *T;                // scratch V^T x
     cd *Xc;               // scratch: X in cluster order (n x nc)
-    const int64_t *offTP; // per low-rank block: start of its segment partials (entries / NC)
+    const int64_t *offTP; // per low-rank block: start of its segment partials (entries / 4)
     cd *TP;               // scratch: segment partials of V^T x
+    const RowEnt *rent;   // row-sum records (one per contribution-list entry)
+    const VtxEnt *vent;   // V^T x records (one per item)
 };
 struct HMats {
     HMat h[4];
 };
 
-// t_b = V_b^T x[cols] in two steps.  Work items vitems[i] = (block, first
-// column, end column, segment index within the block) cover every low-rank
-// block in segments of at most a few hundred columns; one warp per item,
-// lane = factor column q (V is stored transposed: element (j, q) at
-// V[q + j * rank], so the lanes of one j read consecutive words), x in
-// cluster order read as a broadcast.  Blocks of rank <= 16 put 2 or 4
-// columns in flight per warp (groups of 16 or 8 lanes).  The item's partial t goes to
-// TP + (offTP[block] + segment * rank) * NC; hm_vtx_reduce_kernel adds a
-// block's segments in order (deterministic).
-// Warps per block of the product kernels (one work item per warp): small
-// blocks let the SM replace a finished warp's block sooner when the items'
-// lengths differ.
+// Warps per block of the product kernels (one work item per warp) and the
+// launch-bound block count per SM.  Measured on the four matrices of the
+// 25,152-face rod (4 right-hand sides): 4 warps x >= 4 blocks 1.05 ms per
+// product, 8 x 3 1.06 ms, 8 x 4 (64 registers, spills) 1.24 ms.
 #ifndef HM_WPB
-#define HM_WPB 8
+#define HM_WPB 4
 #endif
+#ifndef HM_MINB
+#define HM_MINB 4
+#endif
+constexpr int HM_VSEG = 64;      // columns per V^T x item (the host cuts segments this long)
+constexpr int HM_XS = 32;        // x columns per shared-memory stage of the row sums
 
+// 16-byte asynchronous copies global -> shared (completion per thread via
+// commit / wait groups; a __syncwarp after the wait publishes the warp's copies)
+__device__ __forceinline__ void cp16(void *dst, const void *src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(
+                     (unsigned)__cvta_generic_to_shared(dst)),
+                 "l"(src)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_wait() {
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+__device__ __forceinline__ float2 ld_stream(const float2 *p) { return __ldcs(p); }
+
+// t_b = V_b^T x in two steps.  One warp per VtxEnt item: the item's x
+// columns (<= 64, all right-hand sides) are staged in shared memory with
+// asynchronous copies while the first factor loads are in flight; lane =
+// factor column q (V is stored transposed, so the lanes of one j read
+// consecutive words) and the x values are shared-memory broadcasts.  Blocks
+// of rank <= 16 put 2 or 4 columns in flight per warp (groups of 16 or 8
+// lanes, summed in a fixed order at the end).  hm_vtx_reduce_kernel adds a
+// block's segments in order (deterministic).
 template <int NC>
-__global__ void __launch_bounds__(32 * HM_WPB, 24 / HM_WPB) hm_vtx_kernel(
-    HMats P, int n, int nc, int nvitem, const int4 *__restrict__ vitems,
-    const int4 *__restrict__ lr) {
-    const int it = blockIdx.x * HM_WPB + (threadIdx.x >> 5);
+__global__ void __launch_bounds__(32 * HM_WPB, HM_MINB) hm_vtx_kernel(HMats P, int n, int nc,
+                                                                       int nvitem) {
+    __shared__ __align__(16) cd xsm[HM_WPB][HM_VSEG * NC];
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    const int it = blockIdx.x * HM_WPB + w;
     if (it >= nvitem) return;
     const HMat &H = P.h[blockIdx.y];
-    const int l = threadIdx.x & 31;
-    const int4 vi = vitems[it];
-    const int b = vi.x;
-    const int4 bk = lr[b];
-    const int r = H.rank[b];
-    const float2 *V = H.V + H.offV[b];
-    cd *out = H.TP + (H.offTP[b] + (int64_t)vi.w * r) * NC;
-    const cd *xc = H.Xc + bk.z;
-    constexpr int UN = 8;
+    const VtxEnt ve = H.vent[it];
+    const int r = ve.r, cnt = ve.cnt;
+    if (r == 0 || cnt == 0) return;
+    cd *xb = xsm[w];
+    for (int j = l; j < cnt; j += 32)
+#pragma unroll
+        for (int c = 0; c < NC; ++c)
+            if (c < nc) cp16(xb + j * NC + c, H.Xc + ve.xo + j + (int64_t)c * n);
+    cp_commit();
+    const float2 *V = H.V + ve.v;
+    cd *out = H.TP + ve.out * 4;
     if (r <= 16) {
-        // ranks up to 16 (most blocks): the warp splits into G groups of P
-        // lanes (lane = group * P + q) that take every G-th column, so most
-        // lanes work; the groups' sums are added in a fixed order at the end
-        const int P = r <= 8 ? 8 : 16, G = 32 / P;
-        const int g = l / P, q = l - g * P;
+        const int Pl = r <= 8 ? 8 : 16, G = 32 / Pl;
+        const int g = l / Pl, q = l - g * Pl;
         const bool live = q < r;
+        constexpr int U4 = 4;
         cd acc[NC];
 #pragma unroll
         for (int c = 0; c < NC; ++c) acc[c] = cmk(0, 0);
-        constexpr int U4 = 4;
-        int j = vi.y + g;
-        for (; j + (U4 - 1) * G < vi.z; j += U4 * G) {
-            float2 v[U4];
+        float2 v[U4];
 #pragma unroll
-            for (int u = 0; u < U4; ++u)
-                v[u] = live ? V[(int64_t)(j + u * G) * r + q] : make_float2(0.f, 0.f);
-#pragma unroll
-            for (int u = 0; u < U4; ++u)
-#pragma unroll
-                for (int c = 0; c < NC; ++c)
-                    if (c < nc)
-                        acc[c] = cfma(cmk(v[u].x, v[u].y), xc[(int64_t)c * n + j + u * G], acc[c]);
+        for (int u = 0; u < U4; ++u) {
+            const int j = g + u * G;
+            v[u] = (live && j < cnt) ? ld_stream(V + (int64_t)j * r + q) : make_float2(0.f, 0.f);
         }
-        for (; j < vi.z; j += G) {
-            const float2 v = live ? V[(int64_t)j * r + q] : make_float2(0.f, 0.f);
+        cp_wait<0>();
+        __syncwarp();
+        for (int j = g; j < cnt; j += U4 * G) {
+            float2 nx[U4];
 #pragma unroll
-            for (int c = 0; c < NC; ++c)
-                if (c < nc) acc[c] = cfma(cmk(v.x, v.y), xc[(int64_t)c * n + j], acc[c]);
+            for (int u = 0; u < U4; ++u) {
+                const int jj = j + (U4 + u) * G;
+                nx[u] = (live && jj < cnt) ? ld_stream(V + (int64_t)jj * r + q)
+                                           : make_float2(0.f, 0.f);
+            }
+#pragma unroll
+            for (int u = 0; u < U4; ++u) {
+                const int jj = j + u * G;
+                if (jj < cnt) {
+                    const cd vv = cmk(v[u].x, v[u].y);
+#pragma unroll
+                    for (int c = 0; c < NC; ++c)
+                        if (c < nc) acc[c] = cfma(vv, xb[jj * NC + c], acc[c]);
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < U4; ++u) v[u] = nx[u];
         }
-        for (int o = P; o < 32; o <<= 1)
+        for (int o = Pl; o < 32; o <<= 1)
 #pragma unroll
             for (int c = 0; c < NC; ++c) {
                 acc[c].x += __shfl_xor_sync(0xffffffffu, acc[c].x, o);
@@ -314,36 +367,44 @@ __global__ void __launch_bounds__(32 * HM_WPB, 24 / HM_WPB) hm_vtx_kernel(
             }
         if (g == 0 && live)
 #pragma unroll
-            for (int c = 0; c < NC; ++c) out[(int64_t)q * NC + c] = acc[c];
+            for (int c = 0; c < NC; ++c) out[(int64_t)q * 4 + c] = acc[c];
         return;
     }
+    cp_wait<0>();
+    __syncwarp();
+    constexpr int UN = 8;
     for (int q0 = 0; q0 < r; q0 += 32) {
         const int q = q0 + l;
         const bool live = q < r;
         cd acc[NC];
 #pragma unroll
         for (int c = 0; c < NC; ++c) acc[c] = cmk(0, 0);
-        int j = vi.y;
-        for (; j + UN <= vi.z; j += UN) {
-            float2 v[UN];
+        float2 v[UN];
+#pragma unroll
+        for (int u = 0; u < UN; ++u)
+            v[u] = (live && u < cnt) ? ld_stream(V + (int64_t)u * r + q) : make_float2(0.f, 0.f);
+        for (int j = 0; j < cnt; j += UN) {
+            float2 nx[UN];
+#pragma unroll
+            for (int u = 0; u < UN; ++u) {
+                const int jj = j + UN + u;
+                nx[u] = (live && jj < cnt) ? ld_stream(V + (int64_t)jj * r + q)
+                                           : make_float2(0.f, 0.f);
+            }
 #pragma unroll
             for (int u = 0; u < UN; ++u)
-                v[u] = live ? V[(int64_t)(j + u) * r + q] : make_float2(0.f, 0.f);
+                if (j + u < cnt) {
+                    const cd vv = cmk(v[u].x, v[u].y);
 #pragma unroll
-            for (int u = 0; u < UN; ++u)
+                    for (int c = 0; c < NC; ++c)
+                        if (c < nc) acc[c] = cfma(vv, xb[(j + u) * NC + c], acc[c]);
+                }
 #pragma unroll
-                for (int c = 0; c < NC; ++c)
-                    if (c < nc) acc[c] = cfma(cmk(v[u].x, v[u].y), xc[(int64_t)c * n + j + u], acc[c]);
-        }
-        for (; j < vi.z; ++j) {
-            const float2 v = live ? V[(int64_t)j * r + q] : make_float2(0.f, 0.f);
-#pragma unroll
-            for (int c = 0; c < NC; ++c)
-                if (c < nc) acc[c] = cfma(cmk(v.x, v.y), xc[(int64_t)c * n + j], acc[c]);
+            for (int u = 0; u < UN; ++u) v[u] = nx[u];
         }
         if (live)
 #pragma unroll
-            for (int c = 0; c < NC; ++c) out[(int64_t)q * NC + c] = acc[c];
+            for (int c = 0; c < NC; ++c) out[(int64_t)q * 4 + c] = acc[c];
     }
 }
 
@@ -374,93 +435,110 @@ __global__ void __launch_bounds__(256) hm_vtx_reduce_kernel(HMats P, int nc, int
     }
 }
 
-// Row sums in two steps.  Work items: (32-row chunk of a leaf, segment of at
-// most a few entries of the leaf's contribution list); items[i] = (chunk,
-// first entry, end entry), chunks[k] = (leaf, first row offset).  One warp
-// per item, lane = row: the warp sums its entries (entry e >= 0 dense block
-// e, e < 0 low-rank block -e-1) in registers and writes a 32 x NC partial;
+// Row sums in two steps.  Work items (shared by the matrices): (chunk,
+// first entry, end entry, first row within the leaf << 6 | live rows) -- a
+// 32-row piece of a leaf and a segment of at most a few entries of the
+// leaf's contribution list.  One warp per item, lane = row.  The entries'
+// columns are walked in stages of HM_XS: the x values of the next stage
+// (X in cluster order for a dense block, t for a low-rank one) are copied
+// to shared memory asynchronously while the current stage is multiplied, so
+// the only long-latency loads in the inner loop are the streamed matrix
+// columns (prefetched UN at a time).  The warp writes a 32 x NC partial;
 // hm_reduce_kernel adds the partials of each chunk in item order (so the
 // result is deterministic) and scatters the rows to face order.
-template <int NC, int UN>
-__device__ __forceinline__ void rows_accumulate(const float2 *__restrict__ A, int64_t lda, int cnt,
-                                                const cd *__restrict__ B, int64_t bj, int64_t bc,
-                                                bool live, cd (&acc)[NC]) {
-    // acc += sum_j A[j * lda] * B[j * bj + c * bc]   (A per lane, B broadcast).
-    // Software-pipelined: the loads of the next UN columns of A are issued
-    // before the current UN columns are multiplied, so two chunks of the
-    // matrix stream are in flight per lane.
-    const int full = cnt / UN;
-    if (full > 0) {
-        float2 a[UN];
-#pragma unroll
-        for (int u = 0; u < UN; ++u) a[u] = live ? A[(int64_t)u * lda] : make_float2(0.f, 0.f);
-        for (int ch = 0; ch < full; ++ch) {
-            const int j = ch * UN;
-            const bool more = ch + 1 < full;
-            float2 nx[UN];
-#pragma unroll
-            for (int u = 0; u < UN; ++u)
-                nx[u] = (live && more) ? A[(int64_t)(j + UN + u) * lda] : make_float2(0.f, 0.f);
-#pragma unroll
-            for (int u = 0; u < UN; ++u) {
-                const cd av = cmk(a[u].x, a[u].y);
-#pragma unroll
-                for (int c = 0; c < NC; ++c)
-                    acc[c] = cfma(av, B[(int64_t)(j + u) * bj + c * bc], acc[c]);
-            }
-#pragma unroll
-            for (int u = 0; u < UN; ++u) a[u] = nx[u];
-        }
-    }
-    for (int j = full * UN; j < cnt; ++j) {
-        const float2 a = live ? A[(int64_t)j * lda] : make_float2(0.f, 0.f);
-        const cd av = cmk(a.x, a.y);
-#pragma unroll
-        for (int c = 0; c < NC; ++c) acc[c] = cfma(av, B[(int64_t)j * bj + c * bc], acc[c]);
-    }
-}
-
-// Launch-bound occupancy and software-pipelining width of the row sums.
-#ifndef HM_ROWS_MINB
-#define HM_ROWS_MINB 4
-#endif
-#ifndef HM_ROWS_UN
-#define HM_ROWS_UN 4
-#endif
-
 template <int NC>
-__global__ void __launch_bounds__(32 * HM_WPB, HM_ROWS_MINB * 8 / HM_WPB) hm_rows_kernel(HMats P, int n, int nitem,
-                                                         const int4 *__restrict__ items,
-                                                         const int2 *__restrict__ chunks,
-                                                         const int2 *__restrict__ leaf_rows,
-                                                         const int *__restrict__ lent,
-                                                         const int4 *__restrict__ dn,
-                                                         const int4 *__restrict__ lr,
-                                                         cd *__restrict__ partial) {
-    const int it = blockIdx.x * HM_WPB + (threadIdx.x >> 5);
+__global__ void __launch_bounds__(32 * HM_WPB, HM_MINB) hm_rows_kernel(
+    HMats P, int n, int nitem, const int4 *__restrict__ items, cd *__restrict__ partial) {
+    __shared__ __align__(16) cd xsm[HM_WPB][2][HM_XS * NC];
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    const int it = blockIdx.x * HM_WPB + w;
     if (it >= nitem) return;
     const HMat &H = P.h[blockIdx.y];
-    const int l = threadIdx.x & 31;
     const int4 item = items[it];
-    const int2 ch = chunks[item.x];
-    const int2 lf = leaf_rows[ch.x];
-    const bool live = ch.y + l < lf.y;
-    const int row = lf.x + ch.y + l;          // cluster position
+    const int ne = item.z - item.y;           // <= 32 (host cuts the lists)
+    const int r0 = item.w >> 6;
+    const bool live = l < (item.w & 63);
+    // lane q holds the record of entry item.y + q
+    RowEnt mine;
+    mine.a = 0; mine.xo = 0; mine.lda = 0; mine.cnt = 0; mine.kind = 0; mine.pad = 0;
+    if (l < ne) mine = H.rent[item.y + l];
+    const unsigned FULL = 0xffffffffu;
+    // (e, j0): current stage = columns j0 .. j0 + HM_XS of entry e
+    auto advance = [&](int &e, int &j0, int &cnt) -> bool {
+        j0 += HM_XS;
+        if (j0 < cnt) return true;
+        j0 = 0;
+        do {
+            if (++e >= ne) return false;
+            cnt = __shfl_sync(FULL, mine.cnt, e);
+        } while (cnt == 0);
+        return true;
+    };
+    auto stage_x = [&](int e, int j0, int cnt, cd *buf) {
+        const long long xo = __shfl_sync(FULL, mine.xo, e);
+        const int kind = __shfl_sync(FULL, mine.kind, e);
+        const int ncol = min(HM_XS, cnt - j0);
+        if (l < ncol) {
+            if (kind == 0) {
+                const cd *src = H.Xc + xo + j0 + l;
+#pragma unroll
+                for (int c = 0; c < NC; ++c) cp16(buf + l * NC + c, src + (int64_t)c * n);
+            } else {
+                const cd *src = H.T + (xo + j0 + l) * NC;
+#pragma unroll
+                for (int c = 0; c < NC; ++c) cp16(buf + l * NC + c, src + c);
+            }
+        }
+        cp_commit();
+    };
     cd acc[NC];
 #pragma unroll
     for (int c = 0; c < NC; ++c) acc[c] = cmk(0, 0);
-    for (int e = item.y; e < item.z; ++e) {
-        const int id = lent[e];
-        if (id >= 0) {
-            const int4 bk = dn[id];
-            rows_accumulate<NC, HM_ROWS_UN>(H.D + H.offD[id] + (row - bk.x), bk.y, bk.w, H.Xc + bk.z, 1, n,
-                                   live, acc);
-        } else {
-            const int b = -id - 1;
-            const int4 bk = lr[b];
-            rows_accumulate<NC, HM_ROWS_UN>(H.U + H.offU[b] + (row - bk.x), bk.y, H.rank[b],
-                                   H.T + H.offT[b] * NC, NC, 1, live, acc);
+    int e = -1, j0 = 0, cnt = 0, buf = 0;
+    bool have = advance(e, j0, cnt);
+    if (have) stage_x(e, j0, cnt, xsm[w][0]);
+    constexpr int UN = 4;
+    while (have) {
+        int en = e, jn = j0, cn = cnt;
+        const bool more = advance(en, jn, cn);
+        if (more) stage_x(en, jn, cn, xsm[w][buf ^ 1]);
+        else cp_commit();                       // an empty group keeps the count uniform
+        const long long ao = __shfl_sync(FULL, mine.a, e);
+        const int lda = __shfl_sync(FULL, mine.lda, e);
+        const int kind = __shfl_sync(FULL, mine.kind, e);
+        const int ncol = min(HM_XS, cnt - j0);
+        const float2 *A = (kind == 0 ? H.D : H.U) + ao + r0 + l + (int64_t)j0 * lda;
+        float2 a[UN];
+#pragma unroll
+        for (int u = 0; u < UN; ++u)
+            a[u] = (live && u < ncol) ? ld_stream(A + (int64_t)u * lda) : make_float2(0.f, 0.f);
+        cp_wait<1>();
+        __syncwarp();
+        const cd *xb = xsm[w][buf];
+        for (int j = 0; j < ncol; j += UN) {
+            float2 nx[UN];
+#pragma unroll
+            for (int u = 0; u < UN; ++u) {
+                const int jj = j + UN + u;
+                nx[u] = (live && jj < ncol) ? ld_stream(A + (int64_t)jj * lda)
+                                            : make_float2(0.f, 0.f);
+            }
+#pragma unroll
+            for (int u = 0; u < UN; ++u)
+                if (j + u < ncol) {
+                    const cd av = cmk(a[u].x, a[u].y);
+#pragma unroll
+                    for (int c = 0; c < NC; ++c) acc[c] = cfma(av, xb[(j + u) * NC + c], acc[c]);
+                }
+#pragma unroll
+            for (int u = 0; u < UN; ++u) a[u] = nx[u];
         }
+        __syncwarp();                           // stage buffer free for the copy after next
+        buf ^= 1;
+        e = en;
+        j0 = jn;
+        cnt = cn;
+        have = more;
     }
     cd *out = partial + ((int64_t)blockIdx.y * nitem + it) * 32 * 4;
 #pragma unroll
@@ -593,35 +671,35 @@ extern "C" int mnpb_hmat_compact(void *stream, int64_t nblk, const int32_t *bloc
 struct mnpb_hmat_desc {
     const float *D, *U, *V;
     const int32_t *rank;
-    const int64_t *offD, *offU, *offV, *offT;
+    const int64_t *offT;
     const double *X;
     double *Y, *T, *Xc;
     const int64_t *offTP;
     double *TP;
+    const void *rent, *vent;
 };
 
 extern "C" int mnpb_hmat_matvec(void *stream, int64_t n, int64_t nc, int64_t nmat,
-                                const void *descs, const int32_t *c2p, int64_t ndense,
-                                const int32_t *dense, int64_t nlr, const int32_t *lowrank,
-                                int64_t nleaf, const int32_t *leaf_rows, const int32_t *lptr,
-                                const int32_t *lent, int64_t nchunk, const int32_t *chunks,
+                                const void *descs, const int32_t *c2p, int64_t nlr,
+                                int64_t nchunk, const int32_t *chunks, const int32_t *leaf_rows,
                                 int64_t nitem, const int32_t *items, const int32_t *cptr,
-                                double *partial, int64_t nvitem, const int32_t *vitems,
-                                const int32_t *vptr) {
+                                double *partial, int64_t nvitem, const int32_t *vptr) {
     clear_error();
-    MNPB_REQUIRE(n > 0 && nc > 0 && nc <= 64 && nmat >= 1 && nmat <= 4 && nleaf > 0,
+    MNPB_REQUIRE(n > 0 && nc > 0 && nc <= 64 && nmat >= 1 && nmat <= 4 && nchunk > 0 &&
+                     nitem > 0,
                  "hmat_matvec: bad sizes (nc <= 64, nmat <= 4)");
-    MNPB_REQUIRE(descs && c2p && leaf_rows && lptr && lent && chunks && nchunk > 0 && items &&
-                     nitem > 0 && cptr && partial && (nlr == 0 || (vitems && vptr && nvitem > 0)),
+    MNPB_REQUIRE(descs && c2p && leaf_rows && chunks && items && cptr && partial &&
+                     (nlr == 0 || (vptr && nvitem > 0)),
                  "hmat_matvec: null pointer");
     cudaStream_t s = as_stream(stream);
     const mnpb_hmat_desc *d = (const mnpb_hmat_desc *)descs;
     hm::HMats P;
     for (int q = 0; q < 4; ++q) {
         const mnpb_hmat_desc &e = d[q < nmat ? q : 0];
+        MNPB_REQUIRE(e.rent && (nlr == 0 || e.vent), "hmat_matvec: missing work records");
         P.h[q] = hm::HMat{(const float2 *)e.D, (const float2 *)e.U, (const float2 *)e.V, e.rank,
-                          e.offD, e.offU, e.offV, e.offT, (const cd *)e.X, (cd *)e.Y, (cd *)e.T,
-                          (cd *)e.Xc, e.offTP, (cd *)e.TP};
+                          e.offT, (const cd *)e.X, (cd *)e.Y, (cd *)e.T, (cd *)e.Xc, e.offTP,
+                          (cd *)e.TP, (const hm::RowEnt *)e.rent, (const hm::VtxEnt *)e.vent};
     }
     ProfScope ps(s, PC_HMATVEC, 0.0);
     // columns in chunks of at most 4 (register bound of the kernels); T
@@ -638,8 +716,7 @@ extern "C" int mnpb_hmat_matvec(void *stream, int64_t n, int64_t nc, int64_t nma
         MNPB_LAUNCH_CHECK("hm permute_kernel");
         if (nlr > 0) {
             dim3 g((unsigned)ceil_div(nvitem, HM_WPB), (unsigned)nmat);
-            hm::hm_vtx_kernel<4><<<g, 32 * HM_WPB, 0, s>>>(Q, (int)n, ncc, (int)nvitem,
-                                                   (const int4 *)vitems, (const int4 *)lowrank);
+            hm::hm_vtx_kernel<4><<<g, 32 * HM_WPB, 0, s>>>(Q, (int)n, ncc, (int)nvitem);
             MNPB_LAUNCH_CHECK("hm_vtx_kernel");
             dim3 gr((unsigned)ceil_div(nlr, 8), (unsigned)nmat);
             hm::hm_vtx_reduce_kernel<4><<<gr, 256, 0, s>>>(Q, ncc, (int)nlr, vptr);
@@ -648,10 +725,8 @@ extern "C" int mnpb_hmat_matvec(void *stream, int64_t n, int64_t nc, int64_t nma
         dim3 g((unsigned)ceil_div(nitem, HM_WPB), (unsigned)nmat);
         dim3 gr((unsigned)ceil_div(nchunk, 8), (unsigned)nmat);
 #define MNPB_HM_ROWS(NCV)                                                                       \
-    hm::hm_rows_kernel<NCV><<<g, 32 * HM_WPB, 0, s>>>(Q, (int)n, (int)nitem, (const int4 *)items,       \
-                                              (const int2 *)chunks, (const int2 *)leaf_rows,    \
-                                              lent, (const int4 *)dense, (const int4 *)lowrank, \
-                                              (cd *)partial);                                   \
+    hm::hm_rows_kernel<NCV><<<g, 32 * HM_WPB, 0, s>>>(Q, (int)n, (int)nitem,                     \
+                                                     (const int4 *)items, (cd *)partial);        \
     hm::hm_reduce_kernel<NCV><<<gr, 256, 0, s>>>(Q, (int)n, NCV, (int)nchunk, (int)nitem, cptr,  \
                                                  (const int2 *)chunks, (const int2 *)leaf_rows,  \
                                                  c2p, (const cd *)partial)

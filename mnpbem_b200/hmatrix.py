@@ -75,27 +75,30 @@ class HTopology(object):
                     lists[L].append(code)
         lptr = np.zeros(self.nleaf + 1, dtype=np.int64)
         lptr[1:] = np.cumsum([len(x) for x in lists])
-        self.lptr = _i32(lptr, device)
         ent = np.concatenate([np.asarray(x, dtype=np.int32) for x in lists]) if lptr[-1] else \
             np.zeros(1, np.int32)
-        self.lent = _i32(ent, device)
+        self.lent_h = ent
+        self.lent_leaf = np.repeat(np.arange(self.nleaf), np.diff(lptr)).astype(np.int64)
+        self.lstart_h = np.asarray(lstart, dtype=np.int64)
         # 32-row chunks of the leaves, and work items (chunk, segment of at
-        # most SEG entries of the leaf's list): one warp per item
+        # most SEG entries of the leaf's list, first row << 6 | rows): one
+        # warp per item
         SEG = 6
         ch, items, cptr = [], [], [0]
         for L in range(self.nleaf):
             for r0 in range(0, int(lsize[L]), 32):
                 k = len(ch)
                 ch.append((L, r0))
+                rows = (r0 << 6) | min(32, int(lsize[L]) - r0)
                 for e in range(int(lptr[L]), int(lptr[L + 1]), SEG):
-                    items.append((k, e, min(e + SEG, int(lptr[L + 1])), 0))
+                    items.append((k, e, min(e + SEG, int(lptr[L + 1])), rows))
                 if lptr[L + 1] == lptr[L]:
-                    items.append((k, 0, 0, 0))
+                    items.append((k, 0, 0, rows))
                 cptr.append(len(items))
         self.nchunk = len(ch)
         self.chunks = _i32(np.asarray(ch, dtype=np.int64).reshape(-1, 2), device)
         # V^T x work items: (block, first column, end column, segment)
-        VSEG = 128
+        VSEG = 64
         vit, vptr = [], [0]
         for b in range(self.nlr):
             ncol = int(lr[b, 3])
@@ -104,12 +107,67 @@ class HTopology(object):
             vptr.append(len(vit))
         self.vseg_count = np.diff(np.asarray(vptr, dtype=np.int64))
         self.nvitem = max(1, len(vit))
-        self.vitems = _i32(np.asarray(vit if vit else [(0, 0, 0, 0)], dtype=np.int64).reshape(-1, 4),
-                           device)
+        self.vitems_h = np.asarray(vit if vit else [(0, 0, 0, 0)], dtype=np.int64).reshape(-1, 4)
         self.vptr = _i32(np.asarray(vptr, dtype=np.int64), device)
         self.nitem = len(items)
+        assert max(it[2] - it[1] for it in items) <= 32    # records held one per lane
         self.items = _i32(np.asarray(items, dtype=np.int64).reshape(-1, 4), device)
         self.cptr = _i32(np.asarray(cptr, dtype=np.int64), device)
+
+
+# work records of the product kernels (layouts of the C ABI's rent / vent)
+ROW_ENT = np.dtype([('a', '<i8'), ('xo', '<i8'), ('lda', '<i4'), ('cnt', '<i4'),
+                    ('kind', '<i4'), ('pad', '<i4')])
+VTX_ENT = np.dtype([('v', '<i8'), ('out', '<i8'), ('xo', '<i4'), ('cnt', '<i4'),
+                    ('r', '<i4'), ('pad', '<i4')])
+
+
+def _records(rec, dev):
+    return torch.from_numpy(np.frombuffer(rec.tobytes(), dtype=np.uint8).copy()).to(dev)
+
+
+def row_records(topo, rank, offU, offT):
+    """One ROW_ENT per entry of the leaves' contribution lists: where the
+    leaf's rows of the entry's dense block (or low-rank factor U) start, its
+    column stride and column count, and where its x (or t) columns are."""
+    code = topo.lent_h[:len(topo.lent_leaf)].astype(np.int64)
+    lst = topo.lstart_h[topo.lent_leaf]
+    rec = np.zeros(max(1, code.size), dtype=ROW_ENT)
+    dn, lr = topo.part.dense, topo.part.lowrank
+    d = code >= 0
+    if d.any():
+        bk = dn[code[d]].astype(np.int64)
+        rec['a'][:code.size][d] = topo.offD_h[code[d]] + lst[d] - bk[:, 0]
+        rec['lda'][:code.size][d] = bk[:, 1]
+        rec['cnt'][:code.size][d] = bk[:, 3]
+        rec['xo'][:code.size][d] = bk[:, 2]
+    q = ~d
+    if q.any():
+        b = -code[q] - 1
+        bk = lr[b].astype(np.int64)
+        rec['a'][:code.size][q] = offU[b] + lst[q] - bk[:, 0]
+        rec['lda'][:code.size][q] = bk[:, 1]
+        rec['cnt'][:code.size][q] = rank[b]
+        rec['xo'][:code.size][q] = offT[b]
+        rec['kind'][:code.size][q] = 1
+    return rec
+
+
+def vtx_records(topo, rank, offV, offTP):
+    """One VTX_ENT per V^T x item (a segment of one low-rank block)."""
+    vi = topo.vitems_h
+    rec = np.zeros(vi.shape[0], dtype=VTX_ENT)
+    if topo.nlr:
+        b, j0, j1, sg = vi[:, 0], vi[:, 1], vi[:, 2], vi[:, 3]
+        if (j1 - j0).max() > 64:
+            raise ValueError("vtx_records: segments of at most 64 columns (kernel staging)")
+        r = rank[b]
+        rec['v'] = offV[b] + j0 * r
+        rec['out'] = offTP[b] + sg * r
+        rec['xo'] = topo.part.lowrank[b, 2].astype(np.int64) + j0
+        rec['cnt'] = j1 - j0
+        rec['r'] = r
+    return rec
 
 
 class HMatrixGPU(object):
@@ -154,6 +212,8 @@ class HMatrixGPU(object):
             call('mnpb_hmat_compact', sh, topo.nlr, ptr(topo.lowrank), ptr(self.rank),
                  ptr(topo.scr_offU), ptr(topo.scr_offV), ptr(scratch), ptr(self.offU),
                  ptr(self.offV), ptr(self.U), ptr(self.V))
+            self.rent = _records(row_records(topo, rank, offU, offT), dev)
+            self.vent = _records(vtx_records(topo, rank, offV, offTP), dev)
         else:
             self.rank_h = np.zeros(0, np.int64)
             z = _i64(np.zeros(1), dev)
@@ -161,6 +221,9 @@ class HMatrixGPU(object):
             self.tp_entries = 0
             self.U = self.V = torch.empty(2, dtype=torch.float32, device=dev)
             self.sum_rank = 0
+            zr = np.zeros(0, np.int64)
+            self.rent = _records(row_records(topo, zr, zr, zr), dev)
+            self.vent = _records(vtx_records(topo, zr, zr, zr), dev)
         self.scratch = scratch
 
     def stored_bytes(self):
@@ -199,7 +262,7 @@ def hmat_matvec(hms, xs, ys, nc, stream=None):
     partial = torch.empty(len(hms) * topo.nitem * 32 * 4 * 2, dtype=torch.float64, device=dev)
     ptp = 2 * 4 * max(1, max(h.tp_entries for h in hms))
     TP = torch.empty(ptp * len(hms), dtype=torch.float64, device=dev)
-    desc = np.zeros((len(hms), 14), dtype=np.uint64)
+    desc = np.zeros((len(hms), 13), dtype=np.uint64)
     keep = []
     for i, (h, x, y) in enumerate(zip(hms, xs, ys)):
         if h.topo is not topo:
@@ -208,13 +271,12 @@ def hmat_matvec(hms, xs, ys, nc, stream=None):
                 or not y.is_contiguous() or x.numel() < n * nc or y.numel() < n * nc:
             raise ValueError("hmat_matvec: x, y must be contiguous complex128 (nc, n)")
         desc[i] = [h.D.data_ptr(), h.U.data_ptr(), h.V.data_ptr(), h.rank.data_ptr(),
-                   topo.offD.data_ptr(), h.offU.data_ptr(), h.offV.data_ptr(),
                    h.offT.data_ptr(), x.data_ptr(), y.data_ptr(), T[i * per:].data_ptr(),
-                   Xc[i * pxc:].data_ptr(), h.offTP.data_ptr(), TP[i * ptp:].data_ptr()]
+                   Xc[i * pxc:].data_ptr(), h.offTP.data_ptr(), TP[i * ptp:].data_ptr(),
+                   h.rent.data_ptr(), h.vent.data_ptr()]
         keep.append((x, y))
     call('mnpb_hmat_matvec', _lib.stream_handle(stream), n, nc, len(hms), ptr(desc),
-         ptr(topo.c2p), topo.ndense, ptr(topo.dense), topo.nlr, ptr(topo.lowrank), topo.nleaf,
-         ptr(topo.leaf_rows), ptr(topo.lptr), ptr(topo.lent), topo.nchunk, ptr(topo.chunks),
+         ptr(topo.c2p), topo.nlr, topo.nchunk, ptr(topo.chunks), ptr(topo.leaf_rows),
          topo.nitem, ptr(topo.items), ptr(topo.cptr), ptr(partial), topo.nvitem,
-         ptr(topo.vitems), ptr(topo.vptr))
+         ptr(topo.vptr))
     return ys
