@@ -64,7 +64,7 @@ def parse():
     ap.add_argument('--prof-dump', default=None, help='CSV of every timed launch')
     ap.add_argument('--no-iterative', action='store_true',
                     help='skip the H-matrix / GMRES measurement on the 25k-face rod')
-    ap.add_argument('--iter-nlam', type=int, default=6)
+    ap.add_argument('--iter-nlam', type=int, default=12)
     ap.add_argument('--probe', default=None,
                     choices=['tc_gemm', 'tc_gemm_packed', 'assemble', 'solve', 'hmat', 'lu'],
                     help='run one representative kernel on a small case (profiling target) '
@@ -225,7 +225,9 @@ ITER_WORKLOAD = ("BEMRetIter H-matrix sweep: trirod(20 nm, 80 nm, [97, 47, 171])
 def iterative_section(args):
     """Solves/s, operator applications, ACA time and H-matrix product
     bandwidth of the iterative path on the 25k-face rod (a short sweep of
-    the 201-wavelength grid, zero-start and extrapolated-start GMRES)."""
+    the 201-wavelength grid): GMRES from a zero start (the reference's),
+    from quadratic extrapolation and from the learned warm start, each of the
+    last two with and without GCRO augmentation by the last 3 solutions."""
     import torch
     import mnpbem_b200 as M
     from mnpbem_b200 import _lib
@@ -242,13 +244,37 @@ def iterative_section(args):
     torch.cuda.synchronize()
     ctor = time.time() - t0
     out = {"workload": ITER_WORKLOAD, "n_faces": cp.n, "constructor_s": ctor}
-    for mode, warm in (("zero_start", None), ("extrapolated_start", "extrapolate")):
+    # the learned warm start: trained on FP64 dense sweeps of two coarse meshes
+    # of the same 20 x 80 nm rod (1000 and 2400 faces, 480-540 nm), applied
+    # to the 25k-face sweep
+    from mnpbem_b200.learned import LearnedWarmStart
+    t0 = time.time()
+    learner = LearnedWarmStart(seed=0)
+    train_lams = list(480.0 + 2.5 * np.arange(25))
+    for dims in ((21, 11, 31), (31, 21, 41)):
+        cpc = M.ComParticle([M.EpsConst(1.0), M.EpsDrude(*DRUDE)],
+                            [M.trirod(20.0, 80.0, dims)], [[2, 1]], 1)
+        learner.add_dense_sweep(cpc, exc, train_lams)
+    learner.fit()
+    torch.cuda.synchronize()
+    train_s = time.time() - t0
+    t0 = time.time()
+    learner.prepare(cp)                         # per-geometry setup (surface modes)
+    torch.cuda.synchronize()
+    out["learned_training"] = {
+        "data": "FP64 dense sweeps of trirod(20, 80, [21, 11, 31]) and [31, 21, 41] (1000 and "
+                "2400 faces), 25 wavelengths 480-540 nm each",
+        "seconds": train_s, "geometry_setup_s": time.time() - t0}
+    modes = (("zero_start", None, False), ("extrapolated_start", "extrapolate", False),
+             ("extrapolated_deflated", "extrapolate", 3), ("learned_start", learner, False),
+             ("learned_deflated", learner, 3))
+    for mode, warm, defl in modes:
         bem.enei = None
         _lib.prof_begin()
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
-        sols, stats, _ = bem.solve_spectrum(exc, eneis, warm=warm)
+        sols, stats, _ = bem.solve_spectrum(exc, eneis, warm=warm, deflate=defl)
         e1.record()
         torch.cuda.synchronize()
         prof = _lib.prof_end()
@@ -692,7 +718,12 @@ def main():
         gathered = int(np.isfinite(spec).all(axis=1).sum())
     value = world * NLAM * args.steps / (ms / 1000.0)
 
-    # end to end through the public API with host buffers
+    # end to end through the public API with host buffers, after the same
+    # warm-up sweeps (they also fill the pinned-memory cache the result
+    # copies come back through: two sets, since a sweep's results are still
+    # held while the next one is copied)
+    for _ in range(args.warmup):
+        sols = solver.solve_spectrum(exc, eneis, batch=B, streams=args.streams)
     torch.cuda.synchronize()
     t0 = time.time()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)

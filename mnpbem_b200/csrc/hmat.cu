@@ -269,13 +269,18 @@ struct HMats {
 
 // Warps per block of the product kernels (one work item per warp) and the
 // launch-bound block count per SM.  Measured on the four matrices of the
-// 25,152-face rod (4 right-hand sides): 4 warps x >= 4 blocks 1.05 ms per
-// product, 8 x 3 1.06 ms, 8 x 4 (64 registers, spills) 1.24 ms.
+// 25,152-face rod (4 right-hand sides): 4 warps x >= 6 blocks 0.971 ms per
+// product, 4 x 4 1.05 ms, 8 x 3 1.06 ms, 8 x 4 (64 registers, spills)
+// 1.24 ms, 4 x 6 with 2 columns in flight 1.18 ms.
 #ifndef HM_WPB
 #define HM_WPB 4
 #endif
 #ifndef HM_MINB
-#define HM_MINB 4
+#define HM_MINB 6
+#endif
+// Matrix columns in flight per lane in the row sums (software pipeline depth).
+#ifndef HM_RUN
+#define HM_RUN 4
 #endif
 constexpr int HM_VSEG = 64;      // columns per V^T x item (the host cuts segments this long)
 constexpr int HM_XS = 32;        // x columns per shared-memory stage of the row sums
@@ -497,7 +502,7 @@ __global__ void __launch_bounds__(32 * HM_WPB, HM_MINB) hm_rows_kernel(
     int e = -1, j0 = 0, cnt = 0, buf = 0;
     bool have = advance(e, j0, cnt);
     if (have) stage_x(e, j0, cnt, xsm[w][0]);
-    constexpr int UN = 4;
+    constexpr int UN = HM_RUN;
     while (have) {
         int en = e, jn = j0, cn = cnt;
         const bool more = advance(en, jn, cn);

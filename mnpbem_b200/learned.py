@@ -331,6 +331,13 @@ class LearnedWarmStart(object):
         return losses
 
     # ------------------------------------------------------------ inference
+    def prepare(self, p):
+        """Per-geometry setup of ``p`` (its smooth surface modes), done by the
+        first prediction otherwise."""
+        if self.smooth_modes > 0 and id(p) not in self._modes:
+            self._modes[id(p)] = (p, surface_modes(p, self.smooth_modes, self.device))
+        return self
+
     def predict(self, p, eneis3, hist, K=1, geo=None):
         """Predicted packed solution at eneis3[0] from hist = (x_{i-1},
         x_{i-2}, x_{i-3})."""

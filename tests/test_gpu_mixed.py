@@ -62,6 +62,51 @@ def test_getrf_getrs_c32p(gpu_ok, n, batch, nrhs):
     assert err < 1e-2, err
 
 
+@pytest.mark.parametrize('n,batch', [(700, 2), (200, 150), (2884, 2)])
+def test_getrf_c32p_pivoting(gpu_ok, n, batch):
+    """Random complex matrices without a dominant diagonal, so partial
+    pivoting moves rows at almost every step (the shared-memory slab leaves
+    of 8 columns, of 4 columns for batches above the SM count, and the full
+    2884-row leaf height): P A = L U to TF32 accuracy (relative to |L||U|),
+    every multiplier |l_ij| <= sqrt(2) (pivots maximise |re| + |im|), and
+    the pivot indices form a permutation."""
+    ld = (n + 3) // 4 * 4
+    g = torch.Generator().manual_seed(11 + n)
+    Ac = (torch.randn((batch, n, n), generator=g, dtype=torch.float64) +
+          1j * torch.randn((batch, n, n), generator=g, dtype=torch.float64))
+    A = torch.zeros((batch, 2, n, ld), dtype=torch.float32)
+    A[:, 0, :, :n] = Ac.real.transpose(1, 2).float()
+    A[:, 1, :, :n] = Ac.imag.transpose(1, 2).float()
+    A = A.cuda()
+    piv = torch.zeros((batch, n), dtype=torch.int32, device='cuda')
+    info = torch.zeros(batch, dtype=torch.int32, device='cuda')
+    wb = int(_lib.lib().mnpb_f32_workspace(n, batch))
+    work = torch.empty(wb, dtype=torch.uint8, device='cuda')
+    call('mnpb_getrf_c32p', _lib.stream_handle(), n, batch, ptr(A), ld, n * ld, 2 * n * ld,
+         ptr(piv), n, ptr(info), ptr(work), wb)
+    torch.cuda.synchronize()
+    assert info.sum().item() == 0
+    F = (A[:, 0, :, :n].double() + 1j * A[:, 1, :, :n].double()).transpose(1, 2).cpu()
+    pv = piv.cpu().numpy()
+    for b in list(range(min(batch, 3))) + [batch - 1]:
+        L = torch.tril(F[b], -1) + torch.eye(n, dtype=F.dtype)
+        U = torch.triu(F[b])
+        assert L.abs().max().item() <= 2 ** 0.5 * (1 + 1e-3)
+        perm = np.arange(n)
+        for c in range(n):
+            p = int(pv[b, c])
+            assert c <= p < n
+            perm[[c, p]] = perm[[p, c]]
+        assert sorted(perm.tolist()) == list(range(n))
+        PA = Ac[b][torch.from_numpy(perm)]
+        # backward error against |L||U| (TF32 storage of the factors alone
+        # gives ~1e-5 here; a wrong interchange gives O(1))
+        err = (torch.linalg.norm(PA - L @ U) / torch.linalg.norm(L.abs() @ U.abs())).item()
+        assert err < 1e-3, (b, err)
+        moved = int((pv[b] != np.arange(n)).sum())
+        assert moved > n // 2, moved
+
+
 @pytest.fixture(scope='module')
 def tiny():
     cp, s = _cp('trisphere_32_10')
