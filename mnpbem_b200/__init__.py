@@ -11,7 +11,7 @@ fallback: importing the solvers requires the built library.
 from .compstruct import CompStruct
 from .geometry import Particle, ComParticle, trisphere, trirod, load_mesh
 from .clustertree import ClusterTree
-from .materials import EpsConst, EpsDrude
+from .materials import EpsConst, EpsDrude, EpsTable
 
 __version__ = "1.0.0"
 

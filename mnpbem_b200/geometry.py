@@ -207,6 +207,55 @@ class Particle(object):
         is_tri = np.isnan(f[:, 3])
         return np.where(is_tri)[0], np.where(~is_tri)[0]
 
+    # ---- interpolation mode ------------------------------------------------
+    def flat(self):
+        """Flat boundary elements (mnpbem/geometry/particle.py:1745)."""
+        self.interp = 'flat'
+        self._norm()
+        return self
+
+    def curved(self):
+        """Curved boundary elements (particle.py:1755).  A particle without
+        midpoint vertices gets the straight-edge midpoints and, for
+        quadrilaterals, the corner mean as centre node (the reference's
+        ``midpoints('flat')``)."""
+        if self.verts2 is None:
+            self._flat_midpoints()
+        self.interp = 'curv'
+        self._norm()
+        return self
+
+    def _flat_midpoints(self):
+        n = self.nverts
+        ind3, ind4 = self.index34()
+        f = self.faces
+        # edges (k, k+1) of every face, triangles (0,1), (1,2), (2,0) and
+        # quadrilaterals (0,1), (1,2), (2,3), (3,0): one midpoint per distinct edge
+        ends = []
+        for k in range(4):
+            a = f[:, k]
+            b = np.where(np.isnan(f[:, 3]) & (k == 2), f[:, 0], f[:, (k + 1) % 4])
+            ends.append(np.column_stack([a, b]))
+        e = np.stack(ends, axis=1)                        # (nfaces, 4, 2)
+        valid = ~np.isnan(e[..., 0]) & ~np.isnan(e[..., 1])
+        valid[ind3, 3] = False
+        key = np.sort(e[valid].astype(np.int64), axis=1)
+        uniq, inv = np.unique(key, axis=0, return_inverse=True)
+        mid = 0.5 * (self.verts[uniq[:, 0]] + self.verts[uniq[:, 1]])
+        faces2 = np.full((self.nfaces, 9), np.nan)
+        faces2[:, :4] = f
+        cols = np.full(e.shape[:2], np.nan)
+        cols[valid] = n + inv.reshape(-1)
+        faces2[:, 4:8] = cols
+        verts2 = np.vstack([self.verts, mid])
+        if len(ind4) > 0:
+            f4 = f[ind4].astype(int)
+            cen = 0.25 * (self.verts[f4[:, 0]] + self.verts[f4[:, 1]] + self.verts[f4[:, 2]] +
+                          self.verts[f4[:, 3]])
+            faces2[ind4, 8] = verts2.shape[0] + np.arange(len(ind4))
+            verts2 = np.vstack([verts2, cen])
+        self.verts2, self.faces2 = verts2, faces2
+
     # ---- normals, centroids, areas ----------------------------------------
     def _norm(self):
         if self.interp == 'flat':
@@ -501,11 +550,24 @@ class ComParticle(object):
     Mirrors mnpbem/geometry/comparticle.py:55-127.
     """
 
-    def __init__(self, eps, particles, inout, *closed):
+    def __init__(self, eps, particles, inout, *closed, **options):
         if eps is None or particles is None or inout is None:
             raise ValueError("ComParticle: eps, particles and inout are required")
         self.eps = list(eps)
         self.p = list(particles) if isinstance(particles, (list, tuple)) else [particles]
+        # particle options, applied to the given particles as the reference
+        # does (comparticle.py:129-163): interp 'curv' / 'flat', quadrature
+        # rule and npol
+        unknown = set(options) - {'interp', 'rule', 'npol'}
+        if unknown:
+            raise TypeError("ComParticle: unsupported options {}".format(sorted(unknown)))
+        if 'rule' in options or 'npol' in options:
+            for q in self.p:
+                q.quad_rules = QuadRules(rule=options.get('rule', 18),
+                                         npol=options.get('npol', (7, 5)))
+        if 'interp' in options:
+            for q in self.p:
+                q.curved() if options['interp'] == 'curv' else q.flat()
         inout = np.atleast_2d(np.asarray(inout, dtype=int))
         if inout.shape != (len(self.p), 2):
             raise ValueError("ComParticle: inout must have one [in, out] row per particle")
@@ -618,8 +680,10 @@ class ComParticle(object):
 _MESH_CACHE = {}
 
 
-def load_mesh(name):
-    """Load a packaged mesh ``(verts, faces)`` by name from ``data/meshes.npz``.
+def load_mesh(name, second=False):
+    """Load a packaged mesh ``(verts, faces)`` by name from ``data/meshes.npz``
+    (``second``: the separately stored midpoint mesh ``(verts2, faces2)`` of a
+    flat particle).
 
     The packaged meshes are the reference's own mesh-generator outputs
     (curved meshes are stored with their midpoint vertices), written by
@@ -631,9 +695,10 @@ def load_mesh(name):
         with np.load(path) as z:
             for k in z.files:
                 _MESH_CACHE[k] = z[k]
-    if name + '_verts' not in _MESH_CACHE:
+    suf = '2' if second else ''
+    if name + '_verts' + suf not in _MESH_CACHE:
         raise KeyError("no packaged mesh named {!r}".format(name))
-    return _MESH_CACHE[name + '_verts'], _MESH_CACHE[name + '_faces']
+    return _MESH_CACHE[name + '_verts' + suf], _MESH_CACHE[name + '_faces' + suf]
 
 
 def trisphere(n, diameter, interp='curv'):
@@ -659,11 +724,18 @@ def trirod(diameter, height, n):
     the reference's ``trirod(diameter, height, n)`` (mnpbem/geometry/
     mesh_generators.py:592).  Packaged parameter sets are the reference's
     output itself; others are built by ``rod_mesh``."""
+    key = 'trirod_{:g}_{:g}_{}_{}_{}'.format(float(diameter), float(height), *n)
     try:
-        v, f = load_mesh('trirod_{:g}_{:g}_{}_{}_{}'.format(float(diameter), float(height), *n))
+        v, f = load_mesh(key)
     except KeyError:
-        v, f = rod_mesh(diameter, height, n)
-    return Particle(v, f, interp='flat')
+        return Particle(*rod_mesh(diameter, height, n), interp='flat')
+    p = Particle(v, f, interp='flat')
+    try:
+        # the reference's midpoint mesh on the rod surface, for curved()
+        p.verts2, p.faces2 = load_mesh(key, second=True)
+    except KeyError:
+        pass
+    return p
 
 
 def rod_mesh(diameter, height, n=(15, 20, 20)):

@@ -12,8 +12,11 @@ a ready surface mesh as input; mesh generation is not part of it):
   curved midpoint vertices (``verts2``/``faces2``, 9 face columns); also
   unit-diameter spheres of several n, which other diameters scale.  The
   underlying point sets are the reference's ``mnpbem/data/sphere*_tri.bin``.
-* ``trirod(d, h, n)`` -- mnpbem/geometry/mesh_generators.py:592 (flat quads +
-  triangles).
+* ``trirod(d, h, n)`` -- mnpbem/geometry/mesh_generators.py:592 (quads +
+  triangles): the flat mesh (``verts``/``faces``) and, separately, its
+  midpoint mesh on the rod surface (``verts2``/``faces2``, which carries its
+  own copies of the corner vertices) that ``ComParticle(..., interp='curv')``
+  uses.
 * ``pinfty256`` -- the far-field integration sphere of
   mnpbem/spectrum/spectrum_ret.py:14 (``mnpbem/data/pinfty256.bin``): unit
   directions and their solid-angle weights.
@@ -32,7 +35,8 @@ DATA = os.path.join(HERE, '..', '..', 'mnpbem_b200', 'data')
 SPHERES = [(32, 10.0), (60, 10.0), (144, 10.0), (144, 20.0), (256, 20.0), (1444, 40.0)]
 # unit-diameter spheres: trisphere(n, D) for other diameters scales these
 UNIT_SPHERES = (144, 256, 400, 576, 784, 1024, 1225)
-RODS = [(20.0, 80.0, (31, 21, 41)), (20.0, 80.0, (61, 31, 101)), (20.0, 80.0, (97, 47, 171))]
+RODS = [(20.0, 80.0, (31, 21, 41)), (20.0, 80.0, (61, 31, 101)), (20.0, 80.0, (97, 47, 171)),
+        (10.0, 40.0, (15, 15, 15))]
 
 
 def main(ref_root):
@@ -57,6 +61,8 @@ def main(ref_root):
         key = 'trirod_{:g}_{:g}_{}_{}_{}'.format(d, h, *n)
         out[key + '_verts'] = np.asarray(p.verts, dtype=np.float64)
         out[key + '_faces'] = np.asarray(p.faces, dtype=np.float64)
+        out[key + '_verts2'] = np.asarray(p.verts2, dtype=np.float64)
+        out[key + '_faces2'] = np.asarray(p.faces2, dtype=np.float64)
     pin = _load_pinfty_default()
     out['pinfty256_nvec'] = np.asarray(pin.nvec, dtype=np.float64)
     out['pinfty256_area'] = np.asarray(pin.area, dtype=np.float64)
