@@ -171,7 +171,6 @@ __global__ void __launch_bounds__(SLAB_THREADS, SW == 4 ? 2 : 1) panel_slab_kern
     __shared__ float red_v[SLAB_THREADS / 32];
     __shared__ int red_i[SLAB_THREADS / 32];
     __shared__ cf u12[SW][TS];
-    __shared__ int s_piv;
     __shared__ int slab_piv[SW];   // local pivot row of each slab column
     __shared__ int sw_dst[2 * SW], sw_src[2 * SW], sw_n;   // the slab's composed interchanges
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
@@ -236,6 +235,12 @@ __global__ void __launch_bounds__(SLAB_THREADS, SW == 4 ? 2 : 1) panel_slab_kern
                 if (ov > best || (ov == best && oi < bi)) { best = ov; bi = oi; }
             }
             if (lane == 0) { red_v[wid] = best; red_i[wid] = bi; }
+            // two barriers per step: (A) the partial maxima are visible and
+            // every row update of the previous step is done; warp 0 then
+            // picks the pivot and, one lane per slab column, swaps the pivot
+            // row into place and stores its U entries as TF32; (B) the pivot
+            // row is ready for the update.  The update's end needs no barrier
+            // of its own: the next step's (A) follows it
             __syncthreads();
             if (wid == 0) {
                 best = (lane < SLAB_THREADS / 32) ? red_v[lane] : -1.f;
@@ -246,35 +251,28 @@ __global__ void __launch_bounds__(SLAB_THREADS, SW == 4 ? 2 : 1) panel_slab_kern
                     const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
                     if (ov > best || (ov == best && oi < bi)) { best = ov; bi = oi; }
                 }
+                // every lane holds the same (best, bi) after the butterfly
+                const int ip = (best > 0.f) ? bi : jj;
                 if (lane == 0) {
-                    int ip = bi;
-                    if (!(best > 0.f)) {
-                        ip = jj;
-                        if (info && info[b] == 0) info[b] = c + 1;
-                    }
-                    s_piv = ip;
+                    if (!(best > 0.f) && info && info[b] == 0) info[b] = c + 1;
                     slab_piv[jj] = ip;
                     ipiv[c] = cs + ip;
                 }
-            }
-            __syncthreads();
-            const int ip = s_piv;
-            if (ip != jj) {
-                for (int j = tid; j < SW; j += SLAB_THREADS) {
-                    float t = sre[j * mmax + jj];
-                    sre[j * mmax + jj] = sre[j * mmax + ip];
-                    sre[j * mmax + ip] = t;
-                    t = sim[j * mmax + jj];
-                    sim[j * mmax + jj] = sim[j * mmax + ip];
-                    sim[j * mmax + ip] = t;
+                if (lane < SW) {
+                    const int j = lane;
+                    if (ip != jj) {
+                        float t = sre[j * mmax + jj];
+                        sre[j * mmax + jj] = sre[j * mmax + ip];
+                        sre[j * mmax + ip] = t;
+                        t = sim[j * mmax + jj];
+                        sim[j * mmax + jj] = sim[j * mmax + ip];
+                        sim[j * mmax + ip] = t;
+                    }
+                    if (j >= jj) {
+                        sre[j * mmax + jj] = tf32_rna(sre[j * mmax + jj]);
+                        sim[j * mmax + jj] = tf32_rna(sim[j * mmax + jj]);
+                    }
                 }
-            }
-            // the pivot row's U entries are final: store them as TF32 (same
-            // thread per column as the swap above)
-            for (int j = tid; j < SW; j += SLAB_THREADS) {
-                if (j < jj) continue;
-                sre[j * mmax + jj] = tf32_rna(sre[j * mmax + jj]);
-                sim[j * mmax + jj] = tf32_rna(sim[j * mmax + jj]);
             }
             __syncthreads();
             const cf pv = fmk(sre[jj * mmax + jj], sim[jj * mmax + jj]);
@@ -297,8 +295,8 @@ __global__ void __launch_bounds__(SLAB_THREADS, SW == 4 ? 2 : 1) panel_slab_kern
                     }
                 }
             }
-            __syncthreads();
         }
+        __syncthreads();
         {
             float *dst = A + (int64_t)cs * lda + cs;
             for (int i = tid; i < ms; i += SLAB_THREADS)
