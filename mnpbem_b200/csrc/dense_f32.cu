@@ -607,6 +607,7 @@ __global__ void __launch_bounds__(128) trsm_small_kernel(int mode, int kb, const
 // column-major, leading dimension 128).
 constexpr int TL = 128;
 constexpr int TINV_THREADS = 512;
+constexpr int TINV_CPW = 4;      // columns a warp inverts together
 
 
 __global__ void __launch_bounds__(TINV_THREADS) tri_inv_kernel(int n, int lower, const float *A,
@@ -637,47 +638,73 @@ __global__ void __launch_bounds__(TINV_THREADS) tri_inv_kernel(int n, int lower,
     __syncthreads();
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     float *ob = out + ((b * nb + blk) * 2) * TL * TL;
-    for (int j = w; j < TL; j += TINV_THREADS / 32) {
-        cf x[4];
+    // Each warp solves two groups of TINV_CPW consecutive columns, group g
+    // paired with group (TL / TINV_CPW - 1 - g) so every warp carries the same
+    // substitution length.  The columns of a group share every step's
+    // triangle loads and run as independent chains; a column whose index is
+    // past the step carries zeros there (x_k = 0 above / below its unit
+    // entry), so running the group's common step range is exact.
+    static_assert(TL / TINV_CPW == 2 * (TINV_THREADS / 32), "two column groups per warp");
+#pragma unroll 1
+    for (int half = 0; half < 2; ++half) {
+        const int grp = half == 0 ? w : TL / TINV_CPW - 1 - w;
+        const int j0 = grp * TINV_CPW;
+        cf x[TINV_CPW][4];
 #pragma unroll
-        for (int r = 0; r < 4; ++r) x[r] = fmk(32 * r + lane == j ? 1.f : 0.f, 0.f);
+        for (int c = 0; c < TINV_CPW; ++c)
+#pragma unroll
+            for (int r = 0; r < 4; ++r) x[c][r] = fmk(32 * r + lane == j0 + c ? 1.f : 0.f, 0.f);
         if (lower) {
 #pragma unroll
             for (int r = 0; r < 4; ++r) {
-                if (32 * r + 31 < j) continue;
-                for (int kk = (32 * r < j ? j - 32 * r : 0); kk < 32; ++kk) {
+                if (32 * r + 31 < j0) continue;
+                for (int kk = (32 * r < j0 ? j0 - 32 * r : 0); kk < 32; ++kk) {
                     const int k = 32 * r + kk;
-                    const cf xk = fmk(__shfl_sync(0xffffffffu, x[r].x, kk),
-                                      __shfl_sync(0xffffffffu, x[r].y, kk));
-                    const cf *tk = Tc + k * TL + lane;
+                    cf t[4];
 #pragma unroll
-                    for (int r2 = r; r2 < 4; ++r2)
-                        if (r2 > r || lane > kk) x[r2] = ffms(tk[32 * r2], xk, x[r2]);
+                    for (int r2 = 0; r2 < 4; ++r2) t[r2] = r2 >= r ? Tc[k * TL + 32 * r2 + lane] : fmk(0.f, 0.f);
+#pragma unroll
+                    for (int c = 0; c < TINV_CPW; ++c) {
+                        const cf xk = fmk(__shfl_sync(0xffffffffu, x[c][r].x, kk),
+                                          __shfl_sync(0xffffffffu, x[c][r].y, kk));
+#pragma unroll
+                        for (int r2 = r; r2 < 4; ++r2)
+                            if (r2 > r || lane > kk) x[c][r2] = ffms(t[r2], xk, x[c][r2]);
+                    }
                 }
             }
         } else {
+            const int jt = j0 + TINV_CPW - 1;      // largest column of the group
 #pragma unroll
             for (int r = 3; r >= 0; --r) {
-                if (32 * r > j) continue;
-                for (int kk = min(31, j - 32 * r); kk >= 0; --kk) {
+                if (32 * r > jt) continue;
+                for (int kk = min(31, jt - 32 * r); kk >= 0; --kk) {
                     const int k = 32 * r + kk;
-                    const cf xk = fmul(fmk(__shfl_sync(0xffffffffu, x[r].x, kk),
-                                           __shfl_sync(0xffffffffu, x[r].y, kk)),
-                                       dinv[k]);
-                    if (lane == kk) x[r] = xk;
-                    const cf *tk = Tc + k * TL + lane;
+                    cf t[4];
 #pragma unroll
-                    for (int r2 = 0; r2 <= r; ++r2)
-                        if (r2 < r || lane < kk) x[r2] = ffms(tk[32 * r2], xk, x[r2]);
+                    for (int r2 = 0; r2 < 4; ++r2) t[r2] = r2 <= r ? Tc[k * TL + 32 * r2 + lane] : fmk(0.f, 0.f);
+                    const cf dk = dinv[k];
+#pragma unroll
+                    for (int c = 0; c < TINV_CPW; ++c) {
+                        const cf xk = fmul(fmk(__shfl_sync(0xffffffffu, x[c][r].x, kk),
+                                               __shfl_sync(0xffffffffu, x[c][r].y, kk)),
+                                           dk);
+                        if (lane == kk) x[c][r] = xk;
+#pragma unroll
+                        for (int r2 = 0; r2 <= r; ++r2)
+                            if (r2 < r || lane < kk) x[c][r2] = ffms(t[r2], xk, x[c][r2]);
+                    }
                 }
             }
         }
         // stored rounded to nearest TF32, the precision the leaf GEMM reads
 #pragma unroll
-        for (int r = 0; r < 4; ++r) {
-            ob[j * TL + 32 * r + lane] = tf32_rna(x[r].x);
-            ob[TL * TL + j * TL + 32 * r + lane] = tf32_rna(x[r].y);
-        }
+        for (int c = 0; c < TINV_CPW; ++c)
+#pragma unroll
+            for (int r = 0; r < 4; ++r) {
+                ob[(j0 + c) * TL + 32 * r + lane] = tf32_rna(x[c][r].x);
+                ob[TL * TL + (j0 + c) * TL + 32 * r + lane] = tf32_rna(x[c][r].y);
+            }
     }
 }
 
