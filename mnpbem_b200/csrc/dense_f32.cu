@@ -490,8 +490,20 @@ __device__ int compact_swaps(const int32_t *pv, int lo, int hi, int2 *list) {
     return n;
 }
 
+// Column segments of one interchange launch: columns [brk[i], brk[i+1])
+// take the interchanges [cs[i], end) (cs[i] == end: none).
+constexpr int SWP_MAXSEG = 24;
+struct SwpSegs {
+    int n, end;
+    int brk[SWP_MAXSEG + 1];
+    int cs[SWP_MAXSEG];
+};
+
+// segs != nullptr: column j takes only the interchanges of its segment's
+// range (the recursive LU's fused forward + deferred backward interchanges)
 __global__ void laswp_kernel(float *A, int64_t lda, int64_t plane, int64_t sA, int j0, int j1,
-                             const int32_t *ipiv, int64_t sP, int c0, int c1, int forward) {
+                             const int32_t *ipiv, int64_t sP, int c0, int c1, int forward,
+                             const SwpSegs segs, int use_segs) {
     __shared__ int2 list[SWP_CHUNK];
     const int64_t b = blockIdx.y;
     const int j = j0 + blockIdx.x * blockDim.x + threadIdx.x;
@@ -503,8 +515,15 @@ __global__ void laswp_kernel(float *A, int64_t lda, int64_t plane, int64_t sA, i
         const int lo = c0 + ch * SWP_CHUNK, hi = min(c1, lo + SWP_CHUNK);
         const int cnt = compact_swaps(pv, lo, hi, list);
         if (j < j1) {
+            int cmin = c0;
+            if (use_segs) {
+                cmin = segs.end;
+                for (int q = 0; q < segs.n; ++q)
+                    if (j >= segs.brk[q] && j < segs.brk[q + 1]) cmin = segs.cs[q];
+            }
             for (int t = 0; t < cnt; ++t) {
                 const int2 e = list[forward ? t : cnt - 1 - t];
+                if (e.x < cmin) continue;
                 const cf x = ld(col, plane, e.x);
                 st(col, plane, e.x, ld(col, plane, e.y));
                 st(col, plane, e.y, x);
@@ -1783,16 +1802,60 @@ int laswp(Ctx &c, CMatF A, int j0, int j1, const int32_t *ipiv, int64_t sP, int 
     if (j1 <= j0 || c1 <= c0) return MNPB_OK;
     dim3 grid(ceil_div(j1 - j0, 128), c.batch);
     ProfScope ps(c.s, PC_SWAP, 0.0);
+    SwpSegs none{};
     laswp_kernel<<<grid, 128, 0, c.s>>>(A.p, A.ld, A.plane, A.stride, j0, j1, ipiv, sP, c0, c1,
-                                        forward ? 1 : 0);
+                                        forward ? 1 : 0, none, 0);
     MNPB_LAUNCH_CHECK("laswp_kernel(f32)");
     return MNPB_OK;
 }
 
+// One launch of the segment table t (forward order): columns [t.brk[0],
+// t.brk[t.n]), interchanges from the smallest segment start to t.end.
+static int laswp_segs(Ctx &c, CMatF A, const int32_t *ipiv, int64_t sP, const SwpSegs &t) {
+    if (t.n == 0) return MNPB_OK;
+    int c0 = t.end;
+    for (int q = 0; q < t.n; ++q) c0 = min(c0, t.cs[q]);
+    const int j0 = t.brk[0], j1 = t.brk[t.n];
+    if (j1 <= j0 || t.end <= c0) return MNPB_OK;
+    dim3 grid(ceil_div(j1 - j0, 128), c.batch);
+    ProfScope ps(c.s, PC_SWAP, 0.0);
+    laswp_kernel<<<grid, 128, 0, c.s>>>(A.p, A.ld, A.plane, A.stride, j0, j1, ipiv, sP, c0,
+                                        t.end, 1, t, 1);
+    MNPB_LAUNCH_CHECK("laswp_kernel(f32, segments)");
+    return MNPB_OK;
+}
+
+// append segment [j0, j1) -> interchanges [cs, t.end) to table t
+static int seg_push(SwpSegs &t, int j0, int j1, int cs) {
+    if (j1 <= j0) return MNPB_OK;
+    if (t.n >= SWP_MAXSEG) {
+        set_error("getrf: interchange segment table full");
+        return MNPB_EINVAL;
+    }
+    if (t.n == 0) t.brk[0] = j0;
+    if (t.brk[t.n] != j0) {               // gap: nothing owed there
+        t.cs[t.n] = t.end;
+        t.brk[++t.n] = j0;
+        if (t.n >= SWP_MAXSEG) {
+            set_error("getrf: interchange segment table full");
+            return MNPB_EINVAL;
+        }
+    }
+    t.cs[t.n] = cs;
+    t.brk[++t.n] = j1;
+    return MNPB_OK;
+}
+
 // Factor columns [off, off+w) over rows [off, n) of the full matrix A;
-// pivots are absolute row indices.
+// pivots are absolute row indices.  The backward interchanges this node's
+// columns still owe (its right half's pivots on its left half, and what its
+// right half owes) are returned in `owed` (pivots up to off + w) instead of
+// applied: the caller applies them in its next interchange launch, together
+// with its own forward interchanges, before anything reads these columns.
 static int rgetrf(Ctx &c, int n, int off, int w, CMatF A, int32_t *ipiv, int64_t sP,
-                  int32_t *info) {
+                  int32_t *info, SwpSegs &owed) {
+    owed.n = 0;
+    owed.end = off + w;
     if (w <= TS) {
         ProfScope ps(c.s, PC_PANEL, 8.0 * w * w * (double)(n - off) * c.batch / 2);
         prof_tag("off=%d w=%d B=%d", off, w, c.batch);
@@ -1819,18 +1882,30 @@ static int rgetrf(Ctx &c, int n, int off, int w, CMatF A, int32_t *ipiv, int64_t
         return MNPB_OK;
     }
     const int w1 = split_point(w);
-    MNPB_TRY(rgetrf(c, n, off, w1, A, ipiv, sP, info));
-    MNPB_TRY(laswp(c, A, off + w1, off + w, ipiv, sP, off, off + w1, true));
+    SwpSegs pl;
+    MNPB_TRY(rgetrf(c, n, off, w1, A, ipiv, sP, info, pl));
+    // one launch: what the left half owes (pivots up to off + w1) and the
+    // left half's pivots on the right half's columns
+    SwpSegs t = pl;
+    MNPB_TRY(seg_push(t, off + w1, off + w, off));
+    MNPB_TRY(laswp_segs(c, A, ipiv, sP, t));
     MNPB_TRY(trsm_llu(c, w1, w - w1, A.sub(off, off), A.sub(off, off + w1)));
     // L21 is stored rounded to TF32 by the panels: read in place
     MNPB_TRY(gemm(c, n - off - w1, w - w1, w1, -1.f, A.sub(off + w1, off),
                   A.sub(off, off + w1), 1.f, A.sub(off + w1, off + w1), false, true));
-    MNPB_TRY(rgetrf(c, n, off + w1, w - w1, A, ipiv, sP, info));
-    return laswp(c, A, off, off + w1, ipiv, sP, off + w1, off + w, true);
+    SwpSegs pr;
+    MNPB_TRY(rgetrf(c, n, off + w1, w - w1, A, ipiv, sP, info, pr));
+    // owed: the right half's pivots on the left half's columns, and what the
+    // right half owes (both up to off + w)
+    MNPB_TRY(seg_push(owed, off, off + w1, off + w1));
+    for (int q = 0; q < pr.n; ++q) MNPB_TRY(seg_push(owed, pr.brk[q], pr.brk[q + 1], pr.cs[q]));
+    return MNPB_OK;
 }
 
 int getrf(Ctx &c, int n, CMatF A, int32_t *ipiv, int64_t sP, int32_t *info) {
-    return rgetrf(c, n, 0, n, A, ipiv, sP, info);
+    SwpSegs owed;
+    MNPB_TRY(rgetrf(c, n, 0, n, A, ipiv, sP, info, owed));
+    return laswp_segs(c, A, ipiv, sP, owed);
 }
 
 int getrs(Ctx &c, int n, int nrhs, CMatF LU, const int32_t *ipiv, int64_t sP, CMatF B) {
