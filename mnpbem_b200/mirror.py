@@ -28,10 +28,10 @@ from ._lib import call, ptr
 from .compstruct import CompStruct
 from .geometry import Particle, ComParticle
 from .greenfun import SurfaceTables
-from .excitation import PlaneWaveRet
+from .excitation import PlaneWaveRet, PlaneWaveStat
 
 __all__ = ["flip", "ComParticleMirror", "CompStructMirror", "PlaneWaveRetMirror",
-           "BEMRetMirror"]
+           "BEMRetMirror", "PlaneWaveStatMirror", "BEMStatMirror"]
 
 
 def flip(p, dirs):
@@ -384,3 +384,133 @@ class BEMRetMirror(object):
 
     def __call__(self, enei):
         return self.init(enei)
+
+
+class PlaneWaveStatMirror(object):
+    """Quasistatic plane wave on a mirror-symmetric particle
+    (mnpbem/simulation/planewave_stat_mirror.py:9-180): the x- and y-polarised
+    potentials phip = -n . e with their symmetry values; ``full`` combines
+    them on the full particle with the requested polarisations."""
+
+    def __init__(self, pol, medium=1, **options):
+        self.pol = np.atleast_2d(np.asarray(pol, dtype=float))
+        self.exc = PlaneWaveStat(self.pol, medium=medium, **options)
+
+    def potential(self, p, enei):
+        pot = CompStructMirror(p, enei, lambda s: self.full(s))
+        nvec = np.asarray(p.nvec)
+        keys = {'x': (['+', '-', '-'], ['-', '+', '-']),
+                'y': (['+', '-', '+'], ['-', '+', '-']),
+                'xy': (['++', '--', '-+'], ['--', '++', '+-'])}
+        if p.sym not in keys:
+            raise ValueError("PlaneWaveStatMirror: unknown symmetry {!r}".format(p.sym))
+        for i in range(2):
+            v = CompStruct(p, enei, phip=-nvec[:, i].copy())
+            v.symval = p.symvalue(keys[p.sym][i])
+            pot.val.append(v)
+        return pot
+
+    __call__ = potential
+
+    def full(self, val):
+        """Values on the full particle: sum over the x and y parts weighted by
+        each polarisation's x and y components (planewave_stat_mirror.py:92)."""
+        parts = val.expand()
+        pf = val.p.full()
+        out = CompStruct(pf, val.enei)
+        npol = self.pol.shape[0]
+        for name in ('sig', 'phi', 'phip'):
+            vecs = [e.val.get(name) for e in parts]
+            if all(isinstance(v, np.ndarray) for v in vecs):
+                r = np.zeros((vecs[0].shape[0], npol), dtype=complex)
+                for ip in range(npol):
+                    for ib, v in enumerate(vecs):
+                        r[:, ip] += self.pol[ip, ib] * v
+                out[name] = r
+        return out, pf
+
+    def extinction(self, sig):
+        return self.exc.extinction(self.full(sig)[0])
+
+    def scattering(self, sig):
+        return self.exc.scattering(self.full(sig)[0])
+
+    def absorption(self, sig):
+        return self.exc.absorption(self.full(sig)[0])
+
+
+class BEMStatMirror(object):
+    """Quasistatic BEM solver on the irreducible part of a mirror-symmetric
+    particle, FP64 on the GPU (mnpbem/bem/bem_stat_mirror.py:140-487): the
+    full particle's refined, closure-corrected F contracted once per
+    symmetry value (F_s = sum_k tab[s, k] F(:, image k), mnpb_mirror_contract),
+    then per wavelength M_s = -(Lambda + F_s) factorised for every symmetry
+    value in one batch, and each excitation value solved with the matrix of
+    its symmetry."""
+
+    def __init__(self, p, enei=None, **options):
+        from .greenfun import CompGreenStat
+        if not isinstance(p, ComParticleMirror):
+            raise TypeError("BEMStatMirror: expected a ComParticleMirror")
+        self.p = p
+        self.device = torch.device('cuda')
+        g = CompGreenStat(p.pfull, **options)
+        n, nf, nk = p.n, g.tables.n, p.nk
+        nsym = p.symtable.shape[0]
+        tab = np.ascontiguousarray(p.symtable, dtype=np.float64)
+        Fc = g.F_dev.to(torch.complex128)              # column-major, ld nf
+        Fs = torch.empty((nsym, n, n), dtype=torch.complex128, device=self.device)
+        call('mnpb_mirror_contract', _lib.stream_handle(), n, nk, nsym, 1, ptr(Fc), nf, nf * nf,
+             ptr(tab), ptr(Fs), n, n * n)
+        self.F = Fs.real.contiguous()                  # (nsym, n, n), column-major each
+        del Fc, Fs, g
+        self.enei = None
+        if enei is not None:
+            self.init(enei)
+
+    def init(self, enei):
+        if self.enei is not None and self.enei == enei:
+            return self
+        p, dev = self.p, self.device
+        n, nsym = p.n, self.F.shape[0]
+        e1, e2 = np.asarray(p.eps1(enei)), np.asarray(p.eps2(enei))
+        eps = np.zeros((1, n, 4))
+        eps[0, :, 0], eps[0, :, 1], eps[0, :, 2], eps[0, :, 3] = e1.real, e1.imag, e2.real, e2.imag
+        d_eps = torch.from_numpy(eps).to(dev)
+        sh = _lib.stream_handle()
+        M = torch.empty((nsym, n, n), dtype=torch.complex128, device=dev)
+        for s in range(nsym):
+            call('mnpb_stat_matrix', sh, n, 1, ptr(self.F[s]), n, ptr(d_eps), ptr(M[s]), n, n * n)
+        piv = torch.empty((nsym, n), dtype=torch.int32, device=dev)
+        info = torch.zeros(nsym, dtype=torch.int32, device=dev)
+        call('mnpb_getrf_f64', sh, n, nsym, ptr(M), n, n * n, ptr(piv), n, ptr(info))
+        if info.cpu().numpy().any():
+            raise _lib.MNPBError('BEMStatMirror', 3, 'zero pivot in a symmetry block')
+        self._M, self._piv = M, piv
+        self.enei = enei
+        return self
+
+    __call__ = init
+
+    def solve(self, exc):
+        """Surface charges of every excitation value (bem_stat_mirror.py:360)."""
+        self.init(exc.enei)
+        p, n = self.p, self.p.n
+        sig = CompStructMirror(p, exc.enei, exc.fun)
+        sh = _lib.stream_handle()
+        for v in exc.val:
+            ind = p.symindex(v.symval[-1, :])
+            phip = np.asarray(v.phip)
+            K = 1 if phip.ndim == 1 else phip.shape[1]
+            B = torch.from_numpy(np.ascontiguousarray(phip.reshape(n, K).T.astype(complex))) \
+                .to(self.device).unsqueeze(0).contiguous()
+            call('mnpb_getrs_f64', sh, n, 1, K, ptr(self._M[ind]), n, n * n, ptr(self._piv[ind]),
+                 n, ptr(B), n, n * K)
+            x = B[0].cpu().numpy().T
+            out = CompStruct(p, exc.enei, sig=x[:, 0] if phip.ndim == 1 else x)
+            out.symval = v.symval
+            sig.val.append(out)
+        return sig, self
+
+    def __truediv__(self, exc):
+        return self.solve(exc)

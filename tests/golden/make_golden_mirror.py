@@ -15,7 +15,11 @@ together with its mirror images (closed_args (1,)):
 ``ComParticleMirror`` (mnpbem/geometry/comparticle_mirror.py:110),
 ``BEMRetMirror`` (mnpbem/bem/bem_ret_mirror.py:147) and
 ``PlaneWaveRetMirror`` (mnpbem/simulation/planewave_ret_mirror.py:8) with
-pol x and pol y along +z, at 500 and 600 nm.  ``golden_mirror.npz`` holds
+pol x and pol y along +z, at 500 and 600 nm; and the quasistatic
+``BEMStatMirror`` (mnpbem/bem/bem_stat_mirror.py:140) with
+``PlaneWaveStatMirror`` (mnpbem/simulation/planewave_stat_mirror.py:9), pol x
+and pol y, at the same wavelengths (keys ``stat_*``: sig and symval per
+symmetry value, extinction, scattering, absorption).  ``golden_mirror.npz`` holds
 the irreducible mesh (verts2, faces2), the full particle's centroids and
 normals, per wavelength and symmetry component sig1, sig2, h1, h2 and the
 symmetry values, and the extinction and scattering cross sections.  Only
@@ -77,6 +81,24 @@ def main(ref_root):
             sca = exc.scattering(sig)
             out['%s_%d_sca' % (sym, i)] = np.asarray(sca[0] if isinstance(sca, tuple) else sca)
             print(sym, lam, 'ext', out['%s_%d_ext' % (sym, i)], flush=True)
+    from mnpbem.bem.bem_stat_mirror import BEMStatMirror
+    from mnpbem.simulation.planewave_stat_mirror import PlaneWaveStatMirror
+    for sym, (ph, th) in CASES.items():
+        p = trispheresegment(np.linspace(*ph), np.linspace(*th), 20.0)
+        cpm = ComParticleMirror(eps, [p], [[2, 1]], sym, (1,))
+        bem = BEMStatMirror(cpm)
+        exc = PlaneWaveStatMirror(pol)
+        for i, lam in enumerate(LAMS):
+            sig, bem = bem.solve(exc.potential(cpm, lam))
+            for v, sv in enumerate(sig.val):
+                out['stat_%s_%d_%d_sig' % (sym, i, v)] = np.asarray(sv.sig)
+                out['stat_%s_%d_%d_symval' % (sym, i, v)] = np.asarray(sv.symval)
+            for key, fn in (('ext', exc.extinction), ('sca', exc.scattering),
+                            ('abs', exc.absorption)):
+                val = fn(sig)
+                out['stat_%s_%d_%s' % (sym, i, key)] = np.asarray(val[0] if isinstance(val, tuple)
+                                                                 else val)
+            print('stat', sym, lam, 'ext', out['stat_%s_%d_ext' % (sym, i)], flush=True)
     np.savez_compressed(os.path.join(HERE, 'golden_mirror.npz'), **out)
     print('wrote golden_mirror.npz')
 
