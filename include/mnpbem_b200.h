@@ -613,13 +613,14 @@ int mnpb_eels_infty(void *stream, int64_t n, int64_t nimp, const double *pos, co
  * impact seg_imp[c] inside particles, -1/vel times the charged-wire integral
  * with wavenumbers q (beam) and k (medium) on the 11 Legendre-Gauss-Lobatto
  * nodes lgl_x / weights lgl_w (host arrays) (eels_base.py:418-523 and
- * 713-783, potinside / potwire). */
+ * 713-783, potinside / potwire); with phip non-null also their surface
+ * derivatives along nvec (nseg x n complex). */
 int mnpb_eels_wire(void *stream, int64_t n, int64_t nimp, const double *pos, const double *nvec,
                    const double *area, const int8_t *face_on, const double *impact,
                    const int8_t *indquad, const double *qpos, const double *qw,
                    const int64_t *qoff, double width, double vel, int64_t nseg,
                    const double *seg, const int32_t *seg_imp, double q, double k_re, double k_im,
-                   const double *lgl_x, const double *lgl_w, double *phi);
+                   const double *lgl_x, const double *lgl_w, double *phi, double *phip);
 
 /* Fields of the beams at nobs positions in media obs_med: e, h (nobs x 3 x
  * nimp complex); mtab (nmed x 3 complex): eps, q = k / (vel sqrt(eps)) and

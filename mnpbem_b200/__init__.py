@@ -3,7 +3,8 @@
 Drop-in classes with the reference call surface (``BEMRet``, ``BEMStat``,
 ``BEMRetIter``,
 ``CompGreenRet``, ``CompGreenStat``, ``PlaneWaveRet``, ``PlaneWaveStat``,
-``DipoleRet``, ``EELSRet``, ``ComPoint``, ``CompStruct``, ``ComParticle``) backed by hand-written sm_100a CUDA kernels
+``DipoleRet``, ``EELSRet``, ``EELSStat``, ``ComPoint``, ``CompStruct``, ``ComParticle``) backed by
+hand-written sm_100a CUDA kernels
 in ``libmnpbem_b200.so`` (C ABI: include/mnpbem_b200.h).  There is no CPU
 fallback: importing the solvers requires the built library.
 """
@@ -33,7 +34,7 @@ def __getattr__(name):
     if name in ('DipoleRet', 'ComPoint', 'Point'):
         from . import points
         return getattr(points, name)
-    if name in ('EELSRet',):
+    if name in ('EELSRet', 'EELSStat'):
         from . import eels
         return getattr(eels, name)
     raise AttributeError(name)

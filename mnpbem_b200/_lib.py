@@ -102,7 +102,7 @@ SIGNATURES = {
     'mnpb_eels_infty': [_P, _I64, _I64, _P, _P, _P, _P, _P, _P, _P, _P, _P, _D, _D, _D, _D, _D,
                         _P, _P],
     'mnpb_eels_wire': [_P, _I64, _I64, _P, _P, _P, _P, _P, _P, _P, _P, _P, _D, _D, _I64, _P, _P,
-                       _D, _D, _D, _P, _P, _P],
+                       _D, _D, _D, _P, _P, _P, _P],
     'mnpb_eels_field': [_P, _I64, _I64, _P, _P, _I, _P, _P, _D, _D, _P, _P, _P],
     'mnpb_pad_entries': [_P, _I64, _I64, _P, _P, _P, _P, _P, _I64, _I64, _P, _P, _P, _P, _I64,
                          _I64, _I64],

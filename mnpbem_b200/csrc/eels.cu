@@ -82,13 +82,17 @@ __device__ __forceinline__ void beam_pot(const double *r, const double *nv, doub
 // Potential of a charged wire from z0 to z1 along the beam through b at
 // distance rr and height z (eels_base.py:713-783, potwire): with
 // u = sinh-type substitution v = log(s + sqrt(rr^2 + s^2)),
-//   I = (v1 - v0)/2 e^{iqz} sum_g w_g exp(i (q u_g + k sqrt(rr^2 + u_g^2))).
-__device__ __forceinline__ cd wire_pot(double rr, double z, double q, cd k, double z0,
-                                       double z1, const LGL &g) {
+//   I  = (v1 - v0)/2 e^{iqz} sum_g w_g f_g,  f_g = exp(i (q u_g + k R_g)),
+//   Ir = (v1 - v0)/2 e^{iqz} sum_g w_g rr (ik/R_g - 1/R_g^2) f_g,
+//   Iz = -(v1 - v0)/2 e^{iqz} sum_g w_g u_g (ik/R_g - 1/R_g^2) f_g,
+// R_g = sqrt(rr^2 + u_g^2).  The derivatives are formed only with DERIV.
+template <bool DERIV>
+__device__ __forceinline__ void wire_pot(double rr, double z, double q, cd k, double z0,
+                                         double z1, const LGL &g, cd &I, cd &Ir, cd &Iz) {
     const double s0 = z0 - z, s1 = z1 - z;
     const double v0 = log(s0 + sqrt(rr * rr + s0 * s0));
     const double v1 = log(s1 + sqrt(rr * rr + s1 * s1));
-    cd acc = cmk(0.0, 0.0);
+    cd acc = cmk(0.0, 0.0), accr = acc, accz = acc;
     for (int a = 0; a < LGL_N; ++a) {
         const double v = 0.5 * ((1.0 - g.x[a]) * v0 + (1.0 + g.x[a]) * v1);
         const double u = 0.5 * (exp(v) - rr * rr * exp(-v));
@@ -98,12 +102,23 @@ __device__ __forceinline__ cd wire_pot(double rr, double z, double q, cd k, doub
         double sn, cs;
         sincos(ph, &sn, &cs);
         const double m = exp(-k.y * R) * g.w[a];
-        acc.x += m * cs;
-        acc.y += m * sn;
+        const cd f = cmk(m * cs, m * sn);
+        acc = cadd(acc, f);
+        if (DERIV) {
+            const double iR = 1.0 / R;
+            const cd d = cmul(cmk(-k.y * iR - iR * iR, k.x * iR), f);   // (ik/R - 1/R^2) f
+            accr = cadd(accr, cscale(d, rr));
+            accz = csub(accz, cscale(d, u));
+        }
     }
     double sn, cs;
     sincos(q * z, &sn, &cs);
-    return cscale(cmul(acc, cmk(cs, sn)), 0.5 * (v1 - v0));
+    const cd pre = cscale(cmk(cs, sn), 0.5 * (v1 - v0));
+    I = cmul(acc, pre);
+    if (DERIV) {
+        Ir = cmul(accr, pre);
+        Iz = cmul(accz, pre);
+    }
 }
 
 struct BeamFaces {
@@ -188,39 +203,51 @@ __global__ void __launch_bounds__(128) eels_infty_kernel(BeamFaces t,
 }
 
 // Wire potentials of beam segments inside particles (eels_base.py:418-523,
-// potinside, scalar potential): segment c of impact imp[c] from z0 to z1,
-//   phi = -1/vel I(rr, z),  face-quadrature average where indquad[i, imp[c]];
-// out (nseg, n), 0 for faces without face_on.
+// potinside): segment c of impact imp[c] from z0 to z1,
+//   phi  = -1/vel I(rr, z),
+//   phip = -1/vel (Iz n_z + Ir (x n_x + y n_y) / rr)      (DERIV only),
+// face-quadrature averages where indquad[i, imp[c]]; out (nseg, n), 0 for
+// faces without face_on.
+template <bool DERIV>
 __global__ void __launch_bounds__(128) eels_wire_kernel(BeamFaces t,
                                                         const int8_t *__restrict__ face_on,
                                                         int nseg, const double *__restrict__ seg,
                                                         const int32_t *__restrict__ seg_imp,
                                                         double q, cd k, LGL g,
-                                                        cd *__restrict__ phi) {
+                                                        cd *__restrict__ phi,
+                                                        cd *__restrict__ phip) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int c = blockIdx.y;
     if (i >= t.n) return;
-    cd acc = cmk(0.0, 0.0);
+    cd acc = cmk(0.0, 0.0), accp = acc;
     if (face_on[i]) {
         const int j = seg_imp[c];
         const double bx = t.impact[2 * j], by = t.impact[2 * j + 1];
         const double z0 = seg[2 * c], z1 = seg[2 * c + 1];
-        auto one = [&](const double *r) {
+        const double *nv = t.nvec + 3 * i;
+        auto one = [&](const double *r, double w) {
             const double x = r[0] - bx, y = r[1] - by;
             const double rp = sqrt(x * x + y * y);
             const double rr = sqrt(rp * rp + t.width * t.width);
-            return wire_pot(rr, r[2], q, k, z0, z1, g);
+            cd I, Ir, Iz;
+            wire_pot<DERIV>(rr, r[2], q, k, z0, z1, g, I, Ir, Iz);
+            acc = cadd(acc, cscale(I, w));
+            if (DERIV)
+                accp = cadd(accp, cscale(cadd(cscale(Iz, nv[2]),
+                                              cscale(Ir, (x * nv[0] + y * nv[1]) / rr)), w));
         };
         if (!t.indquad[(int64_t)i * t.nimp + j]) {
-            acc = one(t.pos + 3 * i);
+            one(t.pos + 3 * i, 1.0);
         } else {
             const double ia = 1.0 / t.area[i];
             for (int64_t p = t.qoff[i]; p < t.qoff[i + 1]; ++p)
-                acc = cadd(acc, cscale(one(t.qpos + 3 * p), t.qw[p] * ia));
+                one(t.qpos + 3 * p, t.qw[p] * ia);
         }
         acc = cscale(acc, -1.0 / t.vel);
+        accp = cscale(accp, -1.0 / t.vel);
     }
     phi[(int64_t)c * t.n + i] = acc;
+    if (DERIV) phip[(int64_t)c * t.n + i] = accp;
 }
 
 // Fields of the beams at observation points in medium med_i (eels_ret.py:
@@ -343,7 +370,7 @@ extern "C" int mnpb_eels_wire(void *stream, int64_t n, int64_t nimp, const doubl
                               const double *qw, const int64_t *qoff, double width, double vel,
                               int64_t nseg, const double *seg, const int32_t *seg_imp, double q,
                               double k_re, double k_im, const double *lgl_x,
-                              const double *lgl_w, double *phi) {
+                              const double *lgl_w, double *phi, double *phip) {
     clear_error();
     BeamFaces t;
     MNPB_TRY(beam_faces(t, n, nimp, pos, nvec, area, impact, indquad, qpos, qw, qoff, width, vel,
@@ -356,8 +383,12 @@ extern "C" int mnpb_eels_wire(void *stream, int64_t n, int64_t nimp, const doubl
         g.w[a] = lgl_w[a];
     }
     dim3 grid(ceil_div(n, 128), (unsigned)nseg);
-    eels_wire_kernel<<<grid, 128, 0, as_stream(stream)>>>(t, face_on, (int)nseg, seg, seg_imp, q,
-                                                          cmk(k_re, k_im), g, (cd *)phi);
+    if (phip)
+        eels_wire_kernel<true><<<grid, 128, 0, as_stream(stream)>>>(
+            t, face_on, (int)nseg, seg, seg_imp, q, cmk(k_re, k_im), g, (cd *)phi, (cd *)phip);
+    else
+        eels_wire_kernel<false><<<grid, 128, 0, as_stream(stream)>>>(
+            t, face_on, (int)nseg, seg, seg_imp, q, cmk(k_re, k_im), g, (cd *)phi, nullptr);
     MNPB_LAUNCH_CHECK("eels_wire_kernel");
     return MNPB_OK;
 }

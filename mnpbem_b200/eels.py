@@ -25,7 +25,7 @@ from .excitation import _inout_faces, pinfty, _Sides
 from .greenfun import _points
 from .materials import eps_k
 
-__all__ = ["EELSRet", "ene2vel", "lgl_nodes"]
+__all__ = ["EELSRet", "EELSStat", "ene2vel", "lgl_nodes"]
 
 # units (mnpbem/misc/units.py)
 EV2NM = 1.0 / 8.0655477e-4
@@ -77,20 +77,19 @@ def _in_polygon(x, y, xv, yv, tol=1e-10):
     return inside | on, on
 
 
-class EELSRet(object):
-    """Electron beams along z (mnpbem/simulation/eels_ret.py:24-670).
-
-    ``EELSRet(p, impact, width, vel, cutoff=None, phiout=1e-2, pinfty=None,
-    medium=1)``: impact (nimp, 2) in nm, width of the beam, velocity in units
-    of c (``ene2vel``), faces closer than ``cutoff`` (default 10 width) to a
-    beam in the xy plane are integrated with their quadrature points.
-    """
+class _EELSBase(object):
+    """Beam set-up shared by the retarded and quasistatic beams
+    (mnpbem/simulation/eels_base.py:25-830): crossing points with the faces,
+    segments inside particles, faces integrated with quadrature, path
+    lengths, and the GPU evaluation of the infinite-beam and wire
+    potentials."""
 
     def __init__(self, p, impact, width, vel, cutoff=None, phiout=1e-2, pinfty=None, medium=1,
                  **options):
         if options.get('refine', None) not in (None, 1) or \
                 (isinstance(options.get('eels'), dict) and options['eels'].get('refine', 1) != 1):
-            raise NotImplementedError("EELSRet: refined face quadrature ('refine') is not supported")
+            raise NotImplementedError("%s: refined face quadrature ('refine') is not supported"
+                                      % type(self).__name__)
         self.p = p
         self.width = float(width)
         self.vel = float(vel)
@@ -235,6 +234,61 @@ class EELSRet(object):
         return (ptr(d['impact']), ptr(d['indquad']), ptr(d['qpos']), ptr(d['qw']),
                 ptr(d['qoff']), self.width, self.vel)
 
+
+    # ---- beam potentials on the GPU ------------------------------------------
+    def _infty(self, q, igam, face_on):
+        d = self._device()
+        K, n = self.impact.shape[0], d['n']
+        phi = torch.empty((K, n), dtype=torch.complex128, device=d['dev'])
+        phip = torch.empty_like(phi)
+        fo = torch.from_numpy(np.ascontiguousarray(face_on, dtype=np.int8)).to(d['dev'])
+        call('mnpb_eels_infty', _lib.stream_handle(), n, K, ptr(d['pos']), ptr(d['nvec']),
+             ptr(d['area']), ptr(fo), *self._quad_args(d), float(q), float(igam.real),
+             float(igam.imag), ptr(phi), ptr(phip))
+        return phi.cpu().numpy().T, phip.cpu().numpy().T            # (n, nimp)
+
+    def _inside(self, q, k, segs, face_on, deriv=False):
+        """Wire potentials (n, nseg) of the segments ``segs`` (indices into
+        the segment list), 0 columns if there are none; with ``deriv`` also
+        their surface derivatives (phi, phip)."""
+        d = self._device()
+        n = d['n']
+        if len(segs) == 0:
+            z = np.zeros((n, 0), dtype=complex)
+            return (z, z.copy()) if deriv else z
+        return self._wire(d['n'], d['pos'], d['nvec'], d['area'], face_on, self._quad_args(d),
+                          q, k, segs, deriv)
+
+    def _wire(self, n, pos, nvec, area, face_on, quad_args, q, k, segs, deriv):
+        d = self._device()
+        dev = d['dev']
+        seg = torch.from_numpy(np.ascontiguousarray(self._z[segs])).to(dev)
+        simp = torch.from_numpy(np.ascontiguousarray(self._indimp[segs], dtype=np.int32)).to(dev)
+        fo = torch.from_numpy(np.ascontiguousarray(face_on, dtype=np.int8)).to(dev)
+        x, w = lgl_nodes(10)
+        phi = torch.empty((len(segs), n), dtype=torch.complex128, device=dev)
+        phip = torch.empty_like(phi) if deriv else None
+        call('mnpb_eels_wire', _lib.stream_handle(), n, self.impact.shape[0], ptr(pos), ptr(nvec),
+             ptr(area), ptr(fo), *quad_args, len(segs), ptr(seg), ptr(simp), float(q),
+             float(np.real(k)), float(np.imag(k)), ptr(x), ptr(w), ptr(phi),
+             ptr(phip) if deriv else None)
+        if deriv:
+            return phi.cpu().numpy().T, phip.cpu().numpy().T
+        return phi.cpu().numpy().T
+
+    def _face_sides(self, m):
+        io = self._device()['h_face_med']
+        return np.where(io[:, 0] == m)[0], np.where(io[:, 1] == m)[0]
+
+class EELSRet(_EELSBase):
+    """Electron beams along z (mnpbem/simulation/eels_ret.py:24-670).
+
+    ``EELSRet(p, impact, width, vel, cutoff=None, phiout=1e-2, pinfty=None,
+    medium=1)``: impact (nimp, 2) in nm, width of the beam, velocity in units
+    of c (``ene2vel``), faces closer than ``cutoff`` (default 10 width) to a
+    beam in the xy plane are integrated with their quadrature points.
+    """
+
     def _media(self, enei):
         eps = np.array([eps_k(f, enei)[0] for f in self.p.eps], dtype=complex)
         gamma = 1.0 / np.sqrt(1 - eps * self.vel ** 2)
@@ -297,39 +351,6 @@ class EELSRet(object):
     __call__ = potential
 
     # ---- loss probabilities ----------------------------------------------------
-    def _infty(self, q, igam, face_on):
-        d = self._device()
-        K, n = self.impact.shape[0], d['n']
-        phi = torch.empty((K, n), dtype=torch.complex128, device=d['dev'])
-        phip = torch.empty_like(phi)
-        fo = torch.from_numpy(np.ascontiguousarray(face_on, dtype=np.int8)).to(d['dev'])
-        call('mnpb_eels_infty', _lib.stream_handle(), n, K, ptr(d['pos']), ptr(d['nvec']),
-             ptr(d['area']), ptr(fo), *self._quad_args(d), float(q), float(igam.real),
-             float(igam.imag), ptr(phi), ptr(phip))
-        return phi.cpu().numpy().T, phip.cpu().numpy().T            # (n, nimp)
-
-    def _inside(self, q, k, segs, face_on):
-        """Wire potentials (n, nseg) of the segments ``segs`` (indices into
-        the segment list), 0 columns if there are none."""
-        d = self._device()
-        n = d['n']
-        if len(segs) == 0:
-            return np.zeros((n, 0), dtype=complex)
-        dev = d['dev']
-        seg = torch.from_numpy(np.ascontiguousarray(self._z[segs])).to(dev)
-        simp = torch.from_numpy(np.ascontiguousarray(self._indimp[segs], dtype=np.int32)).to(dev)
-        fo = torch.from_numpy(np.ascontiguousarray(face_on, dtype=np.int8)).to(dev)
-        x, w = lgl_nodes(10)
-        phi = torch.empty((len(segs), n), dtype=torch.complex128, device=dev)
-        call('mnpb_eels_wire', _lib.stream_handle(), n, self.impact.shape[0], ptr(d['pos']),
-             ptr(d['nvec']), ptr(d['area']), ptr(fo), *self._quad_args(d), len(segs), ptr(seg),
-             ptr(simp), float(q), float(np.real(k)), float(np.imag(k)), ptr(x), ptr(w), ptr(phi))
-        return phi.cpu().numpy().T
-
-    def _face_sides(self, m):
-        io = self._device()['h_face_med']
-        return np.where(io[:, 0] == m)[0], np.where(io[:, 1] == m)[0]
-
     def loss(self, sig):
         """Surface and bulk loss probabilities per impact parameter, in 1/eV
         (eels_ret.py:296-423): psurf = -Im sum_faces area phi* (sig - vel h_z)
@@ -438,3 +459,103 @@ class EELSRet(object):
              ptr(T(med)), d['nmed'], ptr(d['beam_in']), ptr(d['impact']), self.width, self.vel,
              ptr(T(mtab.view(np.float64))), ptr(e), ptr(h))
         return CompStruct(p, enei, e=e.cpu().numpy(), h=h.cpu().numpy())
+
+
+class EELSStat(_EELSBase):
+    """Electron beams along z, quasistatic (mnpbem/simulation/eels_stat.py:23-409).
+
+    ``EELSStat(p, impact, width, vel, cutoff=None, phiout=1e-2)``: the beam
+    set-up of ``EELSRet``; ``potential`` is the excitation of ``BEMStat``
+    (phi, phip), ``loss`` the surface and bulk loss probabilities of its
+    solution, ``field`` the beams' electric field.  The beam potentials are
+    the retarded ones at gamma = 1 (infinite beam) and k = 0 (wire segments),
+    evaluated by the same kernels.
+    """
+
+    name = 'eels'
+    needs = {'sim': 'stat'}
+
+    def _eps(self, p, enei):
+        return np.array([eps_k(f, enei)[0] for f in p.eps], dtype=complex)
+
+    def potential(self, p, enei):
+        """phi, phip (n, nimp) (eels_stat.py:107-161): the infinite beam
+        over eps of the embedding medium plus, for each segment inside
+        medium m, its wire potential times 1/eps_m - 1/eps_1."""
+        eps = self._eps(self.p, enei)
+        q = 2 * np.pi / (enei * self.vel)
+        n = self._device()['n']
+        allf = np.ones(n, dtype=np.int8)
+        phi, phip = self._infty(q, 1.0, allf)
+        phi, phip = phi / eps[0], phip / eps[0]
+        if len(self._z):
+            pin, pinp = self._inside(q, 0.0, np.arange(len(self._z)), allf, deriv=True)
+            f = (1.0 / eps - 1.0 / eps[0])[self._indmat - 1][None, :]
+            phi = phi + self.full(pin * f)
+            phip = phip + self.full(pinp * f)
+        return CompStruct(p, enei, phi=phi, phip=phip)
+
+    __call__ = potential
+
+    def loss(self, sig):
+        """Surface and bulk loss probabilities per impact parameter, in 1/eV
+        (eels_stat.py:163-193): psurf = -FINE^2/(BOHR HARTREE pi)
+        Im sum_faces area conj(phi) sig, phi the infinite beam (gamma = 1)."""
+        q = 2 * np.pi / (sig.enei * self.vel)
+        n = self._device()['n']
+        phi, _ = self._infty(q, 1.0, np.ones(n, dtype=np.int8))
+        s = np.asarray(sig.sig).reshape(n, -1)
+        area = np.asarray(self.p.area, dtype=np.float64)
+        psurf = -FINE ** 2 / (BOHR * HARTREE * np.pi) * np.imag(area @ (np.conj(phi) * s))
+        return psurf, self.bulkloss(sig.enei)
+
+    def bulkloss(self, enei):
+        """Bulk loss probability per impact parameter in 1/eV (Garcia de
+        Abajo, RMP 82, 209 (2010), Eq. 19; eels_stat.py:195-228)."""
+        ene = EV2NM / enei
+        mass = 0.51e6
+        eps = self._eps(self.p, enei)
+        fac = 2 * FINE ** 2 / (BOHR * HARTREE * np.pi * self.vel ** 2)
+        return fac * (np.imag(-1.0 / eps) @ self.path()) * \
+            np.log(np.sqrt((mass / ene) ** 2 * self.vel ** 2 * self.phiout ** 2 + 1))
+
+    def field(self, p, enei, inout=1):
+        """Electric field e (n, 3, nimp) of the beams at the positions of
+        ``p`` (eels_stat.py:230-355): the infinite beam in the embedding
+        medium (q = k_1 / (vel sqrt(eps_1)), gamma = 1), plus the segments
+        inside media (gradients of their k = 0 wire potentials times
+        1/eps_m - 1/eps_1), each segment taken with its own impact parameter
+        and summed into it.  ``inout`` is not used."""
+        d = self._device()
+        dev = d['dev']
+        eps = self._eps(p, enei)
+        k1 = 2 * np.pi / enei * np.sqrt(eps[0])
+        q = k1 / (self.vel * np.sqrt(eps[0]))
+        obs = np.ascontiguousarray(np.asarray(p.pos, dtype=np.float64))
+        nobs, nimp = obs.shape[0], self.impact.shape[0]
+        T = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+        mtab = np.array([[eps[0], q, 1.0]], dtype=complex)
+        e = torch.empty((nobs, 3, nimp), dtype=torch.complex128, device=dev)
+        h = torch.empty_like(e)
+        call('mnpb_eels_field', _lib.stream_handle(), nobs, nimp, ptr(T(obs)),
+             ptr(T(np.ones(nobs, dtype=np.int32))), 1, ptr(T(np.ones((1, nimp), dtype=np.int8))),
+             ptr(d['impact']), self.width, self.vel, ptr(T(mtab.view(np.float64))), ptr(e), ptr(h))
+        e = e.cpu().numpy()
+        if len(self._z):
+            # the derivative along x^, y^, z^ of the wire potentials at every
+            # position: the three copies of the positions carry those normals
+            pos3 = np.concatenate([obs, obs, obs])
+            nv3 = np.repeat(np.eye(3), nobs, axis=0)
+            m = 3 * nobs
+            quad = (d['impact'], T(np.zeros((m, nimp), dtype=np.int8)), T(np.zeros(3)),
+                    T(np.zeros(1)), T(np.zeros(m + 1, dtype=np.int64)), self.width, self.vel)
+            quad = tuple(ptr(a) if torch.is_tensor(a) else a for a in quad)
+            segs = np.arange(len(self._z))
+            _, dphi = self._wire(m, T(pos3), T(nv3), T(np.ones(m)), np.ones(m, dtype=np.int8),
+                                 quad, np.real(q), 0.0, segs, True)
+            f = (1.0 / eps - 1.0 / eps[0])[self._indmat - 1][None, :]
+            # e_c = (1/eps_m - 1/eps_1) (Ir x_c / rr or Iz) / vel, which is
+            # -(1/eps_m - 1/eps_1) phip with the normal c^
+            ein = self.full(-dphi * f)                               # (3 nobs, nimp)
+            e = e + ein.reshape(3, nobs, nimp).transpose(1, 0, 2)
+        return CompStruct(p, enei, e=e)

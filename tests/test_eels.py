@@ -42,3 +42,19 @@ def test_lobatto_rule():
     for deg in range(20):                       # exact through degree 2n - 1 = 19
         exact = 0.0 if deg % 2 else 2.0 / (deg + 1)
         assert abs(w @ x ** deg - exact) < 1e-14
+
+
+@pytest.mark.parametrize('name', ['A', 'B', 'C'])
+def test_stat_beam_setup_and_bulkloss(setup, name):
+    """EELSStat shares the beam set-up; its bulk loss (eels_stat.py:195-228)
+    against the reference's (golden_eels_stat.npz)."""
+    from mnpbem_b200.eels import EELSStat
+    cp, _ = setup
+    z = golden('golden_eels_stat')
+    e = EELSStat(cp, z[name + '_impact_in'], 0.5, float(z['vel']))
+    assert e.name == 'eels' and e.needs == {'sim': 'stat'}
+    assert np.array_equal(e._indimp, z[name + '_indimp'])
+    for i, lam in enumerate(z['lams']):
+        pb = e.bulkloss(float(lam))
+        ref = z['%s_%d_pbulk' % (name, i)]
+        assert np.allclose(pb, ref, rtol=1e-12, atol=0)
