@@ -528,6 +528,16 @@ int mnpb_dipole_field(void *stream, int64_t nobs, int64_t batch, int64_t npt, in
                       const int32_t *pt_med, const double *dip, int nmed, const double *eps,
                       const double *k, const double *nb, double *e, double *h);
 
+/* Quasistatic dipole fields e = (3 x (x.d) - d) / (eps_q r^3) of dipoles
+ * dip (npt x 3 x ndip) at positions ptpos screened by eps_pt (npt complex),
+ * at nobs positions obs: out = e (nobs x 3 x npt x ndip complex), or with
+ * normals nvec (nobs x 3, may be NULL) out = -nvec.e (nobs x npt x ndip
+ * complex).  Replaces dipole_stat.py:149-289 (DipoleStat.field /
+ * potential). */
+int mnpb_dipole_stat_field(void *stream, int64_t nobs, int64_t npt, int64_t ndip,
+                           const double *obs, const double *nvec, const double *ptpos,
+                           const double *dip, const double *eps_pt, double *out);
+
 /* Adds the far fields of the dipoles whose pt_on flag is set (points in the
  * embedding medium) to e, h (batch x K x ndir x 3, the layout of
  * mnpb_farfield).  emb: per wavelength eps, k, nb of the embedding medium

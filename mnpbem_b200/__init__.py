@@ -3,7 +3,7 @@
 Drop-in classes with the reference call surface (``BEMRet``, ``BEMStat``,
 ``BEMRetIter``,
 ``CompGreenRet``, ``CompGreenStat``, ``PlaneWaveRet``, ``PlaneWaveStat``,
-``DipoleRet``, ``EELSRet``, ``EELSStat``, ``ComPoint``, ``CompStruct``, ``ComParticle``) backed by
+``DipoleRet``, ``DipoleStat``, ``EELSRet``, ``EELSStat``, ``ComPoint``, ``CompStruct``, ``ComParticle``) backed by
 hand-written sm_100a CUDA kernels
 in ``libmnpbem_b200.so`` (C ABI: include/mnpbem_b200.h).  There is no CPU
 fallback: importing the solvers requires the built library.
@@ -31,7 +31,7 @@ def __getattr__(name):
     if name in ('PlaneWaveRet', 'PlaneWaveStat'):
         from . import excitation
         return getattr(excitation, name)
-    if name in ('DipoleRet', 'ComPoint', 'Point'):
+    if name in ('DipoleRet', 'DipoleStat', 'ComPoint', 'Point', 'CompGreenStatPoints'):
         from . import points
         return getattr(points, name)
     if name in ('EELSRet', 'EELSStat'):

@@ -103,6 +103,7 @@ SIGNATURES = {
                         _P, _P],
     'mnpb_eels_wire': [_P, _I64, _I64, _P, _P, _P, _P, _P, _P, _P, _P, _P, _D, _D, _I64, _P, _P,
                        _D, _D, _D, _P, _P, _P, _P],
+    'mnpb_dipole_stat_field': [_P, _I64, _I64, _I64, _P, _P, _P, _P, _P, _P],
     'mnpb_eels_field': [_P, _I64, _I64, _P, _P, _I, _P, _P, _D, _D, _P, _P, _P],
     'mnpb_pad_entries': [_P, _I64, _I64, _P, _P, _P, _P, _P, _I64, _I64, _P, _P, _P, _P, _I64,
                          _I64, _I64],

@@ -493,14 +493,12 @@ class BEMStat(object):
         self(exc.enei)
         phip = np.asarray(exc.phip)
         n = self.tables.n
-        K = 1 if phip.ndim == 1 else phip.shape[1]
+        K = phip.size // n                      # trailing axes (npt, ndip, ...) as columns
         B = torch.from_numpy(np.ascontiguousarray(phip.reshape(n, K).T.astype(complex))) \
             .to(self.tables.device).unsqueeze(0).contiguous()
         call('mnpb_getrs_f64', _lib.stream_handle(), n, 1, K, ptr(self._M), n, n * n,
              ptr(self._piv), n, ptr(B), n, n * K)
-        sig = B[0].cpu().numpy().T
-        if phip.ndim == 1:
-            sig = sig[:, 0]
+        sig = B[0].cpu().numpy().T.reshape(phip.shape)
         return CompStruct(self.p, exc.enei, sig=sig), self
 
     def solve_spectrum(self, phip, eneis, batch=32, stream=None):

@@ -14,6 +14,9 @@
 //                          charges and currents (greenfun/compgreen_ret.py:
 //                          912-1036 with a point set as p1)
 //  * point_eval_kernel     entries G / Gp of a point-face region pair
+//  * dipole_stat_kernel    quasistatic dipole fields at observation positions
+//                          and their normal projections (simulation/
+//                          dipole_stat.py:149-289)
 #include "common.cuh"
 
 namespace mnpb {
@@ -152,6 +155,44 @@ __global__ void __launch_bounds__(128) dipole_field_kernel(
         for (int c = 0; c < 3; ++c) {
             ho[c * K + col] = cscale(fh, cr[c]);
             eo[c * K + col] = cadd(cscale(f1, d[c] - in * u[c]), cscale(f2, 3.0 * in * u[c] - d[c]));
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Quasistatic dipole fields (Jackson 4.13), screened by the dielectric
+// function eps_q of the medium of dipole q; every observation position sees
+// every dipole:
+//   e = (3 x (x.d) - d) / (eps_q r^3),   x = (obs_i - pt_q) / r.
+// Without normals out = e [nobs][3][npt][ndip]; with normals n_i out =
+// phi' = -n_i.e [nobs][npt][ndip].  One thread per (observation, dipole
+// position).
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(128) dipole_stat_kernel(
+    int nobs, int npt, int ndip, const double *__restrict__ obs,
+    const double *__restrict__ nvec, const double *__restrict__ ptpos,
+    const double *__restrict__ dip, const double *__restrict__ eps_pt, cd *__restrict__ out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int q = blockIdx.y;
+    if (i >= nobs) return;
+    double x[3];
+    for (int c = 0; c < 3; ++c) x[c] = obs[3 * i + c] - ptpos[3 * q + c];
+    const double r = sqrt(x[0] * x[0] + x[1] * x[1] + x[2] * x[2]);
+    for (int c = 0; c < 3; ++c) x[c] /= r;
+    const cd ie = crcp(cmk(eps_pt[2 * q], eps_pt[2 * q + 1]));
+    const double ir3 = 1.0 / (r * r * r);
+    for (int a = 0; a < ndip; ++a) {
+        const double *d = dip + ((int64_t)q * 3) * ndip + a;       // d[c * ndip]
+        const double in = x[0] * d[0] + x[1] * d[ndip] + x[2] * d[2 * ndip];
+        double e[3];
+        for (int c = 0; c < 3; ++c) e[c] = (3.0 * x[c] * in - d[c * ndip]) * ir3;
+        if (nvec) {
+            const double *nv = nvec + 3 * i;
+            const double en = nv[0] * e[0] + nv[1] * e[1] + nv[2] * e[2];
+            out[((int64_t)i * npt + q) * ndip + a] = cscale(ie, -en);
+        } else {
+            for (int c = 0; c < 3; ++c)
+                out[(((int64_t)i * 3 + c) * npt + q) * ndip + a] = cscale(ie, e[c]);
         }
     }
 }
@@ -521,6 +562,22 @@ extern "C" int mnpb_dipole_field(void *stream, int64_t nobs, int64_t batch, int6
         (int)nobs, (int)npt, (int)ndip, obs, obs_med, ptpos, pt_med, dip, nmed, eps, k, nb,
         (cd *)e, (cd *)h);
     MNPB_LAUNCH_CHECK("dipole_field_kernel");
+    return MNPB_OK;
+}
+
+extern "C" int mnpb_dipole_stat_field(void *stream, int64_t nobs, int64_t npt, int64_t ndip,
+                                      const double *obs, const double *nvec,
+                                      const double *ptpos, const double *dip,
+                                      const double *eps_pt, double *out) {
+    clear_error();
+    MNPB_REQUIRE(nobs > 0 && nobs < (int64_t(1) << 31) && npt > 0 && npt < 65536 && ndip > 0 &&
+                     ndip < 4096,
+                 "dipole_stat_field: bad sizes");
+    MNPB_REQUIRE(obs && ptpos && dip && eps_pt && out, "dipole_stat_field: null pointer");
+    dim3 grid(ceil_div(nobs, 128), (unsigned)npt);
+    dipole_stat_kernel<<<grid, 128, 0, as_stream(stream)>>>((int)nobs, (int)npt, (int)ndip, obs,
+                                                            nvec, ptpos, dip, eps_pt, (cd *)out);
+    MNPB_LAUNCH_CHECK("dipole_stat_kernel");
     return MNPB_OK;
 }
 

@@ -493,6 +493,13 @@ class CompGreenStat(object):
     678-990).  Entries come from the retarded entry kernel at k = 0, where the
     phase is 1 and only the order-0 refined coefficients remain."""
 
+    def __new__(cls, p1, p2=None, **options):
+        # a point set as p1 (the reference's CompGreenStat(ComPoint, particle))
+        from .points import is_point_set, CompGreenStatPoints
+        if is_point_set(p1) and p2 is not None:
+            return CompGreenStatPoints(p1, p2, **options)
+        return super(CompGreenStat, cls).__new__(cls)
+
     def __init__(self, p1, p2=None, **options):
         if p2 is not None and p2 is not p1:
             raise NotImplementedError("CompGreenStat: only p1 is p2 is supported")

@@ -26,7 +26,8 @@ from .excitation import _inout_faces, pinfty
 from .greenfun import _nfaces, _points, refinematrix_csr
 from .materials import eps_k
 
-__all__ = ["Point", "ComPoint", "DipoleRet", "CompGreenRetPoints", "is_point_set"]
+__all__ = ["Point", "ComPoint", "DipoleRet", "DipoleStat", "CompGreenRetPoints",
+           "CompGreenStatPoints", "is_point_set"]
 
 
 class Point(object):
@@ -559,3 +560,228 @@ class DipoleRet(object):
         rad = np.real(sca / (2 * np.pi * k0) / (0.5 * nb[:, None] * gamma))
         rad0 = np.real(np.broadcast_to(nb[:, None] * gamma, (npt, ndip))).copy()
         return tot, rad, rad0
+
+
+class CompGreenStatPoints(CompGreenRetPoints):
+    """Quasistatic Green function between a point set (p1) and a particle
+    (p2): the reference's ``CompGreenStat(pt, p)`` (greenfun/compgreen_stat.py:
+    219-465 with a ComPoint as p1).  G = a_j / d and Gp = -a_j (pt - pos_j) /
+    d^3 for every point and face (no media: the surface charge radiates in
+    free space); pairs closer than RelCutoff boundary radii of the face
+    (greenfun/utils.py:43-140, the same rule as the retarded one) integrate
+    1/d and its gradient over the face's quadrature points.  These are the
+    k = 0 entries of ``CompGreenRetPoints``, evaluated by the same kernels
+    with every point connected to side 0 of every face."""
+
+    def __init__(self, pt, p, **options):
+        CompGreenRetPoints.__init__(self, pt, p, **options)
+        dev = self.device
+        self.ptmed_all = _dev(np.ones(self.npt, dtype=np.int32), dev)
+        fmed = np.zeros((self.faces.n, 2), dtype=np.int32)
+        fmed[:, 0] = 1
+        self.fmed_all = _dev(fmed, dev)
+        self.k_zero = torch.zeros(2, dtype=torch.float64, device=dev)
+
+    def _args_stat(self):
+        fd = self.faces
+        return (self.npt, ptr(self.ptpos), ptr(self.ptmed_all), fd.n, ptr(fd.pos), ptr(fd.area),
+                ptr(self.fmed_all), 1, ptr(self.k_zero), ptr(self.rptr), ptr(self.cols),
+                ptr(self.g), ptr(self.f))
+
+    def eval(self, *args):
+        """(npt, n) for G, (npt, 3, n) for Gp / H1p / H2p
+        (compgreen_stat.py:560-700); 0 for F, H1, H2 (points carry zero
+        normals).  The key is the last argument."""
+        key = args[-1]
+        if key not in ('G', 'F', 'H1', 'H2', 'Gp', 'H1p', 'H2p'):
+            raise ValueError("Unknown key: {}".format(key))
+        if key in ('F', 'H1', 'H2'):
+            return 0
+        vec = key != 'G'
+        n = self.faces.n
+        out = torch.zeros((self.npt, 3, n) if vec else (self.npt, n), dtype=torch.complex128,
+                          device=self.device)
+        call('mnpb_point_green_eval', _lib.stream_handle(), *self._args_stat(), 0, int(vec), 0, n,
+             ptr(out))
+        return out.cpu().numpy()
+
+    def apply_sig(self, sig, mode=0, diag=0):
+        """e (mode 0, (npt, 3, KC)) or phi (mode 1, (npt, KC)) at the points
+        for surface charges sig (n, K) on the device."""
+        n, K = sig.shape
+        sol = torch.zeros((1, 8, K, n), dtype=torch.complex128, device=self.device)
+        sol[0, 0] = sig.T
+        KC = diag if diag > 0 else K
+        c128 = dict(dtype=torch.complex128, device=self.device)
+        o1 = torch.empty((1, self.npt, 3, KC) if mode == 0 else (1, self.npt, KC), **c128)
+        o2 = torch.empty((1, self.npt, 3, KC), **c128)
+        k0 = torch.ones(1, dtype=torch.float64, device=self.device)
+        call('mnpb_point_green', _lib.stream_handle(), *self._args_stat(), mode, 1, K, diag,
+             ptr(k0), ptr(sol), ptr(o1), ptr(o2))
+        return o1[0]
+
+    def _sig(self, sig):
+        s = np.asarray(sig.sig)
+        n = self.faces.n
+        return s.shape[1:], torch.from_numpy(np.ascontiguousarray(
+            s.reshape(n, -1).astype(complex))).to(self.device)
+
+    def field(self, sig, inout=1):
+        """e = -Gp sig at the points (compgreen_stat.py:974-1009):
+        (npt, 3) + the trailing shape of sig."""
+        shape, s = self._sig(sig)
+        e = self.apply_sig(s, mode=0).cpu().numpy()
+        return CompStruct(self.p1, sig.enei, e=e.reshape((self.npt, 3) + shape))
+
+    def potential(self, sig, inout=1):
+        """phi = G sig at the points (compgreen_stat.py:1011-1060); the
+        surface derivative vanishes (zero point normals)."""
+        shape, s = self._sig(sig)
+        phi = self.apply_sig(s, mode=1).cpu().numpy().reshape((self.npt,) + shape)
+        if inout == 1:
+            return CompStruct(self.p1, sig.enei, phi1=phi, phi1p=np.zeros_like(phi))
+        return CompStruct(self.p1, sig.enei, phi2=phi, phi2p=np.zeros_like(phi))
+
+
+class DipoleStat(object):
+    """Oscillating dipoles at the points of a ComPoint, quasistatic
+    (mnpbem/simulation/dipole_stat.py:24-543).
+
+    ``dip``: moments (ndip, 3) shared by all points (default: the unit
+    triple), or (npt, 3[, ndip]) per point with ``full=True``.  The
+    excitation ``phip`` is (n, npt, ndip); ``BEMStat`` solves it column by
+    column (K = npt * ndip).
+    """
+
+    name = 'dipole'
+    needs = {'sim': 'stat'}
+
+    def __init__(self, pt, dip=None, full=False, **options):
+        self.pt = pt
+        self.varargin = options
+        if dip is None:
+            dip, full = np.eye(3), False
+        dip = np.asarray(dip, dtype=float)
+        h_pos, h_med = point_media(pt)
+        npt = h_pos.shape[0]
+        if npt == 0:
+            raise ValueError("DipoleStat: empty point set")
+        if full:
+            self.dip = dip.reshape(dip.shape + (1,)) if dip.ndim == 2 else dip
+        else:
+            dip = np.atleast_2d(dip)
+            self.dip = np.tile(dip.T.reshape(1, 3, dip.shape[0]), (npt, 1, 1))
+        if self.dip.shape[:2] != (npt, 3):
+            raise ValueError("DipoleStat: dipole moments must be (npt, 3, ndip)")
+        self.h_pos, self.h_med = h_pos, h_med
+        self._dev = None
+        self._greens = {}
+
+    @property
+    def ndip(self):
+        return self.dip.shape[2]
+
+    def _device(self):
+        if self._dev is None:
+            dev = torch.device('cuda')
+            self._dev = (dev, _dev(self.h_pos, dev),
+                         _dev(np.ascontiguousarray(self.dip, dtype=np.float64), dev))
+        return self._dev
+
+    def _run(self, obs, nvec, enei):
+        dev, ptpos, dip = self._device()
+        npt, ndip = self.h_pos.shape[0], self.ndip
+        eps = np.asarray(self.pt.eps1(enei), dtype=complex)
+        nobs = obs.shape[0]
+        shape = (nobs, npt, ndip) if nvec is not None else (nobs, 3, npt, ndip)
+        out = torch.empty(shape, dtype=torch.complex128, device=dev)
+        call('mnpb_dipole_stat_field', _lib.stream_handle(), nobs, npt, ndip, ptr(_dev(obs, dev)),
+             ptr(_dev(nvec, dev)) if nvec is not None else None, ptr(ptpos), ptr(dip),
+             ptr(_dev(eps, dev)), ptr(out))
+        return out.cpu().numpy()
+
+    def field(self, p, enei, inout=1):
+        """Electric field e (n, 3, npt, ndip) of the dipoles at the faces or
+        points of ``p`` (dipole_stat.py:149-250), screened by the dielectric
+        function at each dipole; ``inout`` is not used."""
+        obs = np.ascontiguousarray(np.asarray(p.pos, dtype=np.float64).reshape(-1, 3))
+        return CompStruct(p, enei, e=self._run(obs, None, enei))
+
+    def potential(self, p, enei):
+        """phip = -nvec . e at the faces (dipole_stat.py:252-289): (n, npt, ndip)."""
+        obs = np.ascontiguousarray(np.asarray(p.pos, dtype=np.float64))
+        nvec = np.ascontiguousarray(np.asarray(p.nvec, dtype=np.float64))
+        return CompStruct(p, enei, phip=self._run(obs, nvec, enei))
+
+    __call__ = potential
+
+    def _green(self, p):
+        key = id(p)
+        if key not in self._greens:
+            self._greens[key] = (p, CompGreenStatPoints(self.pt, p, **self.varargin))
+        return self._greens[key][1]
+
+    def decayrate(self, sig):
+        """Total, radiative and free-space decay rates (npt, ndip)
+        (dipole_stat.py:291-413): gamma = 4/3 k0^3, nb the refractive index
+        at the dipole, e_ind the field of sig at the dipole's own position,
+        indip = sum area pos sig the induced dipole:
+        tot = 1 + Im(e_ind . dip) / (0.5 nb gamma), rad = |nb^2 indip + dip|^2,
+        rad0 = nb gamma (real parts)."""
+        p = sig.p
+        g = self._green(p)
+        npt, ndip = self.h_pos.shape[0], self.ndip
+        s = np.asarray(sig.sig).reshape(g.faces.n, -1).astype(complex)
+        if s.shape[1] != npt * ndip:
+            raise ValueError("DipoleStat.decayrate: solution has %d columns, expected %d"
+                             % (s.shape[1], npt * ndip))
+        e = g.apply_sig(torch.from_numpy(np.ascontiguousarray(s)).to(g.device), mode=0,
+                        diag=ndip).cpu().numpy()                        # (npt, 3, ndip)
+        gamma = 4.0 / 3.0 * (2 * np.pi / sig.enei) ** 3
+        area_pos = np.asarray(p.pos, dtype=np.float64) * np.asarray(p.area)[:, None]
+        indip = (area_pos.T @ s).reshape(3, npt, ndip)
+        nb = np.sqrt(np.asarray(self.pt.eps1(sig.enei), dtype=complex))
+        dip = self.dip
+        rad = np.sum(np.abs(nb[None, :, None] ** 2 * indip + dip.transpose(1, 0, 2)) ** 2,
+                     axis=0)
+        ed = np.einsum('qcd,qcd->qd', e, dip)
+        tot = np.real(1 + np.imag(ed) / (0.5 * nb[:, None] * gamma))
+        rad0 = np.real(np.broadcast_to(nb[:, None] * gamma, (npt, ndip))).copy()
+        return tot, rad, rad0
+
+    def farfield(self, spec=None, enei=None):
+        """Far fields of the dipoles on the sphere at infinity
+        (dipole_stat.py:415-510): dipoles screened by eps_medium / eps at the
+        dipole, h = k^2/nb (dir x d) g, e = k^2/eps ((dir x d) x dir) g with
+        g = exp(-i k dir . pos); every dipole radiates when any point lies in
+        the medium of the sphere.  e, h (ndir, 3, npt, ndip)."""
+        if enei is None:
+            raise ValueError("DipoleStat.farfield: enei is required")
+        medium = getattr(spec, 'medium', 1) if spec is not None else 1
+        nvec = (np.asarray(spec.pinfty.nvec, dtype=np.float64) if spec is not None
+                else pinfty()[0])
+        dev, ptpos, _ = self._device()
+        npt, ndip = self.h_pos.shape[0], self.ndip
+        epsm, km = eps_k(self.pt.eps[medium - 1], enei)
+        scr = epsm / np.asarray(self.pt.eps1(enei), dtype=complex)
+        dip = self.dip[:, :, :] * scr[:, None, None]
+        on = np.full(npt, int(np.any(self.h_med == medium)), dtype=np.int8)
+        emb = np.array([[epsm, km, np.sqrt(epsm)]], dtype=complex)
+        nd = nvec.shape[0]
+        e = torch.zeros((1, npt * ndip, nd, 3), dtype=torch.complex128, device=dev)
+        h = torch.zeros_like(e)
+        # the screened moments are complex: real and imaginary parts radiate
+        # separately (the far field is linear in the moment)
+        out = []
+        for part in (np.real(dip), np.imag(dip)):
+            ee, hh = torch.zeros_like(e), torch.zeros_like(h)
+            call('mnpb_dipole_farfield', _lib.stream_handle(), nd, 1, npt, ndip, ptr(ptpos),
+                 ptr(_dev(on, dev)), ptr(_dev(np.ascontiguousarray(part), dev)),
+                 ptr(_dev(nvec, dev)), ptr(_dev(emb, dev)), ptr(ee), ptr(hh))
+            out.append((ee, hh))
+        e = out[0][0] + 1j * out[1][0]
+        h = out[0][1] + 1j * out[1][1]
+        shape = (npt, ndip, nd, 3)
+        e = e[0].cpu().numpy().reshape(shape).transpose(2, 3, 0, 1)
+        h = h[0].cpu().numpy().reshape(shape).transpose(2, 3, 0, 1)
+        return CompStruct(None, enei, e=e, h=h)
