@@ -31,7 +31,7 @@ from .greenfun import SurfaceTables
 from .excitation import PlaneWaveRet, PlaneWaveStat
 
 __all__ = ["flip", "ComParticleMirror", "CompStructMirror", "PlaneWaveRetMirror",
-           "BEMRetMirror", "PlaneWaveStatMirror", "BEMStatMirror"]
+           "BEMRetMirror", "PlaneWaveStatMirror", "BEMStatMirror", "DipoleStatMirror"]
 
 
 def flip(p, dirs):
@@ -501,16 +501,100 @@ class BEMStatMirror(object):
         for v in exc.val:
             ind = p.symindex(v.symval[-1, :])
             phip = np.asarray(v.phip)
-            K = 1 if phip.ndim == 1 else phip.shape[1]
+            K = phip.size // n                  # trailing axes (npt, ndip, ...) as columns
             B = torch.from_numpy(np.ascontiguousarray(phip.reshape(n, K).T.astype(complex))) \
                 .to(self.device).unsqueeze(0).contiguous()
             call('mnpb_getrs_f64', sh, n, 1, K, ptr(self._M[ind]), n, n * n, ptr(self._piv[ind]),
                  n, ptr(B), n, n * K)
-            x = B[0].cpu().numpy().T
-            out = CompStruct(p, exc.enei, sig=x[:, 0] if phip.ndim == 1 else x)
+            x = B[0].cpu().numpy().T.reshape(phip.shape)
+            out = CompStruct(p, exc.enei, sig=x)
             out.symval = v.symval
             sig.val.append(out)
         return sig, self
 
     def __truediv__(self, exc):
         return self.solve(exc)
+
+
+class DipoleStatMirror(object):
+    """Quasistatic dipoles next to a mirror-symmetric particle
+    (mnpbem/simulation/dipole_stat_mirror.py:15-274).
+
+    The unit dipoles at the points and at their mirror images (positions and
+    moments flipped at the symmetry planes) give one potential each;
+    their sums and differences are the excitations of the symmetry values
+    (x / y: phip_0 +- phip_1; xy: the four sign combinations of the images).
+    ``full`` takes the mean of the expanded solutions, the response to the
+    unit dipoles at the points on the full particle, and contracts it with
+    the requested moments; ``decayrate`` is ``DipoleStat.decayrate`` of that.
+    """
+
+    # image k: (axes flipped, moment signs of the unit triple)
+    _IMAGES = {'x': [((), (1, 1, 1)), ((0,), (-1, 1, 1))],
+               'y': [((), (1, 1, 1)), ((1,), (1, -1, 1))],
+               'xy': [((), (1, 1, 1)), ((0,), (-1, 1, 1)), ((1,), (1, -1, 1)),
+                      ((0, 1), (-1, -1, 1))]}
+    # symmetry values: (coefficients of the image potentials, symvalue keys)
+    _COMBOS = {'x': [((1, 1), ['-', '+', '+']), ((1, -1), ['+', '-', '-'])],
+               'y': [((1, 1), ['+', '-', '+']), ((1, -1), ['-', '+', '-'])],
+               'xy': [((1, 1, 1, 1), ['-+', '+-', '++']), ((1, -1, 1, -1), ['++', '--', '-+']),
+                      ((1, 1, -1, -1), ['--', '++', '+-']), ((1, -1, -1, 1), ['+-', '-+', '--'])]}
+
+    def __init__(self, pt, dip=None, full=False, **options):
+        from .points import DipoleStat
+        self.dip = DipoleStat(pt, dip, full=full, **options)
+        self.sym = None
+        self.mirror = []
+
+    def _init_mirror(self, p):
+        from .points import DipoleStat
+        if self.sym == p.sym:
+            return
+        pt = self.dip.pt
+        self.mirror = []
+        for axes, signs in self._IMAGES[p.sym]:
+            m = DipoleStat(pt, np.diag(np.asarray(signs, dtype=float)))
+            pos = m.h_pos.copy()
+            for a in axes:
+                pos[:, a] = -pos[:, a]
+            m.h_pos = np.ascontiguousarray(pos)
+            self.mirror.append(m)
+        self.sym = p.sym
+
+    def potential(self, p, enei):
+        """Excitation of every symmetry value, phip (n, npt, 3) of the
+        irreducible part (dipole_stat_mirror.py:87-152)."""
+        self._init_mirror(p)
+        ph = [m.potential(p, enei).phip for m in self.mirror]
+        exc = CompStructMirror(p, enei, lambda x: self.full(x))
+        for coef, key in self._COMBOS[p.sym]:
+            v = CompStruct(p, enei, phip=sum(c * a for c, a in zip(coef, ph)))
+            v.symval = p.symvalue(key)
+            exc.val.append(v)
+        return exc
+
+    __call__ = potential
+
+    def full(self, val):
+        """Surface charges on the full particle for the requested moments
+        (dipole_stat_mirror.py:154-248): (n_full, npt, ndip)."""
+        parts = val.expand()
+        pf = val.p.full()
+        out = CompStruct(pf, val.enei)
+        dip = self.dip.dip                                          # (npt, 3, ndip)
+        for name in ('sig', 'phi1', 'phi1p', 'phi2', 'phi2p'):
+            vecs = [e.val.get(name) for e in parts]
+            if not all(isinstance(v, np.ndarray) for v in vecs):
+                continue
+            mean = sum(vecs) / len(vecs)                            # (n_full, npt, 3)
+            out[name] = np.einsum('nic,icj->nij', mean.reshape(mean.shape[0], -1, 3), dip)
+        return out, pf
+
+    def field(self, p, enei, inout=1):
+        return self.dip.field(p, enei)
+
+    def decayrate(self, sig):
+        return self.dip.decayrate(self.full(sig)[0])
+
+    def farfield(self, spec=None, enei=None):
+        return self.dip.farfield(spec, enei)

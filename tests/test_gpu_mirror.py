@@ -93,3 +93,39 @@ def test_mirror_stat_solve(gpu_ok, sym):
             got = np.real(np.asarray(fn(sig)))
             # the near-zero pol-y entries of symmetry 'x' are held absolutely
             assert np.abs(got - want).max() < 1e-10 * np.abs(want).max(), (sym, lam, key)
+
+
+@pytest.mark.parametrize('sym', ['x', 'xy'])
+def test_mirror_dipole_stat(gpu_ok, sym):
+    """DipoleStatMirror + BEMStatMirror against the reference
+    (golden_dipole_mirror.npz): potentials of every symmetry value 1e-12,
+    surface charges 1e-10, decay rates 1e-9; and the decay rates agree with
+    DipoleStat + BEMStat on the full particle to 1e-5, the level at which the
+    mirror and full-particle solves agree for plane waves too (measured
+    5e-7 here)."""
+    from mnpbem_b200.mirror import BEMStatMirror, DipoleStatMirror
+    from mnpbem_b200.points import ComPoint, DipoleStat
+    z = golden('golden_mirror')
+    zd = golden('golden_dipole_mirror')
+    cpm = mirror_particle(z, sym)
+    pt = ComPoint(cpm, zd['pos_in'])
+    assert np.array_equal(np.asarray(pt.pos), zd[sym + '_pt_pos'])
+    exc = DipoleStatMirror(pt)
+    b = BEMStatMirror(cpm)
+    full = bem.BEMStat(cpm.full())
+    for i, lam in enumerate(zd['lams']):
+        pot = exc(cpm, float(lam))
+        sig, _ = b.solve(pot)
+        for v, (e, s) in enumerate(zip(pot.val, sig.val)):
+            pre = 'stat_%s_%d_%d_' % (sym, i, v)
+            assert np.array_equal(e.symval, zd[pre + 'symval'])
+            assert rel(e.phip, zd[pre + 'phip']) < 1e-12, (sym, lam, v)
+            assert rel(s.sig, zd[pre + 'sig']) < 1e-10, (sym, lam, v)
+        pre = 'stat_%s_%d_' % (sym, i)
+        tot, rad, rad0 = exc.decayrate(sig)
+        assert rel(tot, zd[pre + 'tot']) < 1e-9 and rel(rad, zd[pre + 'rad']) < 1e-9
+        assert rel(rad0, zd[pre + 'rad0']) < 1e-12
+        d = DipoleStat(pt)
+        sf, _ = full.solve(d(cpm.full(), float(lam)))
+        t2, r2, _ = d.decayrate(sf)
+        assert rel(tot, t2) < 1e-5 and rel(rad, r2) < 1e-5, (sym, lam)
