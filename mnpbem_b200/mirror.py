@@ -31,7 +31,8 @@ from .greenfun import SurfaceTables
 from .excitation import PlaneWaveRet, PlaneWaveStat
 
 __all__ = ["flip", "ComParticleMirror", "CompStructMirror", "PlaneWaveRetMirror",
-           "BEMRetMirror", "PlaneWaveStatMirror", "BEMStatMirror", "DipoleStatMirror"]
+           "BEMRetMirror", "PlaneWaveStatMirror", "BEMStatMirror", "DipoleStatMirror",
+           "DipoleRetMirror"]
 
 
 def flip(p, dirs):
@@ -516,17 +517,19 @@ class BEMStatMirror(object):
         return self.solve(exc)
 
 
-class DipoleStatMirror(object):
-    """Quasistatic dipoles next to a mirror-symmetric particle
-    (mnpbem/simulation/dipole_stat_mirror.py:15-274).
+class _DipoleMirror(object):
+    """Dipoles next to a mirror-symmetric particle
+    (mnpbem/simulation/dipole_stat_mirror.py:15-274,
+    dipole_ret_mirror.py:15-347).
 
     The unit dipoles at the points and at their mirror images (positions and
-    moments flipped at the symmetry planes) give one potential each;
+    moments flipped at the symmetry planes) give one excitation each;
     their sums and differences are the excitations of the symmetry values
-    (x / y: phip_0 +- phip_1; xy: the four sign combinations of the images).
-    ``full`` takes the mean of the expanded solutions, the response to the
-    unit dipoles at the points on the full particle, and contracts it with
-    the requested moments; ``decayrate`` is ``DipoleStat.decayrate`` of that.
+    (x / y: image 0 +- image 1; xy: the four sign combinations of the
+    images).  ``full`` takes the mean of the expanded solutions, the
+    response to the unit dipoles at the points on the full particle, and
+    contracts it with the requested moments; ``decayrate`` is the plain
+    dipole class's decay rate of that.
     """
 
     # image k: (axes flipped, moment signs of the unit triple)
@@ -534,26 +537,24 @@ class DipoleStatMirror(object):
                'y': [((), (1, 1, 1)), ((1,), (1, -1, 1))],
                'xy': [((), (1, 1, 1)), ((0,), (-1, 1, 1)), ((1,), (1, -1, 1)),
                       ((0, 1), (-1, -1, 1))]}
-    # symmetry values: (coefficients of the image potentials, symvalue keys)
+    # symmetry values: (coefficients of the image excitations, symvalue keys)
     _COMBOS = {'x': [((1, 1), ['-', '+', '+']), ((1, -1), ['+', '-', '-'])],
                'y': [((1, 1), ['+', '-', '+']), ((1, -1), ['-', '+', '-'])],
                'xy': [((1, 1, 1, 1), ['-+', '+-', '++']), ((1, -1, 1, -1), ['++', '--', '-+']),
                       ((1, 1, -1, -1), ['--', '++', '+-']), ((1, -1, -1, 1), ['+-', '-+', '--'])]}
 
     def __init__(self, pt, dip=None, full=False, **options):
-        from .points import DipoleStat
-        self.dip = DipoleStat(pt, dip, full=full, **options)
+        self.dip = self._klass()(pt, dip, full=full, **options)
         self.sym = None
         self.mirror = []
 
     def _init_mirror(self, p):
-        from .points import DipoleStat
         if self.sym == p.sym:
             return
         pt = self.dip.pt
         self.mirror = []
         for axes, signs in self._IMAGES[p.sym]:
-            m = DipoleStat(pt, np.diag(np.asarray(signs, dtype=float)))
+            m = self._klass()(pt, np.diag(np.asarray(signs, dtype=float)))
             pos = m.h_pos.copy()
             for a in axes:
                 pos[:, a] = -pos[:, a]
@@ -562,13 +563,15 @@ class DipoleStatMirror(object):
         self.sym = p.sym
 
     def potential(self, p, enei):
-        """Excitation of every symmetry value, phip (n, npt, 3) of the
-        irreducible part (dipole_stat_mirror.py:87-152)."""
+        """Excitation of every symmetry value on the irreducible part."""
         self._init_mirror(p)
-        ph = [m.potential(p, enei).phip for m in self.mirror]
+        vals = [m.potential(p, enei) for m in self.mirror]
         exc = CompStructMirror(p, enei, lambda x: self.full(x))
         for coef, key in self._COMBOS[p.sym]:
-            v = CompStruct(p, enei, phip=sum(c * a for c, a in zip(coef, ph)))
+            v = CompStruct(p, enei)
+            for name, a in vals[0].val.items():
+                if isinstance(a, np.ndarray):
+                    v[name] = sum(c * m.val[name] for c, m in zip(coef, vals))
             v.symval = p.symvalue(key)
             exc.val.append(v)
         return exc
@@ -576,18 +579,24 @@ class DipoleStatMirror(object):
     __call__ = potential
 
     def full(self, val):
-        """Surface charges on the full particle for the requested moments
-        (dipole_stat_mirror.py:154-248): (n_full, npt, ndip)."""
+        """Values on the full particle for the requested moments."""
         parts = val.expand()
         pf = val.p.full()
         out = CompStruct(pf, val.enei)
         dip = self.dip.dip                                          # (npt, 3, ndip)
-        for name in ('sig', 'phi1', 'phi1p', 'phi2', 'phi2p'):
+        npt, ndip = dip.shape[0], dip.shape[2]
+        for name in parts[0].val:
             vecs = [e.val.get(name) for e in parts]
             if not all(isinstance(v, np.ndarray) for v in vecs):
                 continue
-            mean = sum(vecs) / len(vecs)                            # (n_full, npt, 3)
-            out[name] = np.einsum('nic,icj->nij', mean.reshape(mean.shape[0], -1, 3), dip)
+            mean = sum(vecs) / len(vecs)
+            nf = mean.shape[0]
+            if name in _VECTORS:
+                r = np.einsum('nlic,icj->nlij', mean.reshape(nf, 3, npt, 3), dip)
+                out[name] = r.reshape(nf, 3, npt * ndip) if self._flat else r
+            else:
+                r = np.einsum('nic,icj->nij', mean.reshape(nf, npt, 3), dip)
+                out[name] = r.reshape(nf, npt * ndip) if self._flat else r
         return out, pf
 
     def field(self, p, enei, inout=1):
@@ -598,3 +607,36 @@ class DipoleStatMirror(object):
 
     def farfield(self, spec=None, enei=None):
         return self.dip.farfield(spec, enei)
+
+
+class DipoleStatMirror(_DipoleMirror):
+    """Quasistatic dipoles next to a mirror-symmetric particle
+    (mnpbem/simulation/dipole_stat_mirror.py:15-274): excitations phip
+    (n, npt, 3) per symmetry value for ``BEMStatMirror``; ``full`` gives
+    (n_full, npt, ndip)."""
+
+    _flat = False
+
+    @staticmethod
+    def _klass():
+        from .points import DipoleStat
+        return DipoleStat
+
+
+class DipoleRetMirror(_DipoleMirror):
+    """Retarded dipoles next to a mirror-symmetric particle
+    (mnpbem/simulation/dipole_ret_mirror.py:15-347): the eight potentials
+    of ``DipoleRet`` per symmetry value for ``BEMRetMirror``; ``full`` gives
+    the charges and currents on the full particle in ``DipoleRet``'s column
+    layout (point q, moment j at column q ndip + j); ``scattering`` and
+    ``decayrate`` are ``DipoleRet``'s of that."""
+
+    _flat = True
+
+    @staticmethod
+    def _klass():
+        from .points import DipoleRet
+        return DipoleRet
+
+    def scattering(self, sig):
+        return self.dip.scattering(self.full(sig)[0])

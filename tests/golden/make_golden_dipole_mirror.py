@@ -12,8 +12,11 @@ positions outside the sphere, ``ComPoint(p, pos)``, the unit moment triple.
 For 500 and 600 nm, ``golden_dipole_mirror.npz`` holds ``DipoleStatMirror``
 (mnpbem/simulation/dipole_stat_mirror.py:15) potentials phip with their
 symmetry values, the ``BEMStatMirror`` (mnpbem/bem/bem_stat_mirror.py:140)
-surface charges, and ``decayrate`` (tot, rad, rad0).  Only ``tests/`` read
-the output.
+surface charges, and ``decayrate`` (tot, rad, rad0); and the retarded
+``DipoleRetMirror`` (mnpbem/simulation/dipole_ret_mirror.py:15) with
+``BEMRetMirror`` (mnpbem/bem/bem_ret_mirror.py): potentials phi2p and a2p,
+surface charges sig2 and currents h2 of every symmetry value, and
+``decayrate`` (tot, rad).  Only ``tests/`` read the output.
 """
 
 import os
@@ -72,6 +75,28 @@ def main(ref_root):
             pre = 'stat_%s_%d_' % (sym, i)
             out[pre + 'tot'], out[pre + 'rad'], out[pre + 'rad0'] = tot, rad, rad0
             print(sym, lam, 'tot', tot[:, 0], flush=True)
+    from mnpbem.bem.bem_ret_mirror import BEMRetMirror
+    from mnpbem.simulation.dipole_ret_mirror import DipoleRetMirror
+    for sym, (ph, th) in CASES.items():
+        p = trispheresegment(np.linspace(*ph), np.linspace(*th), 20.0)
+        cpm = ComParticleMirror(eps, [p], [[2, 1]], sym, (1,))
+        pt = ComPoint(cpm, POS)
+        dip = DipoleRetMirror(pt)
+        bem = BEMRetMirror(cpm)
+        for i, lam in enumerate(LAMS):
+            exc = dip(cpm, lam)
+            sig, bem = bem.solve(exc)
+            for v, (e, s) in enumerate(zip(exc.val, sig.val)):
+                pre = 'ret_%s_%d_%d_' % (sym, i, v)
+                out[pre + 'phi2p'] = np.asarray(e.phi2p)
+                out[pre + 'a2p'] = np.asarray(e.a2p)
+                out[pre + 'symval'] = np.asarray(e.symval)
+                out[pre + 'sig2'] = np.asarray(s.sig2)
+                out[pre + 'h2'] = np.asarray(s.h2)
+            tot, rad = dip.decayrate(sig)[:2]
+            pre = 'ret_%s_%d_' % (sym, i)
+            out[pre + 'tot'], out[pre + 'rad'] = tot, rad
+            print('ret', sym, lam, 'tot', tot[:, 0], flush=True)
     np.savez_compressed(os.path.join(HERE, 'golden_dipole_mirror.npz'), **out)
     print('wrote golden_dipole_mirror.npz')
 

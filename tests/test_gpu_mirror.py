@@ -129,3 +129,31 @@ def test_mirror_dipole_stat(gpu_ok, sym):
         sf, _ = full.solve(d(cpm.full(), float(lam)))
         t2, r2, _ = d.decayrate(sf)
         assert rel(tot, t2) < 1e-5 and rel(rad, r2) < 1e-5, (sym, lam)
+
+
+@pytest.mark.parametrize('sym', ['x', 'xy'])
+def test_mirror_dipole_ret(gpu_ok, sym):
+    """DipoleRetMirror + BEMRetMirror against the reference
+    (golden_dipole_mirror.npz): potentials phi2p, a2p of every symmetry value
+    1e-12, charges sig2 and currents h2 1e-10, decay rates 1e-9."""
+    from mnpbem_b200.mirror import DipoleRetMirror
+    from mnpbem_b200.points import ComPoint
+    z = golden('golden_mirror')
+    zd = golden('golden_dipole_mirror')
+    cpm = mirror_particle(z, sym)
+    pt = ComPoint(cpm, zd['pos_in'])
+    exc = DipoleRetMirror(pt)
+    b = BEMRetMirror(cpm)
+    for i, lam in enumerate(zd['lams']):
+        pot = exc(cpm, float(lam))
+        sig, _ = b.solve(pot)
+        for v, (e, s) in enumerate(zip(pot.val, sig.val)):
+            pre = 'ret_%s_%d_%d_' % (sym, i, v)
+            assert np.array_equal(e.symval, zd[pre + 'symval'])
+            assert rel(e.phi2p, zd[pre + 'phi2p']) < 1e-12, (sym, lam, v)
+            assert rel(e.a2p, zd[pre + 'a2p']) < 1e-12, (sym, lam, v)
+            assert rel(s.sig2, zd[pre + 'sig2']) < 1e-10, (sym, lam, v)
+            assert rel(s.h2, zd[pre + 'h2']) < 1e-10, (sym, lam, v)
+        pre = 'ret_%s_%d_' % (sym, i)
+        tot, rad = exc.decayrate(sig)[:2]
+        assert rel(tot, zd[pre + 'tot']) < 1e-9 and rel(rad, zd[pre + 'rad']) < 1e-9, (sym, lam)
