@@ -32,7 +32,7 @@ from .excitation import PlaneWaveRet, PlaneWaveStat
 
 __all__ = ["flip", "ComParticleMirror", "CompStructMirror", "PlaneWaveRetMirror",
            "BEMRetMirror", "PlaneWaveStatMirror", "BEMStatMirror", "DipoleStatMirror",
-           "DipoleRetMirror"]
+           "DipoleRetMirror", "CompGreenRetMirror"]
 
 
 def flip(p, dirs):
@@ -640,3 +640,98 @@ class DipoleRetMirror(_DipoleMirror):
 
     def scattering(self, sig):
         return self.dip.scattering(self.full(sig)[0])
+
+
+class CompGreenRetMirror(object):
+    """Retarded Green function of a mirror-symmetric particle with itself
+    (mnpbem/greenfun/compgreen_ret_mirror.py:14-240): the full particle's
+    matrices (assembled on the GPU by ``CompGreenRet``), rows of the
+    irreducible part, contracted per symmetry value s as
+    g_s = sum_k symtable[s, k] M(:, block k); ``field`` gives the fields of
+    a mirror solution at the faces, per symmetry value."""
+
+    def __init__(self, p, p2=None, **options):
+        from .greenfun import CompGreenRet
+        if not isinstance(p, ComParticleMirror):
+            raise TypeError("CompGreenRetMirror: expected a ComParticleMirror")
+        self.p = p
+        self.g = CompGreenRet(p.pfull, **options)
+        self.device = torch.device('cuda')
+
+    def eval(self, i, j, key, enei):
+        """Contracted matrices, one per symmetry value: (n, n), or (n, 3, n)
+        for Gp / H1p / H2p; zeros where no block connects."""
+        p = self.p
+        n, nk = p.n, p.nk
+        tab = torch.from_numpy(np.ascontiguousarray(p.symtable)).to(self.device,
+                                                                    torch.complex128)
+        m = self.g.eval(i, j, key, enei)
+        if np.isscalar(m):
+            return [0] * tab.shape[0]
+        m = torch.as_tensor(np.asarray(m) if not torch.is_tensor(m) else m).to(self.device)
+        m = m[:n].to(torch.complex128)
+        if m.dim() == 2:
+            b = m.reshape(n, nk, n)
+            return [torch.einsum('k,rkc->rc', tab[s], b) for s in range(tab.shape[0])]
+        b = m.reshape(n, 3, nk, n)
+        return [torch.einsum('k,rlkc->rlc', tab[s], b) for s in range(tab.shape[0])]
+
+    @staticmethod
+    def _indmul(mats, v, ind):
+        if not torch.is_tensor(mats[0]):
+            return 0
+        return torch.stack([mats[ind[l]] @ v[:, l] for l in range(3)], dim=1)
+
+    @staticmethod
+    def _mm3(a, x):
+        if not torch.is_tensor(a):
+            return 0
+        return torch.stack([a[:, l] @ x for l in range(3)], dim=1)
+
+    @staticmethod
+    def _indcross(mats, v, ind):
+        if not torch.is_tensor(mats[0]):
+            return 0
+        im = lambda k, c: mats[ind[k]][:, c]
+        return torch.stack([im(2, 1) @ v[:, 2] - im(1, 2) @ v[:, 1],
+                            im(0, 2) @ v[:, 0] - im(2, 0) @ v[:, 2],
+                            im(1, 0) @ v[:, 1] - im(0, 1) @ v[:, 0]], dim=1)
+
+    def field(self, sig, inout=1):
+        """e = i k (G1 h1 + G2 h2) - H1p sig1 - H2p sig2 and
+        h = H1p x h1 + H2p x h2 for every symmetry value
+        (compgreen_ret_mirror.py:104-160): matrices of the symmetry value of
+        each Cartesian component, the z one for the charges; e, h (n, 3[, K])."""
+        p, enei = self.p, sig.enei
+        k = 2 * np.pi / enei
+        G1 = self.eval(inout - 1, 0, 'G', enei)
+        G2 = self.eval(inout - 1, 1, 'G', enei)
+        pk = 'H1p' if inout == 1 else 'H2p'
+        H1p = self.eval(inout - 1, 0, pk, enei)
+        H2p = self.eval(inout - 1, 1, pk, enei)
+        out = CompStructMirror(p, enei, sig.fun)
+        T = lambda a: torch.from_numpy(np.ascontiguousarray(np.asarray(a, dtype=complex))) \
+            .to(self.device)
+        for s in sig.val:
+            ind = [p.symindex(s.symval[l]) for l in range(3)]
+            one = np.asarray(s.sig1).ndim == 1
+            sig1, sig2 = T(s.sig1), T(s.sig2)
+            h1, h2 = T(s.h1), T(s.h2)
+            if one:
+                sig1, sig2 = sig1[:, None], sig2[:, None]
+                h1, h2 = h1[:, :, None], h2[:, :, None]
+            e = 0
+            for term in (1j * k * self._indmul(G1, h1, ind) if torch.is_tensor(G1[0]) else 0,
+                         -self._mm3(H1p[ind[2]], sig1) if torch.is_tensor(H1p[0]) else 0,
+                         1j * k * self._indmul(G2, h2, ind) if torch.is_tensor(G2[0]) else 0,
+                         -self._mm3(H2p[ind[2]], sig2) if torch.is_tensor(H2p[0]) else 0):
+                e = e + term
+            h = 0
+            for term in (self._indcross(H1p, h1, ind), self._indcross(H2p, h2, ind)):
+                h = h + term
+            cvt = lambda a: (a.cpu().numpy()[..., 0] if one else a.cpu().numpy()) \
+                if torch.is_tensor(a) else a
+            val = CompStruct(p, enei, e=cvt(e), h=cvt(h))
+            val.symval = s.symval
+            out.val.append(val)
+        return out

@@ -157,3 +157,32 @@ def test_mirror_dipole_ret(gpu_ok, sym):
         pre = 'ret_%s_%d_' % (sym, i)
         tot, rad = exc.decayrate(sig)[:2]
         assert rel(tot, zd[pre + 'tot']) < 1e-9 and rel(rad, zd[pre + 'rad']) < 1e-9, (sym, lam)
+
+
+@pytest.mark.parametrize('sym', ['x', 'xy'])
+def test_mirror_green_field(gpu_ok, sym):
+    """CompGreenRetMirror.field of the reference's own mirror solution
+    against the reference's fields (golden_mirror_field.npz), both sides,
+    every symmetry value, to 1e-10."""
+    from mnpbem_b200.compstruct import CompStruct
+    from mnpbem_b200.mirror import CompGreenRetMirror, CompStructMirror
+    z = golden('golden_mirror')
+    zf = golden('golden_mirror_field')
+    cpm = mirror_particle(z, sym)
+    lam = float(zf['lam'])
+    sig = CompStructMirror(cpm, lam)
+    nval = sum(1 for key in zf.files if key.startswith(sym + '_') and key.endswith('_sig1'))
+    assert nval == 2                    # the x- and y-polarised parts
+    for v in range(nval):
+        pre = '%s_%d_' % (sym, v)
+        s = CompStruct(cpm, lam, sig1=zf[pre + 'sig1'], h1=zf[pre + 'h1'], sig2=zf[pre + 'sig2'],
+                       h2=zf[pre + 'h2'])
+        s.symval = zf[pre + 'symval']
+        sig.val.append(s)
+    g = CompGreenRetMirror(cpm)
+    for inout in (1, 2):
+        f = g.field(sig, inout)
+        for v, fv in enumerate(f.val):
+            pre = '%s_%d_%d_' % (sym, v, inout)
+            assert rel(fv.e, zf[pre + 'e']) < 1e-10, (sym, v, inout)
+            assert rel(fv.h, zf[pre + 'h']) < 1e-10, (sym, v, inout)
